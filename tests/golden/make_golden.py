@@ -1,0 +1,179 @@
+"""Generate the golden vectors in tests/golden/ by running the REFERENCE's own Python (``insilica.gpu``,
+``insilica.layers``, ``insilica.transport``, ``insilica.grid``, ``insilica.cases``; unchanged, imported from the
+reference checkout) on a NumPy-backed CuPy stand-in (``fakecupy.py``) whose kernels are the reference's own CUDA C
+compiled for the host (``oracle/build_ref.py``), in the reference's FP64 form (``INSILICA_PRECISION=double``).
+
+Needs the reference sources (default /root/reference) and ``oracle/_ref`` built. Run from the repository root:
+
+    python tests/golden/make_golden.py [--ref /root/reference] [--cache /tmp/isw-grid-cache]
+
+Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
+- grid_n4.npz    the reference's level-4 grid (Hilbert order), the arrays the step, the tables and the states use
+- w2_n4.npz      Williamson 2, one layer, dt 900 s, Omega 7.292e-5: states after 1, 96 and 480 steps
+- air3_n4.npz    three-layer air stack (terrain, nu4, interfacial stress, nfast 20, 3 FCT tracers): 6 steps
+- ocean2_n4.npz  two-layer ocean stack (bottom and interfacial stress): 6 steps
+- outcrop_n4.npz the reference's own 'outcrop' case (floor, stress, nu4) with the cosine-bell tracer: 24 steps
+- bell_n4.npz    transport alone (solid-body flux): 20 steps of order 1 and of order 3
+- dsum.npz       deterministic tree sums of fixed inputs
+"""
+import argparse
+import hashlib
+import math
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+
+GRID_KEYS = ('n', 'N', 'E', 'NV', 'eI', 'eJ', 'eKi', 'eKj', 'nbr', 'deg', 'cellEdge', 'cellEdgeAsc', 'cellSign', 'ev1', 'ev2',
+             'vEdge', 'vEdgeSign', 'vCell', 'vSlot', 'eoeStart', 'eoe', 'cornerV', 'circ1', 'circ2', 'perm',
+             'le', 'de', 'dist', 'edgeLen', 'areaCell', 'areaV', 'area', 'kite', 'w', 'fV', 'pos', 'lat', 'lon', 'xm', 'ne',
+             'vPos', 'lloydIters')
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def save(name, d):
+    out = {}
+    for k, v in d.items():
+        v = np.asarray(v)
+        out[k] = v
+        if v.dtype.kind in 'fiub' and v.ndim > 0:
+            out[f'sha_{k}'] = np.asarray(sha(v))
+    np.savez_compressed(HERE / name, **out)
+    print(name, (HERE / name).stat().st_size, 'bytes')
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--cache', default='/tmp/isw-grid-cache')
+    a = ap.parse_args()
+    os.environ['INSILICA_PRECISION'] = 'double'
+    os.environ['INSILICA_CACHE'] = a.cache
+    sys.path.insert(0, str(HERE))
+    sys.path.insert(0, str(Path(a.ref) / 'src'))
+    sys.path.insert(0, str(ROOT / 'insilica-world-v2_b200'))
+    import fakecupy
+    fakecupy.install()
+    cp = fakecupy
+    from insilica import cases as rcases
+    from insilica import grid as gridmod
+    from insilica.gpu import DeviceGrid, dsum
+    from insilica.layers import Layers
+    from insilica.transport import Transport
+    from isw import cases as mycases
+
+    base = gridmod.get(4)
+    save('grid_n4.npz', {k: getattr(base, k) for k in GRID_KEYS})
+
+    # ---- config 1: Williamson 2, one layer ----
+    g = gridmod.for_planet(base, 6.371e6, 7.292e-5, 9.80616)
+    dg = DeviceGrid(g)
+    h0, b, u0 = rcases.initial_state(g, 'w2')
+    core = Layers(dg, 1, b=b)
+    h, u = cp.asarray(h0[None]), cp.asarray(u0[None])
+    dt = 900.0
+    sub = core.substeps(h, dt)
+    nfast = int(math.ceil(1.2 * sub))
+    d = dict(omega=7.292e-5, dt=dt, substeps=sub, nfast=nfast, h0=h0[None], u0=u0[None], b=b, energy0=core.energy(h, u))
+    for s in range(1, 481):
+        core.step(h, u, dt, nfast)
+        if s in (1, 96, 480):
+            d[f'h{s}'], d[f'u{s}'] = h.get(), u.get()
+    d['energy480'] = core.energy(h, u)
+    save('w2_n4.npz', d)
+
+    # ---- the stacked-layer workloads (this project's synthetic states) at n = 4, 6 steps with transport ----
+    def run_stack(kind, steps, dt, seed=7):
+        s = mycases.stack_state(g, kind, seed)
+        L = s['L']
+        core = Layers(dg, L, b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'], vmix=s['vmix'])
+        tr = Transport(dg, layers=L, tracers=3)
+        h, u = cp.asarray(s['h']), cp.asarray(s['u'])
+        M = cp.asarray(s['h'] * g.areaCell[None])
+        trc = [cp.asarray(t) for t in s['tracers']]
+        Fm, M1 = cp.zeros((L, g.E)), cp.zeros((L, g.N))
+        out = dict(kind=kind, seed=seed, L=L, dt=dt, nfast=20, h0=s['h'], u0=s['u'], b=s['b'], gprime=s['gprime'],
+                   stress=s['stress'], nu4=s['nu4'], floor=s['floor'], vmix=s['vmix'], lap_max=core.lap_max(),
+                   substeps=core.substeps(h, dt),
+                   energy0=core.energy(h, u))
+        for k, t in enumerate(s['tracers']):
+            out[f'tr{k}_0'] = t
+        for st in range(1, steps + 1):
+            core.step(h, u, dt, 20, Fm)
+            tr.mass_after(M, Fm, M1)
+            tr.step_many(M, M1, Fm, trc, order=3)
+            cp.copyto(M, M1)
+            if st == 1:
+                out['sha_h1'], out['sha_u1'] = sha(h), sha(u)
+                out['sha_M1'] = sha(M)
+                for k, t in enumerate(trc):
+                    out[f'sha_tr{k}_1'] = sha(t)
+        out.update(h=h.get(), u=u.get(), M=M.get(), Fm=Fm.get(), energy=core.energy(h, u))
+        for k, t in enumerate(trc):
+            out[f'tr{k}'] = t.get()
+        return out
+
+    save('air3_n4.npz', run_stack('air', 6, mycases.stack_dt(4)))
+    save('ocean2_n4.npz', run_stack('ocean', 6, mycases.stack_dt(4)))
+
+    # ---- the reference's own outcrop case (reference cases.py:174-182, PRESETS['outcrop']), with the bell tracer ----
+    g0 = base
+    dg0 = DeviceGrid(g0)
+    ho, bo, uo = rcases.outcrop(g0)
+    nu4 = mycases.visc4(g0, 0.5)
+    core = Layers(dg0, 2, b=bo, gprime=[0.02], stress=[0.0, 2.5e-4], nu4=nu4, floor=1.0)
+    tr = Transport(dg0, layers=2, tracers=4)
+    h, u = cp.asarray(ho), cp.asarray(uo)
+    dt = 3600.0
+    nfast = int(math.ceil(1.2 * core.substeps(h, dt)))
+    M = cp.asarray(ho * g0.areaCell[None])
+    psi = cp.asarray(np.tile(rcases.cosine_bell(g0), (2, 1)))
+    d = dict(dt=dt, nfast=nfast, nu4=nu4, h0=ho, u0=uo, b=bo, psi0=psi.get(), lap_max=core.lap_max())
+    Fm, M1 = cp.zeros((2, g0.E)), cp.zeros((2, g0.N))
+    lo = float(h.min())
+    for st in range(1, 25):
+        core.step(h, u, dt, nfast, Fm)
+        tr.mass_after(M, Fm, M1)
+        tr.step_many(M, M1, Fm, [psi], order=3)
+        cp.copyto(M, M1)
+        lo = min(lo, float(h.min()))
+    d.update(h=h.get(), u=u.get(), M=M.get(), psi=psi.get(), Fm=Fm.get(), hmin=lo)
+    save('outcrop_n4.npz', d)
+
+    # ---- transport alone: the cosine bell in solid-body rotation (reference tests/test_accuracy.py:32-48) ----
+    steps = 576
+    dtb = 12 * 86400 / steps
+    _, fm = mycases.solid_body_flux(g0, dtb)
+    d = dict(dt=dtb, Fm=fm[None], psi0=rcases.cosine_bell(g0)[None], M0=g0.areaCell[None])
+    for order in (1, 3):
+        trb = Transport(dg0)
+        psi = cp.asarray(d['psi0'])
+        Mb, Mb1 = cp.asarray(d['M0']), cp.zeros((1, g0.N))
+        Fmb = cp.asarray(d['Fm'])
+        for _ in range(20):
+            trb.mass_after(Mb, Fmb, Mb1)
+            trb.step(Mb, Mb1, Fmb, psi, order)
+            Mb, Mb1 = Mb1, Mb
+        d[f'psi_o{order}'], d[f'M_o{order}'] = psi.get(), Mb.get()
+    save('bell_n4.npz', d)
+
+    # ---- deterministic sums (reference gpu.py:111-126, kernels/trisk.cu:61-81) ----
+    d = {}
+    for n in (1, 2, 255, 2048, 2049, 100003, 1 << 20):
+        i = np.arange(n, dtype=np.int64)
+        x = ((i * 7919) % 10007 - 5003) / 997.0
+        y = ((i * 104729) % 65521) / 4093.0
+        d[f'x_{n}'] = dsum(cp.asarray(x))
+        d[f'xy_{n}'] = dsum(cp.asarray(x), cp.asarray(y))
+    save('dsum.npz', d)
+
+
+if __name__ == '__main__':
+    main()
