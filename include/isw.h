@@ -1,0 +1,110 @@
+/* isw: B200 (sm_100a) dynamical core for the stacked-layer TRiSK shallow-water step and FCT tracer transport.
+ *
+ * C ABI. Every function returns ISW_OK (0) or an error status and never throws; isw_last_error() gives the message of
+ * the calling thread's last failure. Device arrays are plain pointers to the caller's CUDA memory (FP64, C-contiguous,
+ * layer-major x[k * n + i] as the reference lays them out); `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream). Handles are not thread-safe; different handles may be used from different threads on
+ * different streams. Host arrays passed to the create functions are copied; device arrays passed to step functions are
+ * borrowed for the call only (all work is queued on `stream`; nothing is allocated during a step).
+ *
+ * Reference interfaces replaced (paths in goofyboson/insilica-world-v2):
+ *   isw_grid_create            src/insilica/gpu.py:55-83     DeviceGrid(grid)            (+ d2_stencil, gpu.py:86-108)
+ *   isw_layers_create          src/insilica/layers.py:36-92  Layers(dg, layers, b, ...)
+ *   isw_layers_step            src/insilica/layers.py:185-212 Layers.step(h, u, dt, nfast, Fm)
+ *   isw_layers_substeps        src/insilica/layers.py:99-102 Layers.substeps(h, dt)
+ *   isw_layers_lap             src/insilica/layers.py:123-127 Layers._lap(u, out)   (used by lap_max, :111-121)
+ *   isw_transport_create       src/insilica/transport.py:19-30 Transport(dg, layers, beta, tracers)
+ *   isw_transport_mass_after   src/insilica/transport.py:32-35 Transport.mass_after(M0, Fm, M1)
+ *   isw_transport_step_many    src/insilica/transport.py:40-71 Transport.step_many(M0, M1, Fm, tracers, order)
+ *   isw_dsum                   src/insilica/gpu.py:111-126   dsum(x, y)
+ */
+#ifndef ISW_H
+#define ISW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ISW_OK = 0,
+  ISW_EINVAL = 1,        /* bad argument: null handle or pointer, size or shape mismatch, out-of-range index table */
+  ISW_ECUDA = 2,         /* a CUDA runtime call failed (the message names it) */
+  ISW_ENOMEM = 3,        /* device or host allocation failed at create time */
+  ISW_EUNSUPPORTED = 4,  /* an option of the reference API this build does not implement (air, walls, shelf, ...) */
+  ISW_ETIMEOUT = 5,      /* a bounded device-side wait gave up (persistent kernels); the context stays usable */
+  ISW_ENOTFINITE = 6     /* reserved: a NaN/Inf budget */
+};
+
+enum { ISW_FP64 = 0, ISW_MIXED = 1 };   /* precision forms: plain FP64 (reference parity) or mixed FP32/FP64 */
+
+typedef struct isw_grid isw_grid;
+typedef struct isw_layers isw_layers;
+typedef struct isw_transport isw_transport;
+
+/* A host grid: the reference Grid's arrays (names as in src/insilica/grid/trisk.py and icosa.py). Sizes: N cells, E
+ * edges, NV vertices; tables int32 (pads -1), signs and slots int8, geometry FP64. deg, dist, eKi, eKj feed the
+ * 3rd-order transport stencil (gpu.py:86-108). */
+typedef struct isw_grid_host {
+  int n, N, E, NV;
+  const int32_t *eI, *eJ;                 /* E */
+  const int32_t *nbr, *cellEdge, *cellEdgeAsc; /* N x 6 */
+  const int8_t *cellSign;                 /* N x 6 */
+  const int32_t *ev1, *ev2;               /* E */
+  const int32_t *vEdge, *vCell;           /* NV x 3 */
+  const int8_t *vEdgeSign, *vSlot;        /* NV x 3 */
+  const int32_t *eoeStart;                /* E + 1 */
+  const int32_t *eoe;                     /* eoeStart[E] */
+  const double *le, *de;                  /* E */
+  const double *areaCell;                 /* N */
+  const double *areaV, *fV;               /* NV */
+  const double *kite;                     /* N x 6 */
+  const double *w;                        /* eoeStart[E] */
+  const uint8_t *deg;                     /* N */
+  const double *dist;                     /* N x 6 */
+  const uint8_t *eKi, *eKj;               /* E */
+} isw_grid_host;
+
+/* Layers options (reference layers.py:36-37). Boussinesq layers only: the air, wall, shelf, shelf_bed, sig/zm, tide and
+ * cd_bot/cbot options are not implemented (ISW_EUNSUPPORTED when the Python facade is asked for them). */
+typedef struct isw_layers_params {
+  int L;                                  /* 1 .. 8 */
+  double grav;
+  const double *gprime;                   /* L - 1 values (host) */
+  const double *drag, *stress;            /* L values each (host) */
+  double nu4, floor_, rotation, div_damp, thin, vmix, vmix_cd;
+  const double *b;                        /* N topography (host) or NULL for none */
+  int precision;                          /* ISW_FP64 or ISW_MIXED */
+} isw_layers_params;
+
+const char *isw_last_error(void);
+int isw_version(void);
+
+int isw_grid_create(const isw_grid_host *g, int device, isw_grid **out);
+int isw_grid_destroy(isw_grid *g);
+
+int isw_layers_create(isw_grid *g, const isw_layers_params *p, isw_layers **out);
+int isw_layers_destroy(isw_layers *s);
+/* One time-split RK3 step in place on h (L x N), u (L x E); Fm (L x E, or NULL) receives l dt F of the final stage. */
+int isw_layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, void *stream);
+/* max(1, ceil(dt sqrt(max_i g sum_k h_k) / (0.5 d_min))): synchronises `stream`. */
+int isw_layers_substeps(isw_layers *s, const double *h, double dt, int *out, void *stream);
+/* out (L x E) = the edge vector Laplacian of u (L x E). */
+int isw_layers_lap(isw_layers *s, const double *u, double *out, void *stream);
+
+int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int precision, isw_transport **out);
+int isw_transport_destroy(isw_transport *t);
+/* M1 (L x N) = M0 moved by the volume fluxes Fm (L x E). */
+int isw_transport_mass_after(isw_transport *t, const double *M0, const double *Fm, double *M1, void *stream);
+/* Move each of the ntr tracers (device pointers to L x N arrays, given in a host array) in place by Fm; order 1 or 3. */
+int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1, const double *Fm, double *const *tracers,
+                            int ntr, int order, void *stream);
+
+/* Deterministic sum of x[0..n) (or of x * y): the reference's fixed tree; synchronises `stream`, writes *out. */
+int isw_dsum(const double *x, const double *y, long long n, double *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,73 @@
+// Shared definitions of the isw dynamical core: device-side grid and layer descriptors, error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string>
+#include <vector>
+
+#include "../../include/isw.h"
+
+namespace isw {
+
+constexpr int LMAX = 8;          // layers per column (reference layers.py:30)
+constexpr int TRMAX = 16;        // tracers moved in one transport call
+constexpr int THREADS = 256;     // threads per block of the phase kernels
+
+// Thrown inside the library, turned into a status at the C ABI.
+struct Error {
+  int status;
+  std::string msg;
+};
+
+void set_last_error(const std::string &m);
+[[noreturn]] void fail(int status, const std::string &m);
+void check_cuda(cudaError_t e, const char *what);
+#define ISW_CUDA(call) ::isw::check_cuda((call), #call)
+
+// The grid on the device: index tables int32 (pads -1), signs and slots int8, geometry FP64, plus FP32 copies of what the
+// mixed form reads (weights, stencil weights, reciprocals of the metrics it divides by).
+struct GridDev {
+  int N, E, NV, nE2;              // nE2 = eoeStart[E], the length of the TRiSK CSR
+  const int *eI, *eJ, *nbr, *cellEdge, *cellEdgeAsc, *ev1, *ev2, *vEdge, *vCell, *eoeStart, *eoe, *d2idx;
+  const int8_t *cellSign, *vEdgeSign, *vSlot;
+  const double *le, *de, *areaCell, *areaV, *fV, *kite, *w, *d2wt;
+  const float *w32, *d2wt32, *le32, *de32, *rde32, *rA32, *rAV32, *kite32;
+  const double *rA, *rde, *rAV;   // FP64 reciprocals (mixed form multiplies where the reference divides)
+};
+
+// Scratch and parameters of one Layers object (reference layers.py:36-92), by value in kernel parameters.
+struct LayersDev {
+  GridDev g;
+  int L, precision;
+  double grav, nu4, floor_, div_damp, thin, vmix, vmix_cd;
+  double gp[LMAX], drag[LMAX], stress[LMAX];
+  const double *b, *fV, *Gc;
+  double *B, *q, *Tp, *F, *scale, *G, *He, *ubs, *ub0, *ub, *acc, *eta0, *eta, *eta_prev;
+  double *h1, *h2, *u1, *u2, *D1, *Z1, *L1, *L2, *hedge, *diss, *pk;
+  float *q32, *B32, *Tp32, *G32, *pk32;      // mixed-form scratch
+  double *red;                               // reduction scratch (substeps)
+};
+
+// Arguments of one RK3 stage (reference layers.py:129-183).
+struct StageArgs {
+  const double *hs, *us, *h0, *u0;
+  double *hn, *un, *Fm;
+  double cdt, dt, tau, inv_n;
+  int n;                                     // fast sub-steps of this stage
+};
+
+inline int blocks_for(long long n, int threads = THREADS) {
+  long long b = (n + threads - 1) / threads;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace isw
+
+struct isw_grid {
+  int device;
+  int n;
+  isw::GridDev d;
+  std::vector<void *> allocs;
+  double dmin;                   // smallest edge spacing (Layers.dmin)
+};

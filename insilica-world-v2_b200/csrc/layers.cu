@@ -1,0 +1,398 @@
+// The stacked-layer step (reference src/insilica/layers.py:35-212): kernels over the phase functions of layers_fp64.cuh,
+// the step's launch sequence, the CUDA-graph cache for direct calls, and the Layers part of the C ABI.
+//
+// Launch sequence of one step: init, [lap cv, lap e] x 2 if nu4, then per stage: A, E, S, n x (eta, ubar), C, D; then
+// vmix if set. 21 + 2 sum_s n_s launches (95 at nfast = 20), against the reference's 35 + 2 sum_s n_s (+6 with nu4).
+// A direct call (stream not capturing) replays a cached CUDA graph of the whole step: one launch from the host.
+#include <cmath>
+#include <cstring>
+#include <list>
+#include <sstream>
+
+#include "common.cuh"
+#include "layers_fp64.cuh"
+
+namespace isw {
+namespace {
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_init(const LayersDev M, const double *__restrict__ h, const double *__restrict__ u) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::eta0_cell<L>(M, h, t);
+  else if (t < M.g.N + M.g.E) fp64::ubar0_edge<L>(M, h, u, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_lap_cv(const LayersDev M, const double *__restrict__ u) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::div_cell<L>(M, u, t);
+  else if (t < M.g.N + M.g.NV) fp64::curl_vertex<L>(M, u, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_lap_e(const LayersDev M, double *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::lap_edge<L>(M, out, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_stage_a(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::bern_cell<L>(M, a.hs, a.us, t);
+  else if (t < M.g.N + M.g.NV) fp64::pv_vertex<L>(M, a.hs, a.us, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_stage_e(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::edge_hq<L>(M, a.hs, a.us, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_stage_s(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::slow_edge<L>(M, a.us, a.cdt, t);
+}
+
+__global__ void __launch_bounds__(THREADS) k_bt_eta(const LayersDev M, double tau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::bt_eta_cell(M, tau, t);
+}
+
+__global__ void __launch_bounds__(THREADS) k_bt_u(const LayersDev M, double tau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::bt_u_edge(M, tau, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_stage_c(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::scale_cell<L>(M, a, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_stage_d(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::h_cell<L>(M, a, t);
+  else if (t < M.g.N + M.g.E) fp64::u_edge<L>(M, a, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_vmix(const LayersDev M, const double *__restrict__ h, double *__restrict__ u, double dt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::vmix_edge<L>(M, h, u, dt, t);
+}
+
+// max over cells of g sum_k h_k: per-block maxima, then one block over them (values are >= 0 for a valid state;
+// NaN propagates as NaN through fmax's operand order below only if every value is NaN, so a separate flag counts NaNs)
+__global__ void __launch_bounds__(THREADS) k_colmax(const LayersDev M, const double *__restrict__ h, double *out, int *nonfinite) {
+  __shared__ double s[THREADS];
+  double m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.g.N; i += gridDim.x * blockDim.x) {
+    double c = 0;
+    for (int k = 0; k < M.L; k++) c += h[(size_t)k * M.g.N + i];
+    const double v = c * M.Gc[i];
+    if (!isfinite(v)) atomicAdd(nonfinite, 1);
+    else m = fmax(m, v);
+  }
+  s[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+__global__ void k_max_reduce(const double *in, int n, double *out) {
+  __shared__ double s[THREADS];
+  double m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, in[i]);
+  s[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+#define ISW_DISPATCH_L(L, CALL)                      \
+  switch (L) {                                        \
+    case 1: { constexpr int LL = 1; CALL; } break;    \
+    case 2: { constexpr int LL = 2; CALL; } break;    \
+    case 3: { constexpr int LL = 3; CALL; } break;    \
+    case 4: { constexpr int LL = 4; CALL; } break;    \
+    case 5: { constexpr int LL = 5; CALL; } break;    \
+    case 6: { constexpr int LL = 6; CALL; } break;    \
+    case 7: { constexpr int LL = 7; CALL; } break;    \
+    case 8: { constexpr int LL = 8; CALL; } break;    \
+    default: fail(ISW_EINVAL, "layers: L outside 1..8"); \
+  }
+
+}  // namespace
+}  // namespace isw
+
+using namespace isw;
+
+struct GraphEntry {
+  const double *h, *u, *Fm;
+  double dt;
+  int nfast;
+  cudaGraphExec_t exec;
+};
+
+struct isw_layers {
+  isw_grid *grid;
+  LayersDev d;
+  std::vector<void *> allocs;
+  cudaStream_t cap;                 // private stream the step graphs are captured on
+  std::list<GraphEntry> graphs;     // most recent first
+  int colmax_blocks;
+  int *nonfinite;
+};
+
+namespace {
+
+constexpr size_t GRAPH_CACHE = 8;
+
+double *dalloc(isw_layers *s, size_t n) {
+  void *p = nullptr;
+  ISW_CUDA(cudaMalloc(&p, sizeof(double) * (n ? n : 1)));
+  s->allocs.push_back(p);
+  ISW_CUDA(cudaMemset(p, 0, sizeof(double) * (n ? n : 1)));
+  return (double *)p;
+}
+
+// The step's kernels in order on `st` (reference layers.py:185-212, Boussinesq branch).
+void enqueue_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
+  const LayersDev &M = s->d;
+  const GridDev &g = M.g;
+  const int L = M.L;
+  const int N = g.N, E = g.E, NV = g.NV;
+  ISW_DISPATCH_L(L, (k_init<LL><<<blocks_for(N + E), THREADS, 0, st>>>(M, h, u)));
+  if (M.nu4 != 0) {
+    ISW_DISPATCH_L(L, (k_lap_cv<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, u)));
+    ISW_DISPATCH_L(L, (k_lap_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, M.L1)));
+    ISW_DISPATCH_L(L, (k_lap_cv<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, M.L1)));
+    ISW_DISPATCH_L(L, (k_lap_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, M.L2)));
+  }
+  const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
+  for (int st_i = 0; st_i < 3; st_i++) {
+    const double c = cs[st_i];
+    StageArgs a;
+    a.h0 = h;
+    a.u0 = u;
+    a.hs = st_i == 0 ? h : st_i == 1 ? M.h1 : M.h2;
+    a.us = st_i == 0 ? u : st_i == 1 ? M.u1 : M.u2;
+    a.hn = st_i == 0 ? M.h1 : st_i == 1 ? M.h2 : h;
+    a.un = st_i == 0 ? M.u1 : st_i == 1 ? M.u2 : u;
+    a.Fm = st_i == 2 ? Fm : nullptr;
+    a.cdt = c * dt;
+    a.dt = dt;
+    const double cn = std::ceil(c * nfast);
+    a.n = cn > 1 ? (int)cn : 1;
+    a.tau = c * dt / a.n;
+    a.inv_n = 1.0 / a.n;
+    ISW_DISPATCH_L(L, (k_stage_a<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_stage_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_stage_s<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a)));
+    for (int j = 0; j < a.n; j++) {
+      k_bt_eta<<<blocks_for(N), THREADS, 0, st>>>(M, a.tau);
+      k_bt_u<<<blocks_for(E), THREADS, 0, st>>>(M, a.tau);
+    }
+    ISW_DISPATCH_L(L, (k_stage_c<LL><<<blocks_for(N), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_stage_d<LL><<<blocks_for(N + E), THREADS, 0, st>>>(M, a)));
+  }
+  if ((M.vmix != 0 || M.vmix_cd != 0) && L > 1)
+    ISW_DISPATCH_L(L, (k_vmix<LL><<<blocks_for(E), THREADS, 0, st>>>(M, h, u, dt)));
+  ISW_CUDA(cudaGetLastError());
+}
+
+isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
+  if (!g || !p) fail(ISW_EINVAL, "layers: null grid or parameters");
+  if (p->L < 1 || p->L > LMAX) fail(ISW_EINVAL, "layers: L must be in 1..8");
+  if (p->L > 1 && !p->gprime) fail(ISW_EINVAL, "layers: gprime needs L - 1 values");
+  if (p->precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers: the mixed form is not built yet");
+  ISW_CUDA(cudaSetDevice(g->device));
+  isw_layers *s = new isw_layers();
+  s->grid = g;
+  try {
+    LayersDev &d = s->d;
+    std::memset(&d, 0, sizeof(d));
+    d.g = g->d;
+    d.L = p->L;
+    d.precision = p->precision;
+    d.grav = p->grav;
+    d.nu4 = p->nu4;
+    d.floor_ = p->floor_;
+    d.div_damp = p->div_damp;
+    d.thin = p->thin;
+    d.vmix = p->vmix;
+    d.vmix_cd = p->vmix_cd;
+    for (int k = 0; k < LMAX; k++) {
+      d.gp[k] = (p->L > 1 && k < p->L - 1) ? p->gprime[k] : 0.0;
+      d.drag[k] = (p->drag && k < p->L) ? p->drag[k] : 0.0;
+      d.stress[k] = (p->stress && k < p->L) ? p->stress[k] : 0.0;
+    }
+    const int N = g->d.N, E = g->d.E, NV = g->d.NV, L = p->L;
+    double *b = dalloc(s, N);
+    if (p->b) ISW_CUDA(cudaMemcpy(b, p->b, sizeof(double) * N, cudaMemcpyHostToDevice));
+    d.b = b;
+    std::vector<double> hv(NV);
+    ISW_CUDA(cudaMemcpy(hv.data(), g->d.fV, sizeof(double) * NV, cudaMemcpyDeviceToHost));
+    for (int v = 0; v < NV; v++) hv[v] = hv[v] * p->rotation;       // self.fV = dg.fV * rotation (layers.py:62)
+    double *fV = dalloc(s, NV);
+    ISW_CUDA(cudaMemcpy(fV, hv.data(), sizeof(double) * NV, cudaMemcpyHostToDevice));
+    d.fV = fV;
+    std::vector<double> gc(N, p->grav);
+    double *Gc = dalloc(s, N);
+    ISW_CUDA(cudaMemcpy(Gc, gc.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+    d.Gc = Gc;
+    d.B = dalloc(s, (size_t)L * N); d.q = dalloc(s, (size_t)L * NV); d.Tp = dalloc(s, (size_t)L * E);
+    d.F = dalloc(s, (size_t)L * E); d.scale = dalloc(s, (size_t)L * N);
+    d.G = dalloc(s, E); d.He = dalloc(s, E); d.ubs = dalloc(s, E); d.ub0 = dalloc(s, E); d.ub = dalloc(s, E); d.acc = dalloc(s, E);
+    d.eta0 = dalloc(s, N); d.eta = dalloc(s, N); d.eta_prev = dalloc(s, N);
+    d.h1 = dalloc(s, (size_t)L * N); d.h2 = dalloc(s, (size_t)L * N); d.u1 = dalloc(s, (size_t)L * E); d.u2 = dalloc(s, (size_t)L * E);
+    d.D1 = dalloc(s, (size_t)L * N); d.Z1 = dalloc(s, (size_t)L * NV); d.L1 = dalloc(s, (size_t)L * E); d.L2 = dalloc(s, (size_t)L * E);
+    d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
+    s->colmax_blocks = blocks_for(N) < 1024 ? blocks_for(N) : 1024;
+    d.red = dalloc(s, s->colmax_blocks + 1);
+    void *nf = nullptr;
+    ISW_CUDA(cudaMalloc(&nf, sizeof(int)));
+    s->allocs.push_back(nf);
+    s->nonfinite = (int *)nf;
+    ISW_CUDA(cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking));
+  } catch (...) {
+    for (void *q : s->allocs) cudaFree(q);
+    delete s;
+    throw;
+  }
+  return s;
+}
+
+void layers_destroy(isw_layers *s) {
+  cudaSetDevice(s->grid->device);
+  for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);
+  if (s->cap) cudaStreamDestroy(s->cap);
+  for (void *p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+void layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
+  if (!h || !u) fail(ISW_EINVAL, "layers.step: null h or u");
+  if (nfast < 1) fail(ISW_EINVAL, "layers.step: nfast must be >= 1");
+  if (!(dt > 0) || !std::isfinite(dt)) fail(ISW_EINVAL, "layers.step: dt must be positive and finite");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  ISW_CUDA(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {   // the caller is capturing a graph of its own: just queue the kernels
+    enqueue_step(s, h, u, Fm, dt, nfast, st);
+    return;
+  }
+  for (auto it = s->graphs.begin(); it != s->graphs.end(); ++it)
+    if (it->h == h && it->u == u && it->Fm == Fm && it->dt == dt && it->nfast == nfast) {
+      s->graphs.splice(s->graphs.begin(), s->graphs, it);
+      ISW_CUDA(cudaGraphLaunch(it->exec, st));
+      return;
+    }
+  cudaGraph_t graph = nullptr;
+  ISW_CUDA(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_step(s, h, u, Fm, dt, nfast, s->cap);
+  } catch (...) {
+    cudaStreamEndCapture(s->cap, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  ISW_CUDA(cudaStreamEndCapture(s->cap, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  ISW_CUDA(ie);
+  s->graphs.push_front(GraphEntry{h, u, Fm, dt, nfast, exec});
+  if (s->graphs.size() > GRAPH_CACHE) {
+    cudaGraphExecDestroy(s->graphs.back().exec);
+    s->graphs.pop_back();
+  }
+  ISW_CUDA(cudaGraphLaunch(exec, st));
+}
+
+int layers_substeps(isw_layers *s, const double *h, double dt, cudaStream_t st) {
+  if (!h) fail(ISW_EINVAL, "layers.substeps: null h");
+  ISW_CUDA(cudaMemsetAsync(s->nonfinite, 0, sizeof(int), st));
+  k_colmax<<<s->colmax_blocks, THREADS, 0, st>>>(s->d, h, s->d.red, s->nonfinite);
+  k_max_reduce<<<1, THREADS, 0, st>>>(s->d.red, s->colmax_blocks, s->d.red + s->colmax_blocks);
+  ISW_CUDA(cudaGetLastError());
+  double c2 = 0;
+  int nf = 0;
+  ISW_CUDA(cudaMemcpyAsync(&c2, s->d.red + s->colmax_blocks, sizeof(double), cudaMemcpyDeviceToHost, st));
+  ISW_CUDA(cudaMemcpyAsync(&nf, s->nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ISW_CUDA(cudaStreamSynchronize(st));
+  if (nf) fail(ISW_ENOTFINITE, "layers.substeps: non-finite column thickness");
+  const double n = std::ceil(dt * std::sqrt(c2) / (0.5 * s->grid->dmin));
+  return n > 1 ? (int)n : 1;
+}
+
+void layers_lap(isw_layers *s, const double *u, double *out, cudaStream_t st) {
+  if (!u || !out) fail(ISW_EINVAL, "layers.lap: null array");
+  const LayersDev &M = s->d;
+  ISW_DISPATCH_L(M.L, (k_lap_cv<LL><<<blocks_for(M.g.N + M.g.NV), THREADS, 0, st>>>(M, u)));
+  ISW_DISPATCH_L(M.L, (k_lap_e<LL><<<blocks_for(M.g.E), THREADS, 0, st>>>(M, out)));
+  ISW_CUDA(cudaGetLastError());
+}
+
+template <class F>
+int guarded(F f) {
+  try {
+    f();
+    return ISW_OK;
+  } catch (const Error &e) {
+    set_last_error(e.msg);
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return ISW_ENOMEM;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int isw_layers_create(isw_grid *g, const isw_layers_params *p, isw_layers **out) {
+  return guarded([&] {
+    if (!out) fail(ISW_EINVAL, "layers: null output handle");
+    *out = layers_create(g, p);
+  });
+}
+
+int isw_layers_destroy(isw_layers *s) {
+  if (s) layers_destroy(s);
+  return ISW_OK;
+}
+
+int isw_layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.step: null handle");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    layers_step(s, h, u, Fm, dt, nfast, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_substeps(isw_layers *s, const double *h, double dt, int *out, void *stream) {
+  return guarded([&] {
+    if (!s || !out) fail(ISW_EINVAL, "layers.substeps: null handle or output");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    *out = layers_substeps(s, h, dt, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_lap(isw_layers *s, const double *u, double *out, void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.lap: null handle");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    layers_lap(s, u, out, (cudaStream_t)stream);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,377 @@
+// Phase functions of the time-split RK3 step, plain FP64 form: one call per cell, edge or vertex, every layer of the
+// column in one thread. The arithmetic of each phase is the reference kernel's, operation for operation and in the
+// same summation order (compiled with -fmad=false), so results are bit-identical to the reference's FP64 path.
+//
+// Phase plan of one step (reference layers.py:185-212 with _stage :129-183, Boussinesq branch):
+//   init     cells: eta0 = b + sum h (layers.cu:33-38)          edges: ubar0 (layers.cu:64-74)
+//   lap x2   cells+vertices: D, zeta (trisk.cu:14-37)          edges: dD/dn - dzeta/dt (trisk.cu:39-45)
+//   per stage c = 1/3, 1/2, 1:
+//     A      cells: B_k (layers.cu:83-109), eta = eta0          vertices: q_k (fused.cu:82-98)
+//     E      edges: h_e, packed (h_e, u, q_e) (layers.cu:254-263), ubar = ubar0, acc = 0
+//     S      edges: slow tendency (layers.cu:269-359)
+//     n x    cells: eta step (layers.cu:366-377)   then   edges: ubar step (layers.cu:379-388)
+//     C      cells: layer fluxes F (layers.cu:392-397, recomputed here per cell edge; the edge's eI cell stores it)
+//                   and the floor limiter's scale (layers.cu:401-416)
+//     D      cells: h_n with the limited flux (layers.cu:418-441)   edges: Fm, u_n (layers.cu:418-426, :443-447)
+//   vmix     edges: interfacial stress (layers.cu:575-593)
+#pragma once
+#include "common.cuh"
+
+namespace isw {
+namespace fp64 {
+
+__device__ __forceinline__ double edge_h(double a, double b) { return 0.5 * (a + b); }
+
+// ---- init ----
+template <int L>
+__device__ __forceinline__ void eta0_cell(const LayersDev &M, const double *__restrict__ h, int i) {
+  const int N = M.g.N;
+  double z = M.b[i];
+#pragma unroll
+  for (int k = L - 1; k >= 0; k--) z += h[(size_t)k * N + i];
+  M.eta0[i] = z;
+}
+
+template <int L>
+__device__ __forceinline__ void ubar0_edge(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int e) {
+  const int N = M.g.N, E = M.g.E;
+  const int a = M.g.eI[e], b = M.g.eJ[e];
+  double H = 0, U = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double he = edge_h(h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    H += he;
+    U += he * u[(size_t)k * E + e];
+  }
+  M.ub0[e] = U / H;
+}
+
+// ---- vector Laplacian ----
+template <int L>
+__device__ __forceinline__ void div_cell(const LayersDev &M, const double *__restrict__ u, int i) {
+  const GridDev &g = M.g;
+  int es[6];
+  double c[6];
+  int m = 0;
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdge[i * 6 + s];
+    es[s] = e;
+    if (e >= 0) { c[s] = (double)g.cellSign[i * 6 + s] * g.le[e]; m = s + 1; }
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double *ul = u + (size_t)k * g.E;
+    double s = 0;
+    for (int t = 0; t < m; t++) s += c[t] * ul[es[t]];
+    M.D1[(size_t)k * g.N + i] = s / A;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void curl_vertex(const LayersDev &M, const double *__restrict__ u, int v) {
+  const GridDev &g = M.g;
+  int es[3];
+  double c[3];
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const int e = g.vEdge[v * 3 + s];
+    es[s] = e;
+    c[s] = (double)g.vEdgeSign[v * 3 + s] * g.de[e];
+  }
+  const double A = g.areaV[v];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double *ul = u + (size_t)k * g.E;
+    double z = 0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) z += c[s] * ul[es[s]];
+    M.Z1[(size_t)k * g.NV + v] = z / A;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void lap_edge(const LayersDev &M, double *__restrict__ out, int e) {
+  const GridDev &g = M.g;
+  const int a = g.eI[e], b = g.eJ[e], v1 = g.ev1[e], v2 = g.ev2[e];
+  const double de = g.de[e], le = g.le[e];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double *Dl = M.D1 + (size_t)k * g.N;
+    const double *Zl = M.Z1 + (size_t)k * g.NV;
+    out[(size_t)k * g.E + e] = (Dl[b] - Dl[a]) / de - (Zl[v2] - Zl[v1]) / le;
+  }
+}
+
+// ---- stage phase A ----
+template <int L>
+__device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double z[L];
+  double s = M.b[i];
+#pragma unroll
+  for (int k = L - 1; k >= 0; k--) { s += h[(size_t)k * N + i]; z[k] = s; }
+  int es[6];
+  double c[6];
+  int m = 0;
+#pragma unroll
+  for (int t = 0; t < 6; t++) {
+    const int e = g.cellEdge[i * 6 + t];
+    es[t] = e;
+    if (e >= 0) { c[t] = g.le[e] * g.de[e] * 0.25; m = t + 1; }
+  }
+  const double A = g.areaCell[i];
+  double Mp = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    if (k > 0) Mp += M.gp[k - 1] * z[k];
+    const double *ul = u + (size_t)k * E;
+    double ke = 0;
+    for (int t = 0; t < m; t++) {
+      const double ue = ul[es[t]];
+      ke += c[t] * ue * ue;
+    }
+    M.B[(size_t)k * N + i] = Mp + ke / A;
+  }
+  M.eta[i] = M.eta0[i];
+}
+
+template <int L>
+__device__ __forceinline__ void pv_vertex(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int v) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E, NV = g.NV;
+  int cs[3], es[3];
+  double kw[3], c[3];
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const int cc = g.vCell[v * 3 + s];
+    cs[s] = cc;
+    kw[s] = g.kite[cc * 6 + g.vSlot[v * 3 + s]];
+    const int e = g.vEdge[v * 3 + s];
+    es[s] = e;
+    c[s] = (double)g.vEdgeSign[v * 3 + s] * g.de[e];
+  }
+  const double Av = g.areaV[v], f = M.fV[v];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double *hl = h + (size_t)k * N;
+    const double *ul = u + (size_t)k * E;
+    double hv = 0, z = 0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) hv += kw[s] * hl[cs[s]] * 1.0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) z += c[s] * ul[es[s]];
+    M.q[(size_t)k * NV + v] = (z / Av + f) / (hv / Av);
+  }
+}
+
+// ---- stage phase E ----
+template <int L>
+__device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E, NV = g.NV;
+  const int a = g.eI[e], b = g.eJ[e], v1 = g.ev1[e], v2 = g.ev2[e];
+  double *pp = M.pk + (size_t)e * L * 3;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const size_t o = (size_t)k * E + e;
+    const double hv = edge_h(h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    const double qv = 0.5 * (M.q[(size_t)k * NV + v1] + M.q[(size_t)k * NV + v2]);
+    M.hedge[o] = hv;
+    pp[k * 3 + 0] = hv;
+    pp[k * 3 + 1] = u[o];
+    pp[k * 3 + 2] = qv;
+  }
+  M.ub[e] = M.ub0[e];
+  M.acc[e] = 0.0;
+}
+
+// ---- stage phase S: slow tendencies ----
+template <int L>
+__device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__restrict__ u, double dts, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double he[L], cap[L], qf[L], Q[L];
+  const double *pe = M.pk + (size_t)e * L * 3;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    he[k] = M.hedge[(size_t)k * E + e];
+    cap[k] = M.thin * he[k];
+    qf[k] = pe[k * 3 + 2];
+    Q[k] = 0;
+  }
+  const int m0 = g.eoeStart[e], m1 = g.eoeStart[e + 1];
+  for (int m = m0; m < m1; m++) {
+    const double wm = g.w[m];
+    const double *pp = M.pk + (size_t)g.eoe[m] * L * 3;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      double h2 = pp[k * 3 + 0];
+      if (h2 > cap[k]) h2 = cap[k];
+      const double F2 = h2 * pp[k * 3 + 1];
+      Q[k] += wm * F2 * 0.5 * (qf[k] + pp[k * 3 + 2]);
+    }
+  }
+  const int a = g.eI[e], b = g.eJ[e];
+  const double de = g.de[e];
+  double T[L];
+  double H = 0, U = 0, GT = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double ue = u[(size_t)k * E + e];
+    const double *Bl = M.B + (size_t)k * N;
+    // shelf off: sq = 1, so the force is -(B_J - B_I) / d and the squeezed-layer drag term is (1 - 1) / 21600 = 0
+    const double sq = 1.0;
+    double d = Q[k] - (sq * (Bl[b] - Bl[a])) / de - (M.drag[k] + (1 - sq) / 21600.0) * ue;
+    const double ck = M.stress[k];
+    if (ck != 0) {
+      const double r = ck / (he[k] > M.floor_ ? he[k] : M.floor_);
+      d = d - ((r * dts > 1e-8) ? (1 - exp(-r * dts)) / dts : r) * ue;
+    }
+    if (M.nu4 != 0) d = d - M.nu4 * M.L2[(size_t)k * E + e];
+    T[k] = d;
+    H += he[k];
+    U += he[k] * ue;
+  }
+#pragma unroll
+  for (int k = 0; k < L; k++) GT += he[k] * T[k];
+  const double gm = GT / H;
+#pragma unroll
+  for (int k = 0; k < L; k++) M.Tp[(size_t)k * E + e] = T[k] - gm;
+  M.G[e] = gm;
+  M.He[e] = H;
+  M.ubs[e] = U / H;
+}
+
+// ---- fast mode ----
+__device__ __forceinline__ void bt_eta_cell(const LayersDev &M, double tau, int i) {
+  const GridDev &g = M.g;
+  const double e0 = M.eta[i];
+  M.eta_prev[i] = e0;
+  double div = 0;
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdge[i * 6 + s];
+    if (e < 0) break;
+    div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
+  }
+  M.eta[i] = e0 - (tau * div) / g.areaCell[i];
+}
+
+__device__ __forceinline__ void bt_u_edge(const LayersDev &M, double tau, int e) {
+  const GridDev &g = M.g;
+  const double v = M.ub[e];
+  M.acc[e] += v;
+  const int i = g.eI[e], j = g.eJ[e];
+  const double gam = M.div_damp;
+  const double ej = M.Gc[j] * (M.eta[j] + gam * (M.eta[j] - M.eta_prev[j]));
+  const double ei = M.Gc[i] * (M.eta[i] + gam * (M.eta[i] - M.eta_prev[i]));
+  M.ub[e] = v + tau * ((-(ej - ei)) / g.de[e] + M.G[e]);
+}
+
+// ---- stage phase C: layer fluxes and the floor limiter's scale ----
+template <int L>
+__device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double out[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) out[k] = 0;
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdgeAsc[i * 6 + s];
+    if (e < 0) break;
+    const int ea = g.eI[e], eb = g.eJ[e];
+    const bool mine = ea == i;
+    const double ubs = M.ubs[e], acc = M.acc[e], le = g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const double he = edge_h(a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
+      const double F = he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
+      if (mine) M.F[(size_t)k * E + e] = F;
+      const double f = F * le * a.cdt;
+      if (mine) { if (f > 0) out[k] += f; }
+      else if (!(f > 0)) out[k] -= f;
+    }
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double avail = a.h0[(size_t)k * N + i] - M.floor_;
+    const double cap = (avail > 0 ? avail : 0.0) * A;
+    M.scale[(size_t)k * N + i] = out[k] > cap ? cap / out[k] : 1.0;
+  }
+}
+
+// ---- stage phase D ----
+__device__ __forceinline__ double limited(const LayersDev &M, int k, int e) {
+  const GridDev &g = M.g;
+  double f = M.F[(size_t)k * g.E + e];
+  f *= f > 0 ? M.scale[(size_t)k * g.N + g.eI[e]] : M.scale[(size_t)k * g.N + g.eJ[e]];
+  return f;
+}
+
+template <int L>
+__device__ __forceinline__ void h_cell(const LayersDev &M, const StageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N;
+  double div[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) div[k] = 0;
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdge[i * 6 + s];
+    if (e < 0) break;
+    const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) div[k] += c * limited(M, k, e);
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const size_t o = (size_t)k * N + i;
+    a.hn[o] = a.h0[o] - (a.cdt * div[k]) / A;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void u_edge(const LayersDev &M, const StageArgs &a, int e) {
+  const GridDev &g = M.g;
+  const int E = g.E;
+  const double dub = M.ub[e] - M.ub0[e];
+  const double le = g.le[e];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const size_t o = (size_t)k * E + e;
+    if (a.Fm) a.Fm[o] = limited(M, k, e) * le * a.dt;
+    a.un[o] = a.u0[o] + a.cdt * M.Tp[o] + dub;
+  }
+}
+
+// ---- after the stages: interfacial stress ----
+template <int L>
+__device__ __forceinline__ void vmix_edge(const LayersDev &M, const double *__restrict__ h, double *__restrict__ u, double dt, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  const int ia = g.eI[e], ib = g.eJ[e];
+  const double c = M.vmix, cd = M.vmix_cd;
+  double d = 0;
+#pragma unroll
+  for (int k = 0; k + 1 < L; k++) {
+    const double ha = 0.5 * (h[(size_t)k * N + ia] + h[(size_t)k * N + ib]);
+    const double hb = 0.5 * (h[(size_t)(k + 1) * N + ia] + h[(size_t)(k + 1) * N + ib]);
+    double *ua = u + (size_t)k * E + e;
+    double *ub = u + (size_t)(k + 1) * E + e;
+    const double mean = (ha * *ua + hb * *ub) / (ha + hb);
+    const double du0 = *ua - *ub;
+    double du1 = du0 * exp(-c * (1 / ha + 1 / hb) * dt);
+    if (cd > 0) du1 = du1 / (1 + cd * fabs(du0) * (1 / ha + 1 / hb) * dt);
+    *ua = mean + hb / (ha + hb) * du1;
+    *ub = mean - ha / (ha + hb) * du1;
+    d += 0.5 * ha * hb / (ha + hb) * (du0 * du0 - du1 * du1);
+  }
+  M.diss[e] = d;
+}
+
+}  // namespace fp64
+}  // namespace isw

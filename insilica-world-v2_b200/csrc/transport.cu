@@ -1,0 +1,298 @@
+// Flux-corrected tracer transport (reference src/insilica/transport.py:18-71 with kernels/fused.cu:122-241 and
+// kernels/trisk.cu:48-59), plain FP64 form, and the Transport part of the C ABI.
+//
+// Rows y = tracer j * L + layer l, as the reference stacks them; row y's tracer values live in the caller's own array
+// tracers[j] + l * N (no packed copy). The reference's 8 launches per call (td, 2 x (hflux, stage), aflux, ratios,
+// apply) become 4 cell passes: every 3rd-order edge flux is recomputed by the cell pass that sums it, with the
+// reference's arithmetic, so results are bit-identical:
+//   P1  td (fused.cu:146-160) and the first RK stage p1 (fused.cu:163-186, frac 1/3, fluxes of psi)
+//   P2  the second RK stage p2 (frac 1/2, fluxes of p1)
+//   P3  antidiffusive fluxes A (fused.cu:189-194; stored by each edge's eI cell) and the Zalesak ratios (fused.cu:197-222)
+//   P4  the limited update (fused.cu:225-241), written into the caller's tracer arrays
+// Order 1 stops after td, which is copied out (the reference returns td).
+#include <cstring>
+
+#include "common.cuh"
+
+namespace isw {
+namespace {
+
+struct TrArgs {
+  const double *M0, *M1, *Fm;
+  double *tr[TRMAX];              // the caller's tracer arrays
+  int L, rows;
+  double beta;
+};
+
+struct TransportDev {
+  GridDev g;
+  double *psi0, *td, *p1, *p2, *A, *Rp, *Rm;   // rows x N (A rows x E); psi0 holds the tracers as they came in
+};
+
+__device__ __forceinline__ double upwind(const double *__restrict__ Fml, const double *__restrict__ p, const int *eI, const int *eJ,
+                                         int e) {
+  const double f = Fml[e];
+  return f * (f >= 0 ? p[eI[e]] : p[eJ[e]]);
+}
+
+// reference fused.cu:131-138, FP64 form
+__device__ __forceinline__ double hoflux(const GridDev &g, const double *__restrict__ Fml, const double *__restrict__ ps, int e,
+                                         double beta) {
+  const double f = Fml[e];
+  const int o = e * 8;
+  const int *idx = g.d2idx;
+  const double *wt = g.d2wt;
+  const double a = wt[o] * ps[idx[o]] + wt[o + 1] * ps[idx[o + 1]] + wt[o + 2] * ps[idx[o + 2]] + wt[o + 3] * ps[idx[o + 3]];
+  const double b = wt[o + 4] * ps[idx[o + 4]] + wt[o + 5] * ps[idx[o + 5]] + wt[o + 6] * ps[idx[o + 6]] + wt[o + 7] * ps[idx[o + 7]];
+  return f * (0.5 * (ps[g.eI[e]] + ps[g.eJ[e]]) - (a + b)) + fabs(f) * ((b - a) * beta);
+}
+
+// reference trisk.cu:48-59
+__global__ void __launch_bounds__(THREADS) k_mass(const GridDev g, int L, const double *__restrict__ M0, const double *__restrict__ Fm,
+                                                  double *__restrict__ M1) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.N * L) return;
+  const int l = t / g.N, i = t - l * g.N;
+  const size_t o = (size_t)l * g.N + i;
+  const double *f = Fm + (size_t)l * g.E;
+  double m = M0[o];
+  for (int k = 0; k < 6; k++) {
+    const int e = g.cellEdgeAsc[i * 6 + k];
+    if (e < 0) break;
+    if (g.eI[e] == i) m -= f[e]; else m += f[e];
+  }
+  M1[o] = m;
+}
+
+// P1: copy psi in, td, and p1 (frac 1/3 from psi)
+__global__ void __launch_bounds__(THREADS) k_p1(const TransportDev T, const TrArgs a, int order) {
+  const GridDev &g = T.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.N * a.rows) return;
+  const int y = t / g.N, i = t - y * g.N, l = y % a.L, j = y / a.L;
+  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
+  const double *p = a.tr[j] + (size_t)l * g.N;
+  const double *Fml = a.Fm + (size_t)l * g.E;
+  const double pi = p[i];
+  T.psi0[o] = pi;
+  double td = a.M0[om] * pi;
+  double s = a.M0[om] * pi, mx = a.M0[om];
+  const double frac = 1.0 / 3.0;
+  for (int k = 0; k < 6; k++) {
+    const int e = g.cellEdgeAsc[i * 6 + k];
+    if (e < 0) break;
+    const bool out = g.eI[e] == i;
+    const double fu = upwind(Fml, p, g.eI, g.eJ, e);
+    if (out) td -= fu; else td += fu;
+    if (order != 1) {
+      const double f = frac * hoflux(g, Fml, p, e, a.beta);
+      const double m = frac * Fml[e];
+      if (out) { s -= f; mx -= m; } else { s += f; mx += m; }
+    }
+  }
+  T.td[o] = td / a.M1[om];
+  if (order != 1) T.p1[o] = s / mx;
+}
+
+// P2: p2 (frac 1/2 from p1)
+__global__ void __launch_bounds__(THREADS) k_p2(const TransportDev T, const TrArgs a) {
+  const GridDev &g = T.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.N * a.rows) return;
+  const int y = t / g.N, i = t - y * g.N, l = y % a.L;
+  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
+  const double *p1 = T.p1 + (size_t)y * g.N;
+  const double *Fml = a.Fm + (size_t)l * g.E;
+  const double frac = 1.0 / 2.0;
+  double s = a.M0[om] * T.psi0[o], mx = a.M0[om];
+  for (int k = 0; k < 6; k++) {
+    const int e = g.cellEdgeAsc[i * 6 + k];
+    if (e < 0) break;
+    const double f = frac * hoflux(g, Fml, p1, e, a.beta);
+    const double m = frac * Fml[e];
+    if (g.eI[e] == i) { s -= f; mx -= m; } else { s += f; mx += m; }
+  }
+  T.p2[o] = s / mx;
+}
+
+// P3: antidiffusive fluxes and Zalesak ratios
+__global__ void __launch_bounds__(THREADS) k_p3(const TransportDev T, const TrArgs a) {
+  const GridDev &g = T.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.N * a.rows) return;
+  const int y = t / g.N, i = t - y * g.N, l = y % a.L;
+  const double *p = T.psi0 + (size_t)y * g.N;
+  const double *tt = T.td + (size_t)y * g.N;
+  const double *p2 = T.p2 + (size_t)y * g.N;
+  const double *Fml = a.Fm + (size_t)l * g.E;
+  double hi = fmax(p[i], tt[i]), lo = fmin(p[i], tt[i]);
+  for (int k = 0; k < 6; k++) {
+    const int j = g.nbr[i * 6 + k];
+    if (j < 0) break;
+    hi = fmax(hi, fmax(p[j], tt[j]));
+    lo = fmin(lo, fmin(p[j], tt[j]));
+  }
+  const double m1 = a.M1[(size_t)l * g.N + i];
+  const double qmax = (hi - tt[i]) * m1, qmin = (tt[i] - lo) * m1;
+  double Pp = 0, Pm = 0;
+  for (int k = 0; k < 6; k++) {
+    const int e = g.cellEdgeAsc[i * 6 + k];
+    if (e < 0) break;
+    const double A = hoflux(g, Fml, p2, e, a.beta) - upwind(Fml, p, g.eI, g.eJ, e);
+    if (g.eI[e] == i) {
+      T.A[(size_t)y * g.E + e] = A;
+      if (A > 0) Pm += A; else Pp -= A;
+    } else {
+      if (A > 0) Pp += A; else Pm -= A;
+    }
+  }
+  T.Rp[(size_t)y * g.N + i] = Pp > 0 ? fmin(1.0, qmax / Pp) : 0.0;
+  T.Rm[(size_t)y * g.N + i] = Pm > 0 ? fmin(1.0, qmin / Pm) : 0.0;
+}
+
+// P4: the limited update into the caller's tracer arrays
+__global__ void __launch_bounds__(THREADS) k_p4(const TransportDev T, const TrArgs a) {
+  const GridDev &g = T.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.N * a.rows) return;
+  const int y = t / g.N, i = t - y * g.N, l = y % a.L, j = y / a.L;
+  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
+  const double *Al = T.A + (size_t)y * g.E;
+  const double *rp = T.Rp + (size_t)y * g.N;
+  const double *rm = T.Rm + (size_t)y * g.N;
+  const double m1 = a.M1[om];
+  double s = T.td[o] * m1;
+  for (int k = 0; k < 6; k++) {
+    const int e = g.cellEdgeAsc[i * 6 + k];
+    if (e < 0) break;
+    const double A = Al[e];
+    const int ea = g.eI[e], eb = g.eJ[e];
+    const double c = A > 0 ? fmin(rp[eb], rm[ea]) : fmin(rp[ea], rm[eb]);
+    if (ea == i) s -= c * A; else s += c * A;
+  }
+  a.tr[j][(size_t)l * g.N + i] = s / m1;
+}
+
+// order 1: td out
+__global__ void __launch_bounds__(THREADS) k_td_out(const TransportDev T, const TrArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T.g.N * a.rows) return;
+  const int y = t / T.g.N, i = t - y * T.g.N, l = y % a.L, j = y / a.L;
+  a.tr[j][(size_t)l * T.g.N + i] = T.td[(size_t)y * T.g.N + i];
+}
+
+}  // namespace
+}  // namespace isw
+
+using namespace isw;
+
+struct isw_transport {
+  isw_grid *grid;
+  TransportDev d;
+  int L, T, precision;
+  double beta;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+template <class F>
+int guarded(F f) {
+  try {
+    f();
+    return ISW_OK;
+  } catch (const Error &e) {
+    set_last_error(e.msg);
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return ISW_ENOMEM;
+  }
+}
+
+double *talloc(isw_transport *t, size_t n) {
+  void *p = nullptr;
+  ISW_CUDA(cudaMalloc(&p, sizeof(double) * (n ? n : 1)));
+  t->allocs.push_back(p);
+  ISW_CUDA(cudaMemset(p, 0, sizeof(double) * (n ? n : 1)));
+  return (double *)p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int precision, isw_transport **out) {
+  return guarded([&] {
+    if (!g || !out) fail(ISW_EINVAL, "transport: null grid or output handle");
+    if (L < 1 || L > LMAX) fail(ISW_EINVAL, "transport: L must be in 1..8");
+    if (tracers < 1 || tracers > TRMAX) fail(ISW_EINVAL, "transport: tracers must be in 1..16");
+    if (precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "transport: the mixed form is not built yet");
+    ISW_CUDA(cudaSetDevice(g->device));
+    isw_transport *t = new isw_transport();
+    t->grid = g;
+    t->L = L;
+    t->T = tracers;
+    t->precision = precision;
+    t->beta = beta;
+    try {
+      const size_t R = (size_t)L * tracers, N = g->d.N, E = g->d.E;
+      t->d.g = g->d;
+      t->d.psi0 = talloc(t, R * N); t->d.td = talloc(t, R * N); t->d.p1 = talloc(t, R * N); t->d.p2 = talloc(t, R * N);
+      t->d.Rp = talloc(t, R * N); t->d.Rm = talloc(t, R * N); t->d.A = talloc(t, R * E);
+    } catch (...) {
+      for (void *p : t->allocs) cudaFree(p);
+      delete t;
+      throw;
+    }
+    *out = t;
+  });
+}
+
+int isw_transport_destroy(isw_transport *t) {
+  if (!t) return ISW_OK;
+  cudaSetDevice(t->grid->device);
+  for (void *p : t->allocs) cudaFree(p);
+  delete t;
+  return ISW_OK;
+}
+
+int isw_transport_mass_after(isw_transport *t, const double *M0, const double *Fm, double *M1, void *stream) {
+  return guarded([&] {
+    if (!t || !M0 || !Fm || !M1) fail(ISW_EINVAL, "transport.mass_after: null argument");
+    ISW_CUDA(cudaSetDevice(t->grid->device));
+    const GridDev &g = t->d.g;
+    k_mass<<<blocks_for((long long)g.N * t->L), THREADS, 0, (cudaStream_t)stream>>>(g, t->L, M0, Fm, M1);
+    ISW_CUDA(cudaGetLastError());
+  });
+}
+
+int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1, const double *Fm, double *const *tracers, int ntr,
+                            int order, void *stream) {
+  return guarded([&] {
+    if (!t || !M0 || !M1 || !Fm || !tracers) fail(ISW_EINVAL, "transport.step_many: null argument");
+    if (ntr < 1 || ntr > t->T) fail(ISW_EINVAL, "transport.step_many: more tracers than the transport was built for");
+    if (order != 1 && order != 3) fail(ISW_EINVAL, "transport.step_many: order must be 1 or 3");
+    ISW_CUDA(cudaSetDevice(t->grid->device));
+    TrArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.M0 = M0; a.M1 = M1; a.Fm = Fm; a.L = t->L; a.rows = ntr * t->L; a.beta = t->beta;
+    for (int j = 0; j < ntr; j++) {
+      if (!tracers[j]) fail(ISW_EINVAL, "transport.step_many: null tracer");
+      a.tr[j] = tracers[j];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nb = blocks_for((long long)t->d.g.N * a.rows);
+    k_p1<<<nb, THREADS, 0, st>>>(t->d, a, order);
+    if (order == 1) {
+      k_td_out<<<nb, THREADS, 0, st>>>(t->d, a);
+    } else {
+      k_p2<<<nb, THREADS, 0, st>>>(t->d, a);
+      k_p3<<<nb, THREADS, 0, st>>>(t->d, a);
+      k_p4<<<nb, THREADS, 0, st>>>(t->d, a);
+    }
+    ISW_CUDA(cudaGetLastError());
+  });
+}
+
+}  // extern "C"

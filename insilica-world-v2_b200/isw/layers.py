@@ -1,0 +1,140 @@
+"""Stacked-layer shallow water with a split-explicit fast mode, on the isw CUDA core (reference src/insilica/layers.py).
+
+``Layers`` keeps the reference's constructor and methods (``step``, ``substeps``, ``lap_max``, ``energy``) and argument
+meanings; the arrays are the caller's device arrays (h (L, N), u (L, E), Fm (L, E), FP64), updated in place on the
+current CUDA stream. Options of the reference that this core does not implement raise ``NotImplementedError`` at
+construction (air layers, walls, the shelf, the squeezed-layer bed, per-cell buoyancy, tides, the bottom drag law) or
+at the call (``exchange``).
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .gpu import DeviceGrid, device_ptr, dsum, stream_of
+
+LMAX = 8
+FAST_COURANT = 0.5          # fast sub-step: tau sqrt(gH) / d_min <= this (reference layers.py:31)
+DIV_DAMP = 0.1              # divergence damping of the fast mode (reference layers.py:32)
+GRAV = 9.80616
+
+
+class Layers:
+    def __init__(self, dg, layers=1, b=None, grav=GRAV, gprime=(), drag=0.0, stress=0.0, nu4=0.0, floor=1.0, rotation=1.0,
+                 div_damp=DIV_DAMP, air=None, vmix=0.0, thin=2.0, wall=None, thin_wind=0.0, shelf=0.0, vmix_cd=0.0,
+                 shelf_bed=False):
+        if air:
+            raise NotImplementedError('Layers: air layers (the theta branch) are not implemented by this core')
+        if wall is not None:
+            raise NotImplementedError('Layers: thin walls are not implemented by this core')
+        if shelf:
+            raise NotImplementedError('Layers: the shelf option is not implemented by this core')
+        if shelf_bed:
+            raise NotImplementedError('Layers: shelf_bed is not implemented by this core')
+        if thin_wind:
+            raise NotImplementedError('Layers: thin_wind (air exchange) is not implemented by this core')
+        assert 1 <= layers <= LMAX and len(gprime) == layers - 1
+        if not isinstance(dg, DeviceGrid):
+            raise TypeError('Layers: dg must be an isw DeviceGrid')
+        self.dg, self.L = dg, layers
+        self.grav, self.nu4, self.floor, self.div_damp, self.thin = grav, nu4, floor, div_damp, thin
+        self.vmix, self.vmix_cd = vmix, vmix_cd
+        self.air = None
+        self.shelf = 0.0
+        self.sig = self.zm = self.tide = None
+        self.cd_bot, self.cbot = 0.0, None
+        self.precision = _lib.ISW_MIXED if dg.mixed else _lib.ISW_FP64
+        self._b_host = np.zeros(dg.N) if b is None else np.ascontiguousarray(np.asarray(
+            b.detach().cpu().numpy() if isinstance(b, torch.Tensor) else b, dtype=np.float64))
+        self.b = torch.as_tensor(self._b_host, device=f'cuda:{dg.device}')
+        gp = np.ascontiguousarray(np.asarray(gprime, dtype=np.float64).reshape(-1)) if layers > 1 else np.zeros(1)
+        self._drag = np.ascontiguousarray(np.broadcast_to(np.asarray(drag, dtype=np.float64), (layers,)))
+        self._stress = np.ascontiguousarray(np.broadcast_to(np.asarray(stress, dtype=np.float64), (layers,)))
+        self.gp = gp
+        p = _lib.LayersParams(L=layers, grav=float(grav), gprime=_lib.host_ptr(gp), drag=_lib.host_ptr(self._drag),
+                              stress=_lib.host_ptr(self._stress), nu4=float(nu4), floor_=float(floor), rotation=float(rotation),
+                              div_damp=float(div_damp), thin=float(thin), vmix=float(vmix), vmix_cd=float(vmix_cd),
+                              b=_lib.host_ptr(self._b_host), precision=self.precision)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.isw_layers_create(dg.handle, ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.dmin = float(np.min(dg.host.de))
+        self._L1 = None
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        destroy = getattr(_lib, 'isw_layers_destroy', None) if _lib is not None else None
+        if h is not None and h.value and destroy is not None:      # (module globals are gone at interpreter exit)
+            destroy(h)
+            self._h = None
+
+    def _shapes(self):
+        return (self.L, self.dg.N), (self.L, self.dg.E)
+
+    def step(self, h, u, dt, nfast, Fm=None, theta=None, stream=None):
+        """One time-split RK3 step in place on h (L, N), u (L, E), with nfast fast sub-steps per full step (stage s takes
+        ceil(c_s nfast)). Fm, if given, receives each layer's final-stage volume flux l dt F (m^3)."""
+        if theta is not None:
+            raise NotImplementedError('Layers.step: theta (air layers) is not implemented by this core')
+        sh, su = self._shapes()
+        dev = self.dg.device
+        ph = device_ptr(h, shape=sh, name='h', device=dev)
+        pu = device_ptr(u, shape=su, name='u', device=dev)
+        pf = device_ptr(Fm, shape=su, name='Fm', device=dev)
+        _lib.check(_lib.isw_layers_step(self._h, ph, pu, pf, float(dt), int(nfast), stream_of(dev, stream)))
+
+    def substeps(self, h, dt, stream=None):
+        """Fast sub-steps per full step for the current deepest column (reference layers.py:99-102)."""
+        sh, _ = self._shapes()
+        out = ctypes.c_int()
+        _lib.check(_lib.isw_layers_substeps(self._h, device_ptr(h, shape=sh, name='h', device=self.dg.device), float(dt),
+                                            ctypes.byref(out), stream_of(self.dg.device, stream)))
+        return out.value
+
+    def lap(self, u, out, stream=None):
+        """out = the edge vector Laplacian of u (reference layers.py:123-127)."""
+        _, su = self._shapes()
+        dev = self.dg.device
+        _lib.check(_lib.isw_layers_lap(self._h, device_ptr(u, shape=su, name='u', device=dev),
+                                       device_ptr(out, shape=su, name='out', device=dev), stream_of(dev, stream)))
+
+    def lap_max(self, iters=30):
+        """Largest |eigenvalue| of the edge vector Laplacian by power iteration from a fixed seed, 1/m^2
+        (reference layers.py:111-121). Norms are deterministic tree sums."""
+        dev = f'cuda:{self.dg.device}'
+        v = torch.as_tensor(np.random.default_rng(0).standard_normal((self.L, self.dg.E)), device=dev)
+        out = torch.empty_like(v)
+        lam = 0.0
+        for _ in range(iters):
+            self.lap(v, out)
+            n1 = math.sqrt(dsum(out[0], out[0]))
+            lam = n1 / math.sqrt(dsum(v[0], v[0]))
+            v = out / n1
+            out = torch.empty_like(v)
+        return lam
+
+    def update_gfast(self, h, theta):
+        if self.air:
+            raise NotImplementedError('Layers.update_gfast: air layers are not implemented by this core')
+
+    def exchange(self, wx, h, u, M, psi, theta=None, seq=False):
+        raise NotImplementedError('Layers.exchange: the between-layer exchange hook is not implemented by this core')
+
+    def energy(self, h, u, theta=None):
+        """Total energy per unit density (J/rho0), Boussinesq form (reference layers.py:234-253), on the host."""
+        if theta is not None:
+            raise NotImplementedError('Layers.energy: air layers are not implemented by this core')
+        gh = self.dg.host
+        hh = h.detach().cpu().numpy() if isinstance(h, torch.Tensor) else np.asarray(h)
+        uu = u.detach().cpu().numpy() if isinstance(u, torch.Tensor) else np.asarray(u)
+        b = self._b_host
+        ce = np.where(gh.cellEdge >= 0, gh.cellEdge, 0)
+        ok = gh.cellEdge >= 0
+        kin = sum(np.sum(hh[k] * np.sum(np.where(ok, gh.le[ce] * gh.de[ce] * 0.25 * uu[k][ce] ** 2, 0.0), axis=1)) for k in range(self.L))
+        z = b + np.cumsum(hh[::-1], axis=0)[::-1]
+        pot = np.sum(gh.areaCell * self.grav * (z[0] ** 2 - b ** 2) / 2)
+        for k in range(1, self.L):
+            pot += np.sum(gh.areaCell * self.gp[k - 1] * (z[k] ** 2 - b ** 2) / 2)
+        return float(kin + pot)

@@ -1,0 +1,234 @@
+"""Parity of the CUDA core with the reference, through the C ABI (isw Python facade), on a B200.
+
+The golden vectors were produced by the reference's own Layers / Transport / dsum (tests/golden/make_golden.py). Runs
+without exp() in their arithmetic must match bit for bit; runs whose stress terms call exp() may differ from the host
+build in the last bit of exp, so they are held to 1e-12 relative (the FP64 bar) and are reported as bit-exact or not.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+@pytest.fixture(scope='module')
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    return torch.device('cuda:0')
+
+
+@pytest.fixture(scope='module')
+def isw(dev):
+    from isw import gpu, layers, transport
+    gpu.set_precision('double')
+    return gpu, layers, transport
+
+
+def T(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_w2_bit_exact(dev, isw, grid4):
+    """Config 1 (Williamson 2, n = 4, dt 900 s, nfast from the reference's rule): 1, 96 and 480 steps bit for bit."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('w2_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616))
+    core = layers.Layers(dg, 1, b=z['b'])
+    h, u = T(z['h0'], dev), T(z['u0'], dev)
+    assert core.substeps(h, float(z['dt'])) == int(z['substeps'])
+    for s in range(1, 481):
+        core.step(h, u, float(z['dt']), int(z['nfast']))
+        if s in (1, 96, 480):
+            torch.cuda.synchronize()
+            assert np.array_equal(h.cpu().numpy(), z[f'h{s}']), (s, rel(h.cpu().numpy(), z[f'h{s}']))
+            assert np.array_equal(u.cpu().numpy(), z[f'u{s}']), (s, rel(u.cpu().numpy(), z[f'u{s}']))
+    assert core.energy(h, u) == float(z['energy480'])
+
+
+def run_stack(isw, grid4, z, dev, steps):
+    from isw import grid as G
+    gpu, layers, transport = isw
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    L = int(z['L'])
+    core = layers.Layers(dg, L, b=z['b'], gprime=list(z['gprime']), stress=list(z['stress']), nu4=float(z['nu4']),
+                         floor=float(z['floor']), vmix=float(z['vmix']))
+    tr = transport.Transport(dg, layers=L, tracers=3)
+    h, u = T(z['h0'], dev), T(z['u0'], dev)
+    M = T(z['h0'] * grid4.areaCell[None], dev)
+    M1 = torch.zeros_like(M)
+    Fm = torch.zeros_like(u)
+    trc = [T(z[f'tr{k}_0'], dev) for k in range(3)]
+    for _ in range(steps):
+        core.step(h, u, float(z['dt']), int(z['nfast']), Fm)
+        tr.mass_after(M, Fm, M1)
+        tr.step_many(M, M1, Fm, trc, order=3)
+        M, M1 = M1, M
+    torch.cuda.synchronize()
+    return core, h, u, M, trc, Fm
+
+
+@pytest.mark.parametrize('case', ['air3_n4', 'ocean2_n4'])
+def test_stacks_golden(dev, isw, grid4, case, record_property):
+    """Stacked layers (nu4, stress, interfacial stress, 20 fast sub-steps, 3 FCT tracers), 6 steps: <= 1e-12 relative
+    to the reference in every field (bit-exact where no exp() is involved)."""
+    z = golden(case)
+    core, h, u, M, trc, Fm = run_stack(isw, grid4, z, dev, 6)
+    worst = 0.0
+    exact = True
+    for name, a in (('h', h), ('u', u), ('M', M), ('Fm', Fm)) + tuple((f'tr{k}', trc[k]) for k in range(3)):
+        a = a.cpu().numpy()
+        exact &= bool(np.array_equal(a, z[name]))
+        worst = max(worst, rel(a, z[name]))
+    record_property('bit_exact', exact)
+    record_property('worst_rel', worst)
+    assert worst <= REL, worst
+    assert abs(core.lap_max() - float(z['lap_max'])) <= 1e-10 * float(z['lap_max'])
+
+
+def test_outcrop_golden(dev, isw, grid4):
+    """The reference's outcrop case: floor limiter active, bottom stress, nu4, bell tracer, 24 steps; <= 1e-12."""
+    gpu, layers, transport = isw
+    z = golden('outcrop_n4')
+    dg = gpu.DeviceGrid(grid4)
+    core = layers.Layers(dg, 2, b=z['b'], gprime=[0.02], stress=[0.0, 2.5e-4], nu4=float(z['nu4']), floor=1.0)
+    tr = transport.Transport(dg, layers=2, tracers=4)
+    h, u, psi = T(z['h0'], dev), T(z['u0'], dev), T(z['psi0'], dev)
+    M = T(z['h0'] * grid4.areaCell[None], dev)
+    M1, Fm = torch.zeros_like(M), torch.zeros_like(u)
+    lo = float(h.min())
+    for _ in range(24):
+        core.step(h, u, float(z['dt']), int(z['nfast']), Fm)
+        tr.mass_after(M, Fm, M1)
+        tr.step_many(M, M1, Fm, [psi], order=3)
+        M, M1 = M1, M
+        lo = min(lo, float(h.min()))
+    for name, a in (('h', h), ('u', u), ('M', M), ('psi', psi), ('Fm', Fm)):
+        assert rel(a.cpu().numpy(), z[name]) <= REL, name
+    assert lo >= 1.0 - 1e-9
+
+
+def test_bell_bit_exact(dev, isw, grid4):
+    """Transport alone (cosine bell, solid-body flux), order 1 and 3, 20 steps: bit for bit."""
+    gpu, _, transport = isw
+    z = golden('bell_n4')
+    dg = gpu.DeviceGrid(grid4)
+    for order in (1, 3):
+        tr = transport.Transport(dg)
+        psi, M, M1, Fm = T(z['psi0'], dev), T(z['M0'], dev), torch.zeros(1, dg.N, dtype=torch.float64, device=dev), T(z['Fm'], dev)
+        for _ in range(20):
+            tr.mass_after(M, Fm, M1)
+            tr.step(M, M1, Fm, psi, order)
+            M, M1 = M1, M
+        assert np.array_equal(psi.cpu().numpy(), z[f'psi_o{order}']), order
+        assert np.array_equal(M.cpu().numpy(), z[f'M_o{order}']), order
+
+
+def test_dsum_bit_exact(dev, isw):
+    """The deterministic tree sum equals the reference's, for sizes from 1 to 2^20, with and without y."""
+    gpu = isw[0]
+    z = golden('dsum')
+    for n in (1, 2, 255, 2048, 2049, 100003, 1 << 20):
+        i = np.arange(n, dtype=np.int64)
+        x = ((i * 7919) % 10007 - 5003) / 997.0
+        y = ((i * 104729) % 65521) / 4093.0
+        assert gpu.dsum(T(x, dev)) == float(z[f'x_{n}'])
+        assert gpu.dsum(T(x, dev), T(y, dev)) == float(z[f'xy_{n}'])
+
+
+def test_graph_capture_equals_direct(dev, isw, grid4):
+    """A step queued inside the caller's own CUDA-graph capture and replayed equals direct steps, bit for bit
+    (reference REPRO: graph vs direct)."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('w2_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616))
+    a, b = layers.Layers(dg, 1, b=z['b']), layers.Layers(dg, 1, b=z['b'])
+    ha, ua = T(z['h0'], dev), T(z['u0'], dev)
+    hb, ub = ha.clone(), ua.clone()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b.step(hb, ub, 900.0, 2)            # first step direct (as World does), then capture
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            b.step(hb, ub, 900.0, 2)
+    torch.cuda.synchronize()
+    for _ in range(10):
+        g.replay()
+    for _ in range(11):                     # b: one direct step and ten replays
+        a.step(ha, ua, 900.0, 2)
+    torch.cuda.synchronize()
+    assert torch.equal(ha, hb) and torch.equal(ua, ub)
+
+
+def test_two_equal_layers_equal_one(dev, isw, grid4):
+    """A one-layer case split into two equal layers with g' = 0 moves exactly as one layer (reference REPRO, layers)."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('w2_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616))
+    one = layers.Layers(dg, 1, b=z['b'])
+    two = layers.Layers(dg, 2, b=z['b'], gprime=[0.0])
+    h1, u1 = T(z['h0'], dev), T(z['u0'], dev)
+    h2, u2 = T(np.repeat(z['h0'] / 2, 2, axis=0), dev), T(np.repeat(z['u0'], 2, axis=0), dev)
+    for _ in range(50):
+        one.step(h1, u1, 900.0, 2)
+        two.step(h2, u2, 900.0, 2)
+    torch.cuda.synchronize()
+    assert torch.equal(h2[0], h2[1]) and torch.equal(u2[0], u2[1])
+    assert torch.equal(2 * h2[0], h1[0]) and torch.equal(u2[0], u1[0])
+
+
+def test_stack_conservation(dev, isw, grid4):
+    """Per-layer volume and tracer mass are conserved to roundoff (reference CONSERVE bar 1e-13) over 6 steps."""
+    gpu = isw[0]
+    z = golden('air3_n4')
+    core, h, u, M, trc, Fm = run_stack(isw, grid4, z, dev, 6)
+    A = T(grid4.areaCell, dev)
+    M0 = T(z['h0'] * grid4.areaCell[None], dev)
+    for k in range(int(z['L'])):
+        v0, v1 = gpu.dsum(M0[k]), gpu.dsum(h[k] * A)
+        assert abs(v1 - v0) / v0 <= 1e-13
+        t0 = gpu.dsum(M0[k], T(z['tr0_0'][k], dev))
+        t1 = gpu.dsum(M[k], trc[0][k])
+        assert abs(t1 - t0) / abs(t0) <= 1e-13
+
+
+def test_repeat_runs_identical(dev, isw, grid4):
+    """Two runs from the same state are bit-identical (no atomics, fixed summation order)."""
+    a = run_stack(isw, grid4, golden('ocean2_n4'), dev, 3)
+    b = run_stack(isw, grid4, golden('ocean2_n4'), dev, 3)
+    for x, y in zip(a[1:4], b[1:4]):
+        assert torch.equal(x, y)
+
+
+def test_unsupported_options_refused(dev, isw, grid4):
+    gpu, layers, _ = isw
+    dg = gpu.DeviceGrid(grid4)
+    for kw in (dict(air={'cp': 1004.6}), dict(wall=np.ones(dg.E)), dict(shelf=50.0)):
+        with pytest.raises(NotImplementedError):
+            layers.Layers(dg, 1, **kw)
+
+
+def test_bad_arguments_rejected(dev, isw, grid4):
+    gpu, layers, _ = isw
+    dg = gpu.DeviceGrid(grid4)
+    core = layers.Layers(dg, 1)
+    h = torch.zeros(1, dg.N, dtype=torch.float64, device=dev)
+    u = torch.zeros(1, dg.E, dtype=torch.float64, device=dev)
+    with pytest.raises(ValueError):
+        core.step(h[:, :10], u, 900.0, 2)
+    with pytest.raises(TypeError):
+        core.step(h.float(), u, 900.0, 2)
+    with pytest.raises(ValueError):
+        core.step(h, u, -1.0, 2)
