@@ -17,6 +17,9 @@
  *   isw_transport_mass_after   src/insilica/transport.py:32-35 Transport.mass_after(M0, Fm, M1)
  *   isw_transport_step_many    src/insilica/transport.py:40-71 Transport.step_many(M0, M1, Fm, tracers, order)
  *   isw_dsum                   src/insilica/gpu.py:111-126   dsum(x, y)
+ *   isw_mesh_build / _get      src/insilica/grid/__init__.py:86-103 make(n, order): icosa.py build_grid :227-277 with
+ *                              lloyd_scvt :194-223, edge_list :280-287, hilbert_order :309-338, reorder :341-353;
+ *                              trisk.py build_trisk :15-113 and gather_tables :116-142
  */
 #ifndef ISW_H
 #define ISW_H
@@ -42,6 +45,7 @@ enum { ISW_FP64 = 0, ISW_MIXED = 1 };   /* precision forms: plain FP64 (referenc
 typedef struct isw_grid isw_grid;
 typedef struct isw_layers isw_layers;
 typedef struct isw_transport isw_transport;
+typedef struct isw_mesh isw_mesh;
 
 /* A host grid: the reference Grid's arrays (names as in src/insilica/grid/trisk.py and icosa.py). Sizes: N cells, E
  * edges, NV vertices; tables int32 (pads -1), signs and slots int8, geometry FP64. deg, dist, eKi, eKj feed the
@@ -103,6 +107,16 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
 
 /* Deterministic sum of x[0..n) (or of x * y): the reference's fixed tree; synchronises `stream`, writes *out. */
 int isw_dsum(const double *x, const double *y, long long n, double *out, void *stream);
+
+/* Build the level-n mesh (N = 10 4^n + 2 cells) on the host: icosphere, Lloyd smoothing to 1e-11 rad (at most max_iters
+ * iterations; on CUDA device `device`, or on host cores when device < 0), geometry, edge list, Hilbert renumbering when
+ * hilbert != 0, TRiSK weights and gather tables. pos_v1 (N x 3, or NULL) supplies the smoothed positions in the
+ * icosphere's numbering instead of running Lloyd. */
+int isw_mesh_build(int n, int hilbert, int max_iters, int device, const double *pos_v1, isw_mesh **out);
+/* A mesh array by its reference name ("eI", "cellEdge", "w", "pos", ...). kind: 0 float64, 1 int32, 2 int8, 3 uint8,
+ * 4 float64 3-vectors (count = vectors), 5 int64 scalar, 6 float64 scalar. The data stays owned by the mesh. */
+int isw_mesh_get(const isw_mesh *m, const char *name, const void **data, int64_t *count, int *kind);
+int isw_mesh_destroy(isw_mesh *m);
 
 #ifdef __cplusplus
 }

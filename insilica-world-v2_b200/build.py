@@ -23,6 +23,7 @@ SOURCES = [  # (file, extra flags)
     ('layers.cu', ['-fmad=false']),
     ('transport.cu', ['-fmad=false']),
     ('dsum.cu', ['-fmad=false']),
+    ('mesh.cu', ['-fmad=false', '-Xcompiler', '-fopenmp']),
 ]
 
 
@@ -44,7 +45,7 @@ def build(verbose=False, check=False, force=False):
         if verbose:
             print(' '.join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    cmd = [NVCC, '-shared', '-o', str(OUT)] + [str(o) for o in objs] + ARCH + ['-cudart', 'static']
+    cmd = [NVCC, '-shared', '-o', str(OUT)] + [str(o) for o in objs] + ARCH + ['-cudart', 'static', '-lgomp']
     if verbose:
         print(' '.join(cmd), flush=True)
     subprocess.run(cmd, check=True)
