@@ -1,0 +1,307 @@
+"""Benchmark: model days per second of the stacked-layer TRiSK step with FCT transport at level 6.
+
+Workload (one "step"): the level-6 member of the stacked-layer benchmark, an air stack of 3 Boussinesq layers and an
+ocean stack of 2 (40962 cells, 122880 edges, 81920 vertices), each advanced by one time-split RK3 step (nfast = 20,
+37 barotropic sub-steps, hyperviscosity, interfacial stress), its receiving masses and one FCT transport step of 3
+tracers. dt = 300 s, so a step is 300 s of model time. Synthetic seeded initial states (balanced jets, random
+spherical-harmonic terrain, 1% perturbations, random tracers); the grid is built on the device (Lloyd to 1e-11 rad).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl isw|reference] [--level 6]
+
+Under torchrun (N > 1) every rank advances its own member (replicas: the members are independent) and rank 0 prints
+one JSON line with the whole job's model days per second (the max step time over ranks). `--impl reference` times
+the reference's own kernels compiled for the host (oracle/_ref), driven through the reference's step sequence, on the
+host cores, rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / 'insilica-world-v2_b200'))
+
+import numpy as np  # noqa: E402
+
+L2_BYTES = 126 * 2 ** 20
+SECONDS_PER_DAY = 86400.0
+
+
+def peaks():
+    p = ROOT / 'MEASURED_PEAKS.json'
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def metric_name(level):
+    return f'model days/s, level {level}, air (3 layers) + ocean (2 layers) stacks, FCT 3 tracers each, nfast 20'
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
+                                          '-lms', '200'], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        if not self.rows:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = [float(r[1]) for r in self.rows if r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace('.', '', 1).isdigit()]
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(mx) if mx else None, 'reasons': reasons,
+                'samples': len(self.rows)}
+
+
+def build_grid(level, device):
+    from isw import grid as G
+    from isw.workload import planet_grid
+    t = time.time()
+    g = G.build(level, device=device)
+    return planet_grid(g), time.time() - t
+
+
+def cpu_member(g, seed, backend):
+    """The same member on the host, through the oracle driver (backend 'oracle': this project's C restatement;
+    'reference': the reference's own kernels compiled for the host)."""
+    from isw import cases
+    from oracle import model as M
+    og = M.OracleGrid(g)
+    stacks = []
+    topo = cases.topography(g, seed)
+    for kind in ('air', 'ocean'):
+        s = cases.stack_state(g, kind, seed, ntracers=3, topo=topo)
+        core = M.Layers(og, s['L'], b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'],
+                        vmix=s['vmix'], backend=backend)
+        tr = M.Transport(og, layers=s['L'], tracers=3, backend=backend)
+        h, u = s['h'].copy(), s['u'].copy()
+        Mm = h * g.areaCell[None]
+        stacks.append(dict(core=core, tr=tr, h=h, u=u, M=Mm, M1=np.zeros_like(Mm), Fm=np.zeros_like(u),
+                           trc=[t.copy() for t in s['tracers']]))
+    dt = cases.stack_dt(g.n)
+
+    def step():
+        for s in stacks:
+            s['core'].step(s['h'], s['u'], dt, 20, s['Fm'])
+            s['tr'].mass_after(s['M'], s['Fm'], s['M1'])
+            s['tr'].step_many(s['M'], s['M1'], s['Fm'], s['trc'], order=3)
+            s['M'], s['M1'] = s['M1'], s['M']
+    return step, dt
+
+
+def time_cpu(step, budget_s, max_steps):
+    """Mean seconds per step over a bounded sample (at least one step, at most max_steps or budget_s)."""
+    step()                                   # warm the caches and the thread pool
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps and (n == 0 or time.perf_counter() - t0 < budget_s):
+        step()
+        n += 1
+    return (time.perf_counter() - t0) / n, n
+
+
+def ensure_oracle():
+    from oracle import model as M
+    if not (ROOT / 'oracle' / 'liboracle.so').exists():
+        M.build()
+
+
+def run_reference(args, rank):
+    """The reference arm: its own kernels (oracle/_ref) on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import refkernels
+    threads = os.cpu_count() or 1
+    out = dict(metric=metric_name(args.level), unit='model days/s', impl='reference', n_gpus=args.gpus, steps=args.steps,
+               warmup=args.warmup, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64', data='synthetic',
+               config=dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s'))
+    if not refkernels.available():
+        out['unavailable'] = 'oracle/_ref was not built (the reference sources were absent when build() ran)'
+        print(json.dumps(out), flush=True)
+        return
+    ensure_oracle()
+    import torch
+    g, _ = build_grid(args.level, 0 if torch.cuda.is_available() else 'cpu')
+    step, dt = cpu_member(g, 0, 'reference')
+    for _ in range(max(0, min(args.warmup, 1))):
+        step()
+    sec, n = time_cpu(step, budget_s=max(20.0, 2.0 * args.steps), max_steps=args.steps)
+    v = dt / SECONDS_PER_DAY / sec
+    out.update(value=v, ms_per_step=sec * 1e3,
+               cpu_baseline=dict(value=v, unit='model days/s', cores=threads, kind='reference',
+                                 sample=f'{n} full steps of the workload (reference kernels compiled for the host, OpenMP over blocks)'),
+               e2e=dict(value=v, unit='model days/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='isw', choices=('isw', 'reference'))
+    ap.add_argument('--level', type=int, default=6)
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from isw import roofline
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid, set_precision
+    from isw.workload import Member
+    set_precision('double')
+    dev = torch.device(f'cuda:{local}')
+    torch.cuda.set_device(dev)
+    g, t_grid = build_grid(args.level, local)
+    dg = DeviceGrid(g, device=local)
+    member = Member(dg, seed=rank, batch=None if args.percall else Batch(local))
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(args.warmup):
+        member.step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_soak = time.time()                     # keep the GPU busy ~1 s so the clock samples cover load, then time
+        while time.time() - t_soak < 1.0:
+            for _ in range(20):
+                member.step()
+            torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()                        # the L2 holds no state from the previous step
+            starts[k].record(stream)
+            member.step()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    finite = all(bool(torch.isfinite(a).all()) for a in member.state())
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    dt = member.dt
+    value = world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
+
+    # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state, every step
+    host = [torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for a in member.state()]
+    for hbuf, a in zip(host, member.state()):
+        hbuf.copy_(a)
+    torch.cuda.synchronize()
+    e2e_steps = max(3, args.steps // 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for hbuf, a in zip(host, member.state()):
+            a.copy_(hbuf, non_blocking=True)
+        member.step()
+        for hbuf, a in zip(host, member.state()):
+            hbuf.copy_(a, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    io_bytes = sum(a.numel() * a.element_size() for a in member.state())
+
+    bytes_step = 0
+    for s in member.stacks:
+        N, E, NV, nE2 = roofline.grid_sizes(g)
+        bytes_step += roofline.layers_step_bytes(N, E, NV, nE2, s.L, s.nfast, nu4=bool(s.core.nu4), vmix=bool(s.core.vmix))
+        bytes_step += roofline.transport_bytes(N, E, s.L, s.T)
+    peak, peak_kind = peaks()
+    achieved = bytes_step / (ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / 'profiles' / 'traffic.json'
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f'level{args.level}_step_bytes')
+
+    out = dict(metric=metric_name(args.level), value=value, unit='model days/s', n_gpus=world, steps=args.steps,
+               warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
+               data='synthetic', impl='isw',
+               config=dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s',
+                           level=args.level, cells=int(g.N), edges=int(g.E), vertices=int(g.NV), precision='fp64',
+                           launch='call by call' if args.percall else 'one persistent launch per step',
+                           parallelism=f'replicas x{world}', l2='flushed between timed steps (252 MB write)'),
+               roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=traffic,
+                             peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step'),
+               e2e=dict(value=world * (dt / SECONDS_PER_DAY) / (e2e_ms / 1e3), unit='model days/s',
+                        h2d_bytes_per_step=io_bytes, d2h_bytes_per_step=io_bytes),
+               gpu_launches=member.launches() * args.steps, clocks=clk.summary(), finite=finite, grid_build_s=t_grid)
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ensure_oracle()
+        step, _ = cpu_member(g, 0, 'oracle')
+        sec, n = time_cpu(step, budget_s=15.0, max_steps=50)
+        out['cpu_baseline'] = dict(value=dt / SECONDS_PER_DAY / sec, unit='model days/s', cores=os.cpu_count() or 1, kind='port',
+                                   sample=f'{n} full steps of the same member (the C oracle, OpenMP on all host threads)')
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -17,6 +17,8 @@
  *   isw_transport_mass_after   src/insilica/transport.py:32-35 Transport.mass_after(M0, Fm, M1)
  *   isw_transport_step_many    src/insilica/transport.py:40-71 Transport.step_many(M0, M1, Fm, tracers, order)
  *   isw_dsum                   src/insilica/gpu.py:111-126   dsum(x, y)
+ *   isw_batch_*                src/insilica/ensemble.py:8-29 Ensemble.step, with each member's world.py:290-301 tick
+ *                              (Layers.step, Transport.mass_after, Transport.step_many, copyto(M, M1)) in one launch
  *   isw_mesh_build / _get      src/insilica/grid/__init__.py:86-103 make(n, order): icosa.py build_grid :227-277 with
  *                              lloyd_scvt :194-223, edge_list :280-287, hilbert_order :309-338, reorder :341-353;
  *                              trisk.py build_trisk :15-113 and gather_tables :116-142
@@ -46,6 +48,7 @@ typedef struct isw_grid isw_grid;
 typedef struct isw_layers isw_layers;
 typedef struct isw_transport isw_transport;
 typedef struct isw_mesh isw_mesh;
+typedef struct isw_batch isw_batch;
 
 /* A host grid: the reference Grid's arrays (names as in src/insilica/grid/trisk.py and icosa.py). Sizes: N cells, E
  * edges, NV vertices; tables int32 (pads -1), signs and slots int8, geometry FP64. deg, dist, eKi, eKj feed the
@@ -107,6 +110,26 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
 
 /* Deterministic sum of x[0..n) (or of x * y): the reference's fixed tree; synchronises `stream`, writes *out. */
 int isw_dsum(const double *x, const double *y, long long n, double *out, void *stream);
+
+/* Batched step: stacks (a Layers handle with its state h, u, Fm, and optionally a Transport with M, M1 and tracers)
+ * registered once, then advanced together by isw_batch_step in ONE persistent cooperative launch per step: the RK3 step,
+ * the receiving masses M1, the FCT step of every tracer, and M <- M1. Stacks may use different grids and layer counts;
+ * each stack's result is bit-identical to stepping it alone. Registered pointers are borrowed until removed. */
+int isw_batch_create(int device, isw_batch **out);
+int isw_batch_destroy(isw_batch *b);
+int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *M, double *M1,
+                  double *const *tracers, int ntr, double dt, int nfast, int *slot);
+int isw_batch_remove(isw_batch *b, int slot);
+int isw_batch_step(isw_batch *b, void *stream);
+/* Tuning: the barotropic fast loop in shared-memory tiles (tiles_enabled != 0, the default) exchanging every tile_k
+ * sub-steps (1..32, default 4), or as grid-wide passes. Results are the same either way. */
+int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k);
+/* The batch's device status word (ISW_OK, or ISW_ETIMEOUT after a grid barrier's bounded wait ran out); synchronises
+ * `stream`; reset != 0 clears it. */
+int isw_batch_status(isw_batch *b, void *stream, int reset);
+/* Failure-detection test: one step in which block 0 never arrives at the first grid barrier, so every other block's
+ * bounded wait runs out after timeout_ns (1 ms .. 2 s) and the status word becomes ISW_ETIMEOUT. Test use only. */
+int isw_batch_fault_test(isw_batch *b, long long timeout_ns, void *stream);
 
 /* Build the level-n mesh (N = 10 4^n + 2 cells) on the host: icosphere, Lloyd smoothing to 1e-11 rad (at most max_iters
  * iterations; on CUDA device `device`, or on host cores when device < 0), geometry, edge list, Hilbert renumbering when

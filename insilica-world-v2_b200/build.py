@@ -24,6 +24,8 @@ SOURCES = [  # (file, extra flags)
     ('transport.cu', ['-fmad=false']),
     ('dsum.cu', ['-fmad=false']),
     ('mesh.cu', ['-fmad=false', '-Xcompiler', '-fopenmp']),
+    ('tiles.cu', ['-fmad=false']),
+    ('batch.cu', ['-fmad=false']),
 ]
 
 

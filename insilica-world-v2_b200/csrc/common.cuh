@@ -45,6 +45,7 @@ struct LayersDev {
   const double *b, *fV, *Gc;
   double *B, *q, *Tp, *F, *scale, *G, *He, *ubs, *ub0, *ub, *acc, *eta0, *eta, *eta_prev;
   double *h1, *h2, *u1, *u2, *D1, *Z1, *L1, *L2, *hedge, *diss, *pk;
+  double *ub2;                               // second exchange buffer of the tiled fast loop
   float *q32, *B32, *Tp32, *G32, *pk32;      // mixed-form scratch
   double *red;                               // reduction scratch (substeps)
 };
@@ -70,4 +71,5 @@ struct isw_grid {
   isw::GridDev d;
   std::vector<void *> allocs;
   double dmin;                   // smallest edge spacing (Layers.dmin)
+  std::vector<int32_t> h_nbr, h_cellEdge, h_eI, h_eJ;   // host copies the fast-loop tiles are built from
 };

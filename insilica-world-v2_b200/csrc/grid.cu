@@ -182,6 +182,10 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     d.le32 = upload_f32(g, h->le, E); d.de32 = upload_f32(g, h->de, E); d.rde32 = upload_f32(g, rde.data(), E);
     d.rA32 = upload_f32(g, rA.data(), N); d.rAV32 = upload_f32(g, rAV.data(), NV);
     d.kite32 = upload_f32(g, h->kite, (size_t)N * 6);
+    g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
+    g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);
+    g->h_eI.assign(h->eI, h->eI + E);
+    g->h_eJ.assign(h->eJ, h->eJ + E);
     double dmin = h->de[0];
     for (int e = 1; e < E; e++) dmin = h->de[e] < dmin ? h->de[e] : dmin;
     g->dmin = dmin;

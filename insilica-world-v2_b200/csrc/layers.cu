@@ -10,6 +10,7 @@
 #include <sstream>
 
 #include "common.cuh"
+#include "handles.cuh"
 #include "layers_fp64.cuh"
 
 namespace isw {
@@ -135,23 +136,6 @@ __global__ void k_max_reduce(const double *in, int n, double *out) {
 
 using namespace isw;
 
-struct GraphEntry {
-  const double *h, *u, *Fm;
-  double dt;
-  int nfast;
-  cudaGraphExec_t exec;
-};
-
-struct isw_layers {
-  isw_grid *grid;
-  LayersDev d;
-  std::vector<void *> allocs;
-  cudaStream_t cap;                 // private stream the step graphs are captured on
-  std::list<GraphEntry> graphs;     // most recent first
-  int colmax_blocks;
-  int *nonfinite;
-};
-
 namespace {
 
 constexpr size_t GRAPH_CACHE = 8;
@@ -256,6 +240,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.h1 = dalloc(s, (size_t)L * N); d.h2 = dalloc(s, (size_t)L * N); d.u1 = dalloc(s, (size_t)L * E); d.u2 = dalloc(s, (size_t)L * E);
     d.D1 = dalloc(s, (size_t)L * N); d.Z1 = dalloc(s, (size_t)L * NV); d.L1 = dalloc(s, (size_t)L * E); d.L2 = dalloc(s, (size_t)L * E);
     d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
+    d.ub2 = dalloc(s, E);
     s->colmax_blocks = blocks_for(N) < 1024 ? blocks_for(N) : 1024;
     d.red = dalloc(s, s->colmax_blocks + 1);
     void *nf = nullptr;

@@ -1,0 +1,37 @@
+// Shared-memory tiles for the barotropic fast loop.
+//
+// The fast loop (reference layers.cu:366-388, driven by layers.py:168-175) alternates a cell pass (eta) and an edge pass
+// (ubar) ceil(c nfast) times per stage. Each tile owns a contiguous (Hilbert-ordered) range of cells and the edges whose
+// eI cell it owns, and stages in shared memory its cells out to k rings (ring 0 = owned) and every edge of those cells.
+// It can then advance k sub-steps with no grid-wide sync: sub-step m (1..k) updates eta on cells of ring <= k - m + 1
+// and ubar on edges whose nearer cell has ring <= k - m, which is exactly what the owned values after k sub-steps
+// depend on. Tiles exchange owned eta and ubar through global memory every k sub-steps (double-buffered, one grid
+// barrier per exchange). Arithmetic is the reference's, per cell and edge, in the same gather order.
+//
+// Local numbering: cells in ring order, edges in order of their nearer cell's ring, so "ring <= r" is a prefix.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+namespace isw {
+
+struct TileSetHost {
+  int P = 0, k = 0;
+  size_t smem = 0;                             // dynamic shared memory of the largest tile
+  std::vector<int32_t> cell_off, edge_off;     // P + 1 offsets
+  std::vector<int32_t> cells, edges;           // global ids, tile by tile, local order
+  std::vector<int32_t> ncnt, ecnt;             // per tile k + 1 prefix counts: cells of ring <= r, edges of ring <= r
+  std::vector<int16_t> cedge;                  // per local cell 6 local edge ids (-1 pads), cellEdge slot order
+  std::vector<int16_t> eIl, eJl;               // per local edge its local cells (-1 outside the tile)
+};
+
+// Per-tile shared-memory bytes: per cell eta, eta_prev, area, Gc, 6 coefficients (8 B each) and 6 local edge ids
+// (2 B); per edge ubar, G, d_e, acc (8 B each) and two local cell ids (2 B).
+inline size_t tile_smem_bytes(size_t nc, size_t ne) { return nc * (4 * 8 + 6 * 8 + 6 * 2) + ne * (4 * 8 + 2 * 2) + 64; }
+
+// Build P tiles over a grid (N cells with neighbour table nbr (N x 6, pads -1), cellEdge (N x 6), eI, eJ (E)).
+TileSetHost build_tiles(int N, int E, const int32_t *nbr, const int32_t *cellEdge, const int32_t *eI, const int32_t *eJ, int P,
+                        int k);
+
+}  // namespace isw

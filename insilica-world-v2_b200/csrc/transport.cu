@@ -13,39 +13,10 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "handles.cuh"
 
 namespace isw {
 namespace {
-
-struct TrArgs {
-  const double *M0, *M1, *Fm;
-  double *tr[TRMAX];              // the caller's tracer arrays
-  int L, rows;
-  double beta;
-};
-
-struct TransportDev {
-  GridDev g;
-  double *psi0, *td, *p1, *p2, *A, *Rp, *Rm;   // rows x N (A rows x E); psi0 holds the tracers as they came in
-};
-
-__device__ __forceinline__ double upwind(const double *__restrict__ Fml, const double *__restrict__ p, const int *eI, const int *eJ,
-                                         int e) {
-  const double f = Fml[e];
-  return f * (f >= 0 ? p[eI[e]] : p[eJ[e]]);
-}
-
-// reference fused.cu:131-138, FP64 form
-__device__ __forceinline__ double hoflux(const GridDev &g, const double *__restrict__ Fml, const double *__restrict__ ps, int e,
-                                         double beta) {
-  const double f = Fml[e];
-  const int o = e * 8;
-  const int *idx = g.d2idx;
-  const double *wt = g.d2wt;
-  const double a = wt[o] * ps[idx[o]] + wt[o + 1] * ps[idx[o + 1]] + wt[o + 2] * ps[idx[o + 2]] + wt[o + 3] * ps[idx[o + 3]];
-  const double b = wt[o + 4] * ps[idx[o + 4]] + wt[o + 5] * ps[idx[o + 5]] + wt[o + 6] * ps[idx[o + 6]] + wt[o + 7] * ps[idx[o + 7]];
-  return f * (0.5 * (ps[g.eI[e]] + ps[g.eJ[e]]) - (a + b)) + fabs(f) * ((b - a) * beta);
-}
 
 // reference trisk.cu:48-59
 __global__ void __launch_bounds__(THREADS) k_mass(const GridDev g, int L, const double *__restrict__ M0, const double *__restrict__ Fm,
@@ -53,124 +24,31 @@ __global__ void __launch_bounds__(THREADS) k_mass(const GridDev g, int L, const 
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.N * L) return;
   const int l = t / g.N, i = t - l * g.N;
-  const size_t o = (size_t)l * g.N + i;
-  const double *f = Fm + (size_t)l * g.E;
-  double m = M0[o];
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    if (g.eI[e] == i) m -= f[e]; else m += f[e];
-  }
-  M1[o] = m;
+  M1[(size_t)l * g.N + i] = fp64::mass_cell(g, M0, Fm + (size_t)l * g.E, l, i);
 }
 
-// P1: copy psi in, td, and p1 (frac 1/3 from psi)
 __global__ void __launch_bounds__(THREADS) k_p1(const TransportDev T, const TrArgs a, int order) {
-  const GridDev &g = T.g;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.N * a.rows) return;
-  const int y = t / g.N, i = t - y * g.N, l = y % a.L, j = y / a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *p = a.tr[j] + (size_t)l * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
-  const double pi = p[i];
-  T.psi0[o] = pi;
-  double td = a.M0[om] * pi;
-  double s = a.M0[om] * pi, mx = a.M0[om];
-  const double frac = 1.0 / 3.0;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const bool out = g.eI[e] == i;
-    const double fu = upwind(Fml, p, g.eI, g.eJ, e);
-    if (out) td -= fu; else td += fu;
-    if (order != 1) {
-      const double f = frac * hoflux(g, Fml, p, e, a.beta);
-      const double m = frac * Fml[e];
-      if (out) { s -= f; mx -= m; } else { s += f; mx += m; }
-    }
-  }
-  T.td[o] = td / a.M1[om];
-  if (order != 1) T.p1[o] = s / mx;
+  if (t >= T.g.N * a.rows) return;
+  fp64::tr_p1(T, a, order, false, t / T.g.N, t % T.g.N);
 }
 
-// P2: p2 (frac 1/2 from p1)
 __global__ void __launch_bounds__(THREADS) k_p2(const TransportDev T, const TrArgs a) {
-  const GridDev &g = T.g;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.N * a.rows) return;
-  const int y = t / g.N, i = t - y * g.N, l = y % a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *p1 = T.p1 + (size_t)y * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
-  const double frac = 1.0 / 2.0;
-  double s = a.M0[om] * T.psi0[o], mx = a.M0[om];
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double f = frac * hoflux(g, Fml, p1, e, a.beta);
-    const double m = frac * Fml[e];
-    if (g.eI[e] == i) { s -= f; mx -= m; } else { s += f; mx += m; }
-  }
-  T.p2[o] = s / mx;
+  if (t >= T.g.N * a.rows) return;
+  fp64::tr_p2(T, a, t / T.g.N, t % T.g.N);
 }
 
-// P3: antidiffusive fluxes and Zalesak ratios
 __global__ void __launch_bounds__(THREADS) k_p3(const TransportDev T, const TrArgs a) {
-  const GridDev &g = T.g;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.N * a.rows) return;
-  const int y = t / g.N, i = t - y * g.N, l = y % a.L;
-  const double *p = T.psi0 + (size_t)y * g.N;
-  const double *tt = T.td + (size_t)y * g.N;
-  const double *p2 = T.p2 + (size_t)y * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
-  double hi = fmax(p[i], tt[i]), lo = fmin(p[i], tt[i]);
-  for (int k = 0; k < 6; k++) {
-    const int j = g.nbr[i * 6 + k];
-    if (j < 0) break;
-    hi = fmax(hi, fmax(p[j], tt[j]));
-    lo = fmin(lo, fmin(p[j], tt[j]));
-  }
-  const double m1 = a.M1[(size_t)l * g.N + i];
-  const double qmax = (hi - tt[i]) * m1, qmin = (tt[i] - lo) * m1;
-  double Pp = 0, Pm = 0;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double A = hoflux(g, Fml, p2, e, a.beta) - upwind(Fml, p, g.eI, g.eJ, e);
-    if (g.eI[e] == i) {
-      T.A[(size_t)y * g.E + e] = A;
-      if (A > 0) Pm += A; else Pp -= A;
-    } else {
-      if (A > 0) Pp += A; else Pm -= A;
-    }
-  }
-  T.Rp[(size_t)y * g.N + i] = Pp > 0 ? fmin(1.0, qmax / Pp) : 0.0;
-  T.Rm[(size_t)y * g.N + i] = Pm > 0 ? fmin(1.0, qmin / Pm) : 0.0;
+  if (t >= T.g.N * a.rows) return;
+  fp64::tr_p3(T, a, t / T.g.N, t % T.g.N);
 }
 
-// P4: the limited update into the caller's tracer arrays
 __global__ void __launch_bounds__(THREADS) k_p4(const TransportDev T, const TrArgs a) {
-  const GridDev &g = T.g;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.N * a.rows) return;
-  const int y = t / g.N, i = t - y * g.N, l = y % a.L, j = y / a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *Al = T.A + (size_t)y * g.E;
-  const double *rp = T.Rp + (size_t)y * g.N;
-  const double *rm = T.Rm + (size_t)y * g.N;
-  const double m1 = a.M1[om];
-  double s = T.td[o] * m1;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double A = Al[e];
-    const int ea = g.eI[e], eb = g.eJ[e];
-    const double c = A > 0 ? fmin(rp[eb], rm[ea]) : fmin(rp[ea], rm[eb]);
-    if (ea == i) s -= c * A; else s += c * A;
-  }
-  a.tr[j][(size_t)l * g.N + i] = s / m1;
+  if (t >= T.g.N * a.rows) return;
+  fp64::tr_p4(T, a, t / T.g.N, t % T.g.N);
 }
 
 // order 1: td out
@@ -185,14 +63,6 @@ __global__ void __launch_bounds__(THREADS) k_td_out(const TransportDev T, const 
 }  // namespace isw
 
 using namespace isw;
-
-struct isw_transport {
-  isw_grid *grid;
-  TransportDev d;
-  int L, T, precision;
-  double beta;
-  std::vector<void *> allocs;
-};
 
 namespace {
 
@@ -276,7 +146,7 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
     ISW_CUDA(cudaSetDevice(t->grid->device));
     TrArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.M0 = M0; a.M1 = M1; a.Fm = Fm; a.L = t->L; a.rows = ntr * t->L; a.beta = t->beta;
+    a.M0 = M0; a.M1 = const_cast<double *>(M1); a.Fm = Fm; a.L = t->L; a.rows = ntr * t->L; a.beta = t->beta;
     for (int j = 0; j < ntr; j++) {
       if (!tracers[j]) fail(ISW_EINVAL, "transport.step_many: null tracer");
       a.tr[j] = tracers[j];

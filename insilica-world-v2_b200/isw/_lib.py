@@ -57,6 +57,14 @@ isw_dsum = _sig('isw_dsum', I, [P, P, LL, ctypes.POINTER(D), P])
 isw_mesh_build = _sig('isw_mesh_build', I, [I, I, I, I, P, ctypes.POINTER(P)])
 isw_mesh_get = _sig('isw_mesh_get', I, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(I)])
 isw_mesh_destroy = _sig('isw_mesh_destroy', I, [P])
+isw_batch_create = _sig('isw_batch_create', I, [I, ctypes.POINTER(P)])
+isw_batch_destroy = _sig('isw_batch_destroy', I, [P])
+isw_batch_add = _sig('isw_batch_add', I, [P, P, P, P, P, P, P, P, ctypes.POINTER(P), I, D, I, ctypes.POINTER(I)])
+isw_batch_remove = _sig('isw_batch_remove', I, [P, I])
+isw_batch_step = _sig('isw_batch_step', I, [P, P])
+isw_batch_config = _sig('isw_batch_config', I, [P, I, I])
+isw_batch_status = _sig('isw_batch_status', I, [P, P, I])
+isw_batch_fault_test = _sig('isw_batch_fault_test', I, [P, LL, P])
 
 
 class IswError(RuntimeError):

@@ -1,0 +1,165 @@
+"""The batched persistent step (isw.batch.Batch over the C ABI): each stack's result is bit-identical to stepping it
+alone, across stacks of different grids and layer counts in one launch; the golden vectors hold through it; and a
+grid barrier whose wait runs out reports ISW_ETIMEOUT to the host and leaves the context usable."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from isw import gpu
+    gpu.set_precision('double')
+    return torch.device('cuda:0')
+
+
+def T(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+
+
+def make_stack(dg, z, dev):
+    from isw.layers import Layers
+    from isw.transport import Transport
+    L = int(z['L'])
+    core = Layers(dg, L, b=z['b'], gprime=list(z['gprime']), stress=list(z['stress']), nu4=float(z['nu4']),
+                  floor=float(z['floor']), vmix=float(z['vmix']))
+    tr = Transport(dg, layers=L, tracers=3)
+    st = dict(core=core, tr=tr, h=T(z['h0'], dev), u=T(z['u0'], dev))
+    st['M'] = T(z['h0'] * dg.host.areaCell[None], dev)
+    st['M1'] = torch.zeros_like(st['M'])
+    st['Fm'] = torch.zeros_like(st['u'])
+    st['trc'] = [T(z[f'tr{k}_0'], dev) for k in range(3)]
+    return st
+
+
+def percall(st, dt, nfast, steps):
+    for _ in range(steps):
+        st['core'].step(st['h'], st['u'], dt, nfast, st['Fm'])
+        st['tr'].mass_after(st['M'], st['Fm'], st['M1'])
+        st['tr'].step_many(st['M'], st['M1'], st['Fm'], st['trc'], order=3)
+        st['M'].copy_(st['M1'])
+
+
+def fields(st):
+    return [st['h'], st['u'], st['M'], st['Fm']] + st['trc']
+
+
+def test_batch_matches_percall_and_golden(dev, grid4):
+    """Air and ocean stacks in one launch per step: equal to the call-by-call path bit for bit, and to the reference's
+    golden vectors to 1e-12 (bit for bit where no exp() is involved)."""
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    dg = DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    zs = [golden('air3_n4'), golden('ocean2_n4')]
+    a = [make_stack(dg, z, dev) for z in zs]
+    b = [make_stack(dg, z, dev) for z in zs]
+    batch = Batch(0)
+    for st, z in zip(b, zs):
+        batch.add(st['core'], st['h'], st['u'], st['Fm'], tr=st['tr'], M=st['M'], M1=st['M1'], tracers=st['trc'],
+                  dt=float(z['dt']), nfast=int(z['nfast']))
+    for st, z in zip(a, zs):
+        percall(st, float(z['dt']), int(z['nfast']), 6)
+    for _ in range(6):
+        batch.step()
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    for sa, sb, z in zip(a, b, zs):
+        for x, y in zip(fields(sa), fields(sb)):
+            assert torch.equal(x, y)
+        for name, x in (('h', sb['h']), ('u', sb['u']), ('M', sb['M'])):
+            ref = z[name]
+            assert float(np.max(np.abs(x.cpu().numpy() - ref)) / np.max(np.abs(ref))) <= 1e-12, name
+
+
+def test_batch_w2_bit_exact(dev, grid4):
+    """Williamson 2 through the batch (one layer, no transport): 480 steps equal the reference's bit for bit."""
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.layers import Layers
+    z = golden('w2_n4')
+    dg = DeviceGrid(G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616))
+    core = Layers(dg, 1, b=z['b'])
+    h, u = T(z['h0'], dev), T(z['u0'], dev)
+    Fm = torch.zeros_like(u)
+    batch = Batch(0)
+    batch.add(core, h, u, Fm, dt=float(z['dt']), nfast=int(z['nfast']))
+    for s in range(1, 481):
+        batch.step()
+        if s in (1, 96, 480):
+            torch.cuda.synchronize()
+            assert np.array_equal(h.cpu().numpy(), z[f'h{s}']) and np.array_equal(u.cpu().numpy(), z[f'u{s}']), s
+
+
+def test_batch_mixed_levels_equal_alone(dev, grid4):
+    """Members on level 3 and level 4 grids share one launch; each equals its own run alone, bit for bit."""
+    from isw import cases
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg4 = DeviceGrid(planet_grid(grid4))
+    dg3 = DeviceGrid(planet_grid(G.build(3, device='cpu')))
+    batch = Batch(0)
+    mixed = [Member(dg3, 5, nfast=20, batch=batch), Member(dg4, 6, nfast=20, batch=batch)]
+    alone = [Member(dg3, 5, nfast=20), Member(dg4, 6, nfast=20)]
+    for _ in range(4):
+        batch.step()
+        for m in alone:
+            m.step()
+    torch.cuda.synchronize()
+    for mb, ma in zip(mixed, alone):
+        for x, y in zip(mb.state(), ma.state()):
+            assert torch.equal(x, y)
+
+
+def test_barrier_timeout_reports_and_recovers(dev, grid4):
+    """A block that never arrives at a grid barrier: the others' bounded waits run out, the host reads ISW_ETIMEOUT,
+    and the next ordinary step runs normally (same result as a fresh run)."""
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg = DeviceGrid(planet_grid(grid4))
+    batch = Batch(0)
+    Member(dg, 3, nfast=20, batch=batch)
+    batch.fault_test(timeout_s=0.05)
+    assert batch.status(reset=True) == 5
+    assert batch.status() == 0
+    fresh_batch = Batch(0)
+    a = Member(dg, 4, nfast=20, batch=fresh_batch)
+    b = Member(dg, 4, nfast=20)
+    fresh_batch.step()
+    b.step()
+    torch.cuda.synchronize()
+    assert fresh_batch.status() == 0
+    for x, y in zip(a.state(), b.state()):
+        assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize('k', [1, 2, 3, 4, 7, 11])
+def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
+    """The barotropic sub-steps in shared-memory tiles (exchanging every k sub-steps) give the grid-wide passes' result
+    bit for bit, and so does the call-by-call path."""
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg = DeviceGrid(planet_grid(grid4))
+    tiled, flat = Batch(0), Batch(0)
+    tiled.config(tiles=True, tile_k=k)
+    flat.config(tiles=False)
+    a, b, c = Member(dg, 9, batch=tiled), Member(dg, 9, batch=flat), Member(dg, 9)
+    for _ in range(3):
+        tiled.step()
+        flat.step()
+        c.step()
+    torch.cuda.synchronize()
+    assert tiled.status() == 0 and flat.status() == 0
+    for x, y, z in zip(a.state(), b.state(), c.state()):
+        assert torch.equal(x, y) and torch.equal(x, z)
