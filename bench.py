@@ -207,7 +207,9 @@ def main():
     torch.cuda.set_device(dev)
     g, t_grid = build_grid(args.level, local)
     dg = DeviceGrid(g, device=local)
-    member = Member(dg, seed=rank, batch=None if args.percall else Batch(local))
+    batch = None if args.percall else Batch(local)
+    member = Member(dg, seed=rank, batch=batch)
+    layout = batch.info() if batch is not None else None
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
@@ -282,7 +284,8 @@ def main():
                data='synthetic', impl='isw',
                config=dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s',
                            level=args.level, cells=int(g.N), edges=int(g.E), vertices=int(g.NV), precision='fp64',
-                           launch='call by call' if args.percall else 'one persistent launch per step',
+                           launch='call by call' if args.percall else 'one CUDA graph per step (phase kernels + tiled fast loop)',
+                           tiles=layout,
                            parallelism=f'replicas x{world}', l2='flushed between timed steps (252 MB write)'),
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=traffic,
                              peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step'),

@@ -121,9 +121,12 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
                   double *const *tracers, int ntr, double dt, int nfast, int *slot);
 int isw_batch_remove(isw_batch *b, int slot);
 int isw_batch_step(isw_batch *b, void *stream);
-/* Tuning: the barotropic fast loop in shared-memory tiles (tiles_enabled != 0, the default) exchanging every tile_k
- * sub-steps (1..32, default 4), or as grid-wide passes. Results are the same either way. */
+/* Tuning: the barotropic fast loop in shared-memory tiles (tiles_enabled != 0, the default) exchanging every k
+ * sub-steps, k the largest up to tile_k (1..32, default 8) whose tiles fit in shared memory; or as grid-wide passes.
+ * Results are the same either way. */
 int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k);
+/* The batch's layout: registered stacks, fast-loop tiles, the exchange interval in use, tile shared memory (bytes). */
+int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes);
 /* The batch's device status word (ISW_OK, or ISW_ETIMEOUT after a grid barrier's bounded wait ran out); synchronises
  * `stream`; reset != 0 clears it. */
 int isw_batch_status(isw_batch *b, void *stream, int reset);

@@ -37,7 +37,7 @@ constexpr int FAST_THREADS = 512;
 
 struct TileSetDev {
   int P, k;
-  const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt;
+  const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt, *eown;
   const int16_t *cedge, *eIl, *eJl;
 };
 
@@ -222,16 +222,17 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     if (kind == 1) {
       if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
     } else {
-      fp64::tr_p1(d.T, d.tr, 3, true, i / M.g.N, i % M.g.N);
+      ISW_BATCH_L(d.L, LMAXK, fp64::tr_p1<LL>(d.T, d.tr, 3, true, i / M.g.N, i % M.g.N));
     }
   } else if (PH == PH_P2) {
-    fp64::tr_p2(d.T, d.tr, i / M.g.N, i % M.g.N);
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
   } else if (PH == PH_P3) {
-    fp64::tr_p3(d.T, d.tr, i / M.g.N, i % M.g.N);
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
   } else if (PH == PH_P4) {
-    const int y = i / M.g.N, c = i % M.g.N;
-    fp64::tr_p4(d.T, d.tr, y, c);
-    if (y < d.L) d.Mm[(size_t)y * M.g.N + c] = d.tr.M1[(size_t)y * M.g.N + c];
+    const int j = i / M.g.N, c = i % M.g.N;
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p4<LL>(d.T, d.tr, j, c));
+    if (j == 0)
+      for (int l = 0; l < d.L; l++) d.Mm[(size_t)l * M.g.N + c] = d.tr.M1[(size_t)l * M.g.N + c];
   }
 }
 
@@ -241,7 +242,8 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
 // surface and ub2 / F for the barotropic wind (F, the layer fluxes, is not in use during the fast loop). The final
 // barotropic wind and its accumulated sum go to ub and acc, which no round reads.
 __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
-                                                      int rounds, GridBarrier *bar, int *status, long long timeout_ns, int fault_block) {
+                                                         int rounds, GridBarrier *bar, int *status, long long timeout_ns,
+                                                         int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileRef tr = refs[blockIdx.x];
   const StackDesc &d = S[tr.s];
@@ -251,46 +253,42 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
   const int p = tr.p, k = T.k;
   const int c0 = T.cell_off[p], nc = T.cell_off[p + 1] - c0;
   const int e0 = T.edge_off[p], ne = T.edge_off[p + 1] - e0;
+  const int eown = T.eown[p];
   const int *cells = T.cells + c0;
   const int *edges = T.edges + e0;
   const int *ncnt = T.ncnt + (size_t)p * (k + 1);
   const int *ecnt = T.ecnt + (size_t)p * (k + 1);
-  // shared-memory layout: doubles first, then 16-bit ids
+  // shared memory: doubles first, then 16-bit ids
   double *eta = reinterpret_cast<double *>(smem);
   double *eprev = eta + nc;
   double *area = eprev + nc;
   double *gc = area + nc;
-  double *coef = gc + nc;                  // nc x 6: (sign * l_e) * H_e, the reference's product order
-  double *ub = coef + (size_t)nc * 6;
+  double *ub = gc + nc;
   double *G = ub + ne;
   double *de = G + ne;
-  double *acc = de + ne;
-  int16_t *cedge = reinterpret_cast<int16_t *>(acc + ne);
+  double *lh = de + ne;                    // l_e H_e: with the cell's sign, the reference's (sign * l_e) * H_e
+  double *acc = lh + ne;                   // owned edges only
+  int16_t *cedge = reinterpret_cast<int16_t *>(acc + eown);
   int16_t *eIl = cedge + (size_t)nc * 6;
   int16_t *eJl = eIl + ne;
   const int skip = (int)blockIdx.x == fault_block;
   const int n = d.n[st];
   const double tau = d.tau[st], gam = M.div_damp;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-    const int gc_ = cells[c];
-    eta[c] = M.eta0[gc_];
-    area[c] = g.areaCell[gc_];
-    gc[c] = M.Gc[gc_];
-    for (int s = 0; s < 6; s++) {
-      const int16_t le_ = T.cedge[(size_t)(c0 + c) * 6 + s];
-      cedge[c * 6 + s] = le_;
-      if (le_ >= 0) {
-        const int e = g.cellEdge[gc_ * 6 + s];
-        coef[c * 6 + s] = (double)g.cellSign[gc_ * 6 + s] * g.le[e] * M.He[e];
-      }
-    }
+    const int gi = cells[c];
+    eta[c] = M.eta0[gi];
+    area[c] = g.areaCell[gi];
+    gc[c] = M.Gc[gi];
+#pragma unroll
+    for (int s = 0; s < 6; s++) cedge[c * 6 + s] = T.cedge[(size_t)(c0 + c) * 6 + s];
   }
   for (int e = threadIdx.x; e < ne; e += blockDim.x) {
     const int ge = edges[e];
     ub[e] = M.ub0[ge];
     G[e] = M.G[ge];
     de[e] = g.de[ge];
-    acc[e] = 0.0;
+    lh[e] = g.le[ge] * M.He[ge];
+    if (e < eown) acc[e] = 0.0;
     eIl[e] = T.eIl[e0 + e];
     eJl[e] = T.eJl[e0 + e];
   }
@@ -308,16 +306,21 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
     }
     __syncthreads();
     for (int m = 1; m <= K; m++) {
-      const int cn = ncnt[K - m + 1 <= k ? K - m + 1 : k];
+      const int cn = ncnt[K - m + 1];
       for (int c = threadIdx.x; c < cn; c += blockDim.x) {
         const double e0v = eta[c];
         eprev[c] = e0v;
         double div = 0;
+        int vs[6];
+#pragma unroll
+        for (int s = 0; s < 6; s++) vs[s] = cedge[c * 6 + s];
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-          const int le_ = cedge[c * 6 + s];
-          if (le_ < 0) break;
-          div += coef[c * 6 + s] * ub[le_];
+          const int v = vs[s];
+          if (v == 0) continue;
+          const int le_ = (v > 0 ? v : -v) - 1;
+          const double cf = v > 0 ? lh[le_] : -lh[le_];
+          div += cf * ub[le_];
         }
         eta[c] = e0v - (tau * div) / area[c];
       }
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
       const int en = ecnt[K - m];
       for (int e = threadIdx.x; e < en; e += blockDim.x) {
         const double v = ub[e];
-        acc[e] += v;
+        if (e < eown) acc[e] += v;
         const int i = eIl[e], jj = eJl[e];
         const double ej = gc[jj] * (eta[jj] + gam * (eta[jj] - eprev[jj]));
         const double ei = gc[i] * (eta[i] + gam * (eta[i] - eprev[i]));
@@ -337,16 +340,14 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
       double *xe = (r & 1) ? M.eta_prev : M.eta;
       double *xu = (r & 1) ? M.F : M.ub2;
       for (int c = threadIdx.x; c < nown; c += blockDim.x) xe[cells[c]] = eta[c];
-      for (int e = threadIdx.x; e < ne; e += blockDim.x)
-        if (eIl[e] >= 0 && eIl[e] < nown) xu[edges[e]] = ub[e];
+      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = ub[e];
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < ne; e += blockDim.x)
-    if (eIl[e] >= 0 && eIl[e] < nown) {
-      M.ub[edges[e]] = ub[e];
-      M.acc[edges[e]] = acc[e];
-    }
+  for (int e = threadIdx.x; e < eown; e += blockDim.x) {
+    M.ub[edges[e]] = ub[e];
+    M.acc[edges[e]] = acc[e];
+  }
 }
 
 }  // namespace
@@ -367,7 +368,7 @@ struct BatchSlot {
 
 struct TileCache {
   TileSetDev dev{};
-  size_t smem = 0;
+  TileSetHost host;
   std::vector<void *> allocs;
 };
 
@@ -379,14 +380,15 @@ struct isw_batch {
   Chunk *d_chunks = nullptr;
   TileRef *d_refs = nullptr;
   Sched sc{};
-  int lmax = 1, nstacks = 0, ntiles = 0, rounds[3] = {0, 0, 0}, nsub[3] = {0, 0, 0};
+  int lmax = 1, nstacks = 0, ntiles = 0, rounds[3] = {0, 0, 0}, nsub[3] = {0, 0, 0}, kused = 0;
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0;
   size_t fast_smem = 0;
   GridBarrier *bar = nullptr;
   int *status = nullptr;
-  int tile_k = 4;
+  int tile_k = 8;
   int tiles_enabled = 1;
   std::map<std::tuple<const isw_grid *, int, int>, std::unique_ptr<TileCache>> tiles;
+  std::map<std::pair<const isw_grid *, int>, std::vector<int32_t>> parts;
   cudaStream_t cap = nullptr;
   cudaGraphExec_t exec = nullptr;
   int sms = 0;
@@ -409,7 +411,9 @@ int guarded(F f) {
 }
 
 constexpr long long DEFAULT_TIMEOUT_NS = 2000000000LL;   // 2 s: far beyond any stage; only a broken grid reaches it
-constexpr size_t SMEM_BUDGET = 112 * 1024;               // per tile block: two blocks per SM
+constexpr size_t SMEM_TWO = 112 * 1024;                  // per tile block when two share an SM
+constexpr size_t SMEM_ONE = 224 * 1024;                  // per tile block alone on an SM
+constexpr int K_PROBE = 8;                               // the largest exchange interval considered
 
 template <class T>
 T *dupload(std::vector<void *> &allocs, const std::vector<T> &v) {
@@ -420,13 +424,23 @@ T *dupload(std::vector<void *> &allocs, const std::vector<T> &v) {
   return (T *)p;
 }
 
+const std::vector<int32_t> &partition_for(isw_batch *b, const isw_grid *g, int P);
+
+const std::vector<int32_t> &partition_for(isw_batch *b, const isw_grid *g, int P) {
+  auto key = std::make_pair(g, P);
+  auto it = b->parts.find(key);
+  if (it != b->parts.end()) return it->second;
+  return b->parts[key] = partition_cells(g->d.N, g->h_nbr.data(), P);
+}
+
 TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k) {
   auto key = std::make_tuple(g, P, k);
   auto it = b->tiles.find(key);
   if (it != b->tiles.end()) return it->second.get();
-  TileSetHost h = build_tiles(g->d.N, g->d.E, g->h_nbr.data(), g->h_cellEdge.data(), g->h_eI.data(), g->h_eJ.data(), P, k);
   auto c = std::make_unique<TileCache>();
-  c->smem = h.smem;
+  c->host = build_tiles(g->d.N, g->d.E, g->h_nbr.data(), g->h_cellEdge.data(), g->h_cellSign.data(), g->h_eI.data(),
+                        g->h_eJ.data(), partition_for(b, g, P), P, k);
+  const TileSetHost &h = c->host;
   TileSetDev &t = c->dev;
   t.P = P;
   t.k = k;
@@ -436,12 +450,26 @@ TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k) {
   t.edges = dupload(c->allocs, h.edges);
   t.ncnt = dupload(c->allocs, h.ncnt);
   t.ecnt = dupload(c->allocs, h.ecnt);
+  t.eown = dupload(c->allocs, h.eown);
   t.cedge = dupload(c->allocs, h.cedge);
   t.eIl = dupload(c->allocs, h.eIl);
   t.eJl = dupload(c->allocs, h.eJl);
   TileCache *out = c.get();
   b->tiles[key] = std::move(c);
   return out;
+}
+
+// The largest k' <= the probe's k whose largest tile fits `budget` bytes of shared memory (0 if none).
+int fitting_k(const TileSetHost &h, size_t budget) {
+  for (int kk = h.k; kk >= 1; kk--) {
+    size_t worst = 0;
+    for (int p = 0; p < h.P; p++) {
+      const size_t nc = h.ncnt[(size_t)p * (h.k + 1) + kk], ne = h.ecnt[(size_t)p * (h.k + 1) + kk];
+      worst = std::max(worst, tile_smem_bytes(nc, ne, h.eown[p]));
+    }
+    if (worst <= budget) return kk;
+  }
+  return 0;
 }
 
 int kernel_lmax(int L) { return L <= 2 ? 2 : L <= 3 ? 3 : L <= 5 ? 5 : 8; }
@@ -454,12 +482,39 @@ void rebuild(isw_batch *b) {
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
   size_t fast_smem = 0;
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
-  // tiles per stack: an even share of the device's tile slots (two tile blocks per SM), by cell count
+  // the tiling: per stack P tiles (its share of the tile slots by cell count) and one exchange interval k for all
+  // stacks, the largest that fits the shared memory of one or of two tile blocks per SM
   long long cells_total = 0;
   int used = 0;
   for (auto &sl : b->slots)
     if (sl.used) { cells_total += sl.layers->grid->d.N; used++; }
-  const int slots_avail = b->sms * 2;
+  std::vector<int> Pbest(b->slots.size(), 0);
+  int kbest = 0;
+  if (b->tiles_enabled && used > 0) {
+    for (int bps = 2; bps >= 1; bps--) {
+      const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
+      const int slots = b->sms * bps;
+      std::vector<int> P(b->slots.size(), 0);
+      int kmin = b->tile_k;
+      bool any = false;
+      for (size_t q = 0; q < b->slots.size(); q++) {
+        const BatchSlot &sl = b->slots[q];
+        if (!sl.used) continue;
+        const int N = sl.layers->grid->d.N;
+        const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
+        if (Pq * 16 > N) continue;             // tiles of at least 16 owned cells
+        const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget);
+        if (kf == 0) continue;
+        P[q] = Pq;
+        kmin = std::min(kmin, kf);
+        any = true;
+      }
+      if (any && kmin > kbest) {
+        kbest = kmin;
+        Pbest = P;
+      }
+    }
+  }
   for (auto &sl : b->slots) {
     if (!sl.used) continue;
     StackDesc d;
@@ -489,18 +544,13 @@ void rebuild(isw_batch *b) {
     }
     const int s = (int)desc.size();
     d.tiled = 0;
-    if (b->tiles_enabled && used > 0) {
-      const int N = sl.layers->grid->d.N;
-      const int P = std::max(1, (int)((long long)slots_avail * N / std::max(1LL, cells_total)));
-      if (P * 16 <= N) {                       // tiles of at least 16 owned cells
-        TileCache *tc = tiles_for(b, sl.layers->grid, P, b->tile_k);
-        if (tc->smem <= SMEM_BUDGET && (int)refs.size() + P <= slots_avail) {
-          d.tiled = 1;
-          d.tiles = tc->dev;
-          fast_smem = std::max(fast_smem, tc->smem);
-          for (int p = 0; p < P; p++) refs.push_back(TileRef{s, p});
-        }
-      }
+    const size_t q = (size_t)(&sl - &b->slots[0]);
+    if (kbest > 0 && Pbest[q] > 0) {
+      TileCache *tc = tiles_for(b, sl.layers->grid, Pbest[q], kbest);
+      d.tiled = 1;
+      d.tiles = tc->dev;
+      fast_smem = std::max(fast_smem, tc->host.smem);
+      for (int p = 0; p < Pbest[q]; p++) refs.push_back(TileRef{s, p});
     }
     if (!d.tiled) any_untiled = 1;
     auto chunks = [&](std::vector<Chunk> &v, int n) {
@@ -509,7 +559,7 @@ void rebuild(isw_batch *b) {
     chunks(cell, d.M.g.N);
     chunks(edge, d.M.g.E);
     chunks(vert, d.M.g.NV);
-    if (d.has_tr) chunks(rows, d.tr.rows * d.M.g.N);
+    if (d.has_tr) chunks(rows, sl.ntr * d.M.g.N);       // (tracer, cell) pairs
     desc.push_back(d);
   }
   b->nstacks = (int)desc.size();
@@ -562,7 +612,8 @@ void rebuild(isw_batch *b) {
   }
   for (int st = 0; st < 3; st++) {
     b->nsub[st] = nsub[st];
-    b->rounds[st] = (nsub[st] + b->tile_k - 1) / b->tile_k;
+    b->rounds[st] = kbest > 0 ? (nsub[st] + kbest - 1) / kbest : 0;
+  b->kused = kbest;
   }
   b->any_nu4 = any_nu4;
   b->any_vmix = any_vmix;
@@ -755,6 +806,18 @@ int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k) {
     b->tiles_enabled = tiles_enabled ? 1 : 0;
     b->tile_k = tile_k;
     b->dirty = true;
+  });
+}
+
+int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes) {
+  return guarded([&] {
+    if (!b || !stacks || !tiles || !tile_k || !smem_bytes) fail(ISW_EINVAL, "batch.info: null argument");
+    ISW_CUDA(cudaSetDevice(b->device));
+    prepare(b);
+    *stacks = b->nstacks;
+    *tiles = b->ntiles;
+    *tile_k = b->ntiles > 0 ? b->kused : 0;
+    *smem_bytes = (long long)b->fast_smem;
   });
 }
 

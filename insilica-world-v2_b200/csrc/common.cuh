@@ -72,4 +72,5 @@ struct isw_grid {
   std::vector<void *> allocs;
   double dmin;                   // smallest edge spacing (Layers.dmin)
   std::vector<int32_t> h_nbr, h_cellEdge, h_eI, h_eJ;   // host copies the fast-loop tiles are built from
+  std::vector<int8_t> h_cellSign;
 };

@@ -184,6 +184,7 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     d.kite32 = upload_f32(g, h->kite, (size_t)N * 6);
     g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
     g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);
+    g->h_cellSign.assign(h->cellSign, h->cellSign + (size_t)N * 6);
     g->h_eI.assign(h->eI, h->eI + E);
     g->h_eJ.assign(h->eJ, h->eJ + E);
     double dmin = h->de[0];

@@ -1,6 +1,8 @@
 // Phase functions of the time-split RK3 step, plain FP64 form: one call per cell, edge or vertex, every layer of the
 // column in one thread. The arithmetic of each phase is the reference kernel's, operation for operation and in the
-// same summation order (compiled with -fmad=false), so results are bit-identical to the reference's FP64 path.
+// same summation order (compiled with -fmad=false), so results are bit-identical to the reference's FP64 path. A cell's
+// six slots are walked fully unrolled with a guard on padded slots instead of an early exit, so the gathers of all its
+// edges can be in flight together; pads only trail, so each sum keeps the reference's order.
 //
 // Phase plan of one step (reference layers.py:185-212 with _stage :129-183, Boussinesq branch):
 //   init     cells: eta0 = b + sum h (layers.cu:33-38)          edges: ubar0 (layers.cu:64-74)
@@ -52,19 +54,20 @@ __device__ __forceinline__ void div_cell(const LayersDev &M, const double *__res
   const GridDev &g = M.g;
   int es[6];
   double c[6];
-  int m = 0;
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = g.cellEdge[i * 6 + s];
     es[s] = e;
-    if (e >= 0) { c[s] = (double)g.cellSign[i * 6 + s] * g.le[e]; m = s + 1; }
+    c[s] = e >= 0 ? (double)g.cellSign[i * 6 + s] * g.le[e] : 0.0;
   }
   const double A = g.areaCell[i];
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const double *ul = u + (size_t)k * g.E;
     double s = 0;
-    for (int t = 0; t < m; t++) s += c[t] * ul[es[t]];
+#pragma unroll
+    for (int t = 0; t < 6; t++)
+      if (es[t] >= 0) s += c[t] * ul[es[t]];
     M.D1[(size_t)k * g.N + i] = s / A;
   }
 }
@@ -115,12 +118,11 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
   for (int k = L - 1; k >= 0; k--) { s += h[(size_t)k * N + i]; z[k] = s; }
   int es[6];
   double c[6];
-  int m = 0;
 #pragma unroll
   for (int t = 0; t < 6; t++) {
     const int e = g.cellEdge[i * 6 + t];
     es[t] = e;
-    if (e >= 0) { c[t] = g.le[e] * g.de[e] * 0.25; m = t + 1; }
+    c[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
   }
   const double A = g.areaCell[i];
   double Mp = 0;
@@ -129,10 +131,12 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
     if (k > 0) Mp += M.gp[k - 1] * z[k];
     const double *ul = u + (size_t)k * E;
     double ke = 0;
-    for (int t = 0; t < m; t++) {
-      const double ue = ul[es[t]];
-      ke += c[t] * ue * ue;
-    }
+#pragma unroll
+    for (int t = 0; t < 6; t++)
+      if (es[t] >= 0) {
+        const double ue = ul[es[t]];
+        ke += c[t] * ue * ue;
+      }
     M.B[(size_t)k * N + i] = Mp + ke / A;
   }
   M.eta[i] = M.eta0[i];
@@ -250,12 +254,14 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, double tau, int 
   const GridDev &g = M.g;
   const double e0 = M.eta[i];
   M.eta_prev[i] = e0;
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
   double div = 0;
 #pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    if (e < 0) break;
-    div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
+    const int e = es[s];
+    if (e >= 0) div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
   }
   M.eta[i] = e0 - (tau * div) / g.areaCell[i];
 }
@@ -279,9 +285,13 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &
   double out[L];
 #pragma unroll
   for (int k = 0; k < L; k++) out[k] = 0;
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdgeAsc[i * 6 + s];
+#pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdgeAsc[i * 6 + s];
-    if (e < 0) break;
+    const int e = es[s];
+    if (e < 0) continue;
     const int ea = g.eI[e], eb = g.eJ[e];
     const bool mine = ea == i;
     const double ubs = M.ubs[e], acc = M.acc[e], le = g.le[e];
@@ -319,9 +329,13 @@ __device__ __forceinline__ void h_cell(const LayersDev &M, const StageArgs &a, i
   double div[L];
 #pragma unroll
   for (int k = 0; k < L; k++) div[k] = 0;
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+#pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    if (e < 0) break;
+    const int e = es[s];
+    if (e < 0) continue;
     const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
 #pragma unroll
     for (int k = 0; k < L; k++) div[k] += c * limited(M, k, e);

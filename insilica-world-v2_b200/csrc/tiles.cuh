@@ -1,14 +1,16 @@
 // Shared-memory tiles for the barotropic fast loop.
 //
 // The fast loop (reference layers.cu:366-388, driven by layers.py:168-175) alternates a cell pass (eta) and an edge pass
-// (ubar) ceil(c nfast) times per stage. Each tile owns a contiguous (Hilbert-ordered) range of cells and the edges whose
-// eI cell it owns, and stages in shared memory its cells out to k rings (ring 0 = owned) and every edge of those cells.
-// It can then advance k sub-steps with no grid-wide sync: sub-step m (1..k) updates eta on cells of ring <= k - m + 1
+// (ubar) ceil(c nfast) times per stage. Each tile owns a compact region of cells (grown breadth-first from a seed, the
+// smallest region growing first, so regions are compact and within a few cells of equal size) and the edges whose eI
+// cell it owns; it stages in shared memory its cells out to k rings (ring 0 = owned) and every edge of those cells. It
+// can then advance k sub-steps with no grid-wide sync: sub-step m (1..k) updates eta on cells of ring <= k - m + 1
 // and ubar on edges whose nearer cell has ring <= k - m, which is exactly what the owned values after k sub-steps
 // depend on. Tiles exchange owned eta and ubar through global memory every k sub-steps (double-buffered, one grid
 // barrier per exchange). Arithmetic is the reference's, per cell and edge, in the same gather order.
 //
-// Local numbering: cells in ring order, edges in order of their nearer cell's ring, so "ring <= r" is a prefix.
+// Local numbering: cells in ring order, edges in order of their nearer cell's ring with the owned edges first, so
+// "ring <= r" is a prefix and the owned edges are [0, eown).
 #pragma once
 #include <stdint.h>
 
@@ -22,16 +24,21 @@ struct TileSetHost {
   std::vector<int32_t> cell_off, edge_off;     // P + 1 offsets
   std::vector<int32_t> cells, edges;           // global ids, tile by tile, local order
   std::vector<int32_t> ncnt, ecnt;             // per tile k + 1 prefix counts: cells of ring <= r, edges of ring <= r
-  std::vector<int16_t> cedge;                  // per local cell 6 local edge ids (-1 pads), cellEdge slot order
+  std::vector<int32_t> eown;                   // per tile: owned edges (eI owned), the first of the local edges
+  std::vector<int16_t> cedge;                  // per local cell 6 slots: +-(local edge + 1), sign = cellSign; 0 pads
   std::vector<int16_t> eIl, eJl;               // per local edge its local cells (-1 outside the tile)
 };
 
-// Per-tile shared-memory bytes: per cell eta, eta_prev, area, Gc, 6 coefficients (8 B each) and 6 local edge ids
-// (2 B); per edge ubar, G, d_e, acc (8 B each) and two local cell ids (2 B).
-inline size_t tile_smem_bytes(size_t nc, size_t ne) { return nc * (4 * 8 + 6 * 8 + 6 * 2) + ne * (4 * 8 + 2 * 2) + 64; }
+// Per-tile shared-memory bytes: per cell eta, eta_prev, area, Gc (8 B each) and 6 signed local edge ids (2 B); per
+// edge ubar, G, d_e, l_e H_e (8 B each) and two local cell ids (2 B); per owned edge the sub-step sum acc (8 B).
+inline size_t tile_smem_bytes(size_t nc, size_t ne, size_t nown) { return nc * (4 * 8 + 6 * 2) + ne * (4 * 8 + 2 * 2) + nown * 8 + 64; }
 
-// Build P tiles over a grid (N cells with neighbour table nbr (N x 6, pads -1), cellEdge (N x 6), eI, eJ (E)).
-TileSetHost build_tiles(int N, int E, const int32_t *nbr, const int32_t *cellEdge, const int32_t *eI, const int32_t *eJ, int P,
-                        int k);
+// Compact balanced partition of the N cells into P regions (owner per cell).
+std::vector<int32_t> partition_cells(int N, const int32_t *nbr, int P);
+
+// Build the tiles of a partition over a grid (neighbour table nbr (N x 6, pads -1), cellEdge and cellSign (N x 6),
+// eI, eJ (E)).
+TileSetHost build_tiles(int N, int E, const int32_t *nbr, const int32_t *cellEdge, const int8_t *cellSign, const int32_t *eI,
+                        const int32_t *eJ, const std::vector<int32_t> &owner, int P, int k);
 
 }  // namespace isw

@@ -5,6 +5,7 @@
 // tracers[j] + l * N (no packed copy). The reference's 8 launches per call (td, 2 x (hflux, stage), aflux, ratios,
 // apply) become 4 cell passes: every 3rd-order edge flux is recomputed by the cell pass that sums it, with the
 // reference's arithmetic, so results are bit-identical:
+// Threads are (tracer, cell) pairs, each over every layer of its tracer (transport_fp64.cuh).
 //   P1  td (fused.cu:146-160) and the first RK stage p1 (fused.cu:163-186, frac 1/3, fluxes of psi)
 //   P2  the second RK stage p2 (frac 1/2, fluxes of p1)
 //   P3  antidiffusive fluxes A (fused.cu:189-194; stored by each edge's eI cell) and the Zalesak ratios (fused.cu:197-222)
@@ -27,28 +28,44 @@ __global__ void __launch_bounds__(THREADS) k_mass(const GridDev g, int L, const 
   M1[(size_t)l * g.N + i] = fp64::mass_cell(g, M0, Fm + (size_t)l * g.E, l, i);
 }
 
-__global__ void __launch_bounds__(THREADS) k_p1(const TransportDev T, const TrArgs a, int order) {
+#define ISW_TR_L(LV, CALL)                              \
+  do {                                                  \
+    switch (LV) {                                       \
+      case 1: { constexpr int LL = 1; CALL; } break;    \
+      case 2: { constexpr int LL = 2; CALL; } break;    \
+      case 3: { constexpr int LL = 3; CALL; } break;    \
+      case 4: { constexpr int LL = 4; CALL; } break;    \
+      case 5: { constexpr int LL = 5; CALL; } break;    \
+      case 6: { constexpr int LL = 6; CALL; } break;    \
+      case 7: { constexpr int LL = 7; CALL; } break;    \
+      case 8: { constexpr int LL = 8; CALL; } break;    \
+      default: break;                                   \
+    }                                                   \
+  } while (0)
+
+// one thread per (tracer j, cell i), every layer of it
+__global__ void __launch_bounds__(THREADS) k_p1(const TransportDev T, const TrArgs a, int ntr, int order) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T.g.N * a.rows) return;
-  fp64::tr_p1(T, a, order, false, t / T.g.N, t % T.g.N);
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_p1<LL>(T, a, order, false, t / T.g.N, t % T.g.N));
 }
 
-__global__ void __launch_bounds__(THREADS) k_p2(const TransportDev T, const TrArgs a) {
+__global__ void __launch_bounds__(THREADS) k_p2(const TransportDev T, const TrArgs a, int ntr) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T.g.N * a.rows) return;
-  fp64::tr_p2(T, a, t / T.g.N, t % T.g.N);
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_p2<LL>(T, a, t / T.g.N, t % T.g.N));
 }
 
-__global__ void __launch_bounds__(THREADS) k_p3(const TransportDev T, const TrArgs a) {
+__global__ void __launch_bounds__(THREADS) k_p3(const TransportDev T, const TrArgs a, int ntr) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T.g.N * a.rows) return;
-  fp64::tr_p3(T, a, t / T.g.N, t % T.g.N);
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_p3<LL>(T, a, t / T.g.N, t % T.g.N));
 }
 
-__global__ void __launch_bounds__(THREADS) k_p4(const TransportDev T, const TrArgs a) {
+__global__ void __launch_bounds__(THREADS) k_p4(const TransportDev T, const TrArgs a, int ntr) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T.g.N * a.rows) return;
-  fp64::tr_p4(T, a, t / T.g.N, t % T.g.N);
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_p4<LL>(T, a, t / T.g.N, t % T.g.N));
 }
 
 // order 1: td out
@@ -152,14 +169,14 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
       a.tr[j] = tracers[j];
     }
     cudaStream_t st = (cudaStream_t)stream;
-    const int nb = blocks_for((long long)t->d.g.N * a.rows);
-    k_p1<<<nb, THREADS, 0, st>>>(t->d, a, order);
+    const int nb = blocks_for((long long)t->d.g.N * ntr);
+    k_p1<<<nb, THREADS, 0, st>>>(t->d, a, ntr, order);
     if (order == 1) {
-      k_td_out<<<nb, THREADS, 0, st>>>(t->d, a);
+      k_td_out<<<blocks_for((long long)t->d.g.N * a.rows), THREADS, 0, st>>>(t->d, a);
     } else {
-      k_p2<<<nb, THREADS, 0, st>>>(t->d, a);
-      k_p3<<<nb, THREADS, 0, st>>>(t->d, a);
-      k_p4<<<nb, THREADS, 0, st>>>(t->d, a);
+      k_p2<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
+      k_p3<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
+      k_p4<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
     }
     ISW_CUDA(cudaGetLastError());
   });

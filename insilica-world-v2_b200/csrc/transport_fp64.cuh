@@ -1,10 +1,14 @@
-// Phase functions of the FCT transport step, plain FP64 form (reference kernels/fused.cu:122-241, trisk.cu:48-59): one
-// call per (row, cell), rows y = tracer j * L + layer l. Each 3rd-order edge flux is recomputed by the cell pass that
-// sums it, with the reference's arithmetic (compiled with -fmad=false), so results are bit-identical.
-//   P1  receiving mass M1 (trisk.cu:48-59, stored by the j = 0 rows), td (fused.cu:146-160) and p1 (fused.cu:163-186)
+// Phase functions of the FCT transport step, plain FP64 form (reference kernels/fused.cu:122-241, trisk.cu:48-59).
+// Rows y = tracer j * L + layer l, as the reference stacks them. One call handles one (tracer, cell) and every layer of
+// it: a cell's six edges and their 3rd-order stencils are loaded once and used for all L rows of the tracer. Each
+// 3rd-order edge flux is recomputed by the cell pass that sums it, with the reference's arithmetic (compiled with
+// -fmad=false), and each row's sums keep the reference's edge order, so results are bit-identical.
+//   P1  receiving mass M1 (trisk.cu:48-59, stored by tracer 0), td (fused.cu:146-160) and p1 (fused.cu:163-186)
 //   P2  p2 (frac 1/2 from p1)
 //   P3  antidiffusive fluxes A (fused.cu:189-194; stored by each edge's eI cell) and Zalesak ratios (fused.cu:197-222)
 //   P4  the limited update (fused.cu:225-241) into the caller's tracer arrays
+// Gathers walk a cell's six slots fully unrolled with a guard on the padded slot (no early exit), so the loads of all
+// six edges can be in flight together; pads only ever trail, so the order of the sums is unchanged.
 #pragma once
 #include "common.cuh"
 
@@ -26,22 +30,38 @@ struct TrArgs {
 
 namespace fp64 {
 
-__device__ __forceinline__ double upwind(const double *__restrict__ Fml, const double *__restrict__ p, const int *eI, const int *eJ,
-                                         int e) {
-  const double f = Fml[e];
-  return f * (f >= 0 ? p[eI[e]] : p[eJ[e]]);
+__device__ __forceinline__ double upwind_v(double f, double pi, double pj) { return f * (f >= 0 ? pi : pj); }
+
+// The 3rd-order flux of edge e (reference fused.cu:131-138, FP64 form: the stencil reads the 64-bit field itself),
+// given the edge's stencil cells idx[8] and weights wt[8].
+__device__ __forceinline__ double hoflux_s(double f, const double *__restrict__ ps, const int *idx, const double *wt, int a, int b,
+                                           double beta) {
+  const double x = wt[0] * ps[idx[0]] + wt[1] * ps[idx[1]] + wt[2] * ps[idx[2]] + wt[3] * ps[idx[3]];
+  const double y = wt[4] * ps[idx[4]] + wt[5] * ps[idx[5]] + wt[6] * ps[idx[6]] + wt[7] * ps[idx[7]];
+  return f * (0.5 * (ps[a] + ps[b]) - (x + y)) + fabs(f) * ((y - x) * beta);
 }
 
-// reference fused.cu:131-138, FP64 form (the stencil reads the 64-bit field itself)
-__device__ __forceinline__ double hoflux(const GridDev &g, const double *__restrict__ Fml, const double *__restrict__ ps, int e,
-                                         double beta) {
-  const double f = Fml[e];
-  const int o = e * 8;
-  const int *idx = g.d2idx;
-  const double *wt = g.d2wt;
-  const double a = wt[o] * ps[idx[o]] + wt[o + 1] * ps[idx[o + 1]] + wt[o + 2] * ps[idx[o + 2]] + wt[o + 3] * ps[idx[o + 3]];
-  const double b = wt[o + 4] * ps[idx[o + 4]] + wt[o + 5] * ps[idx[o + 5]] + wt[o + 6] * ps[idx[o + 6]] + wt[o + 7] * ps[idx[o + 7]];
-  return f * (0.5 * (ps[g.eI[e]] + ps[g.eJ[e]]) - (a + b)) + fabs(f) * ((b - a) * beta);
+// A cell's edges in ascending edge order (cellEdgeAsc), with their two cells.
+struct CellEdges {
+  int e[6], a[6], b[6];
+};
+
+__device__ __forceinline__ void load_edges(const GridDev &g, int i, CellEdges &c) {
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdgeAsc[i * 6 + s];
+    c.e[s] = e;
+    c.a[s] = e >= 0 ? g.eI[e] : 0;
+    c.b[s] = e >= 0 ? g.eJ[e] : 0;
+  }
+}
+
+__device__ __forceinline__ void load_stencil(const GridDev &g, int e, int *idx, double *wt) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    idx[q] = g.d2idx[e * 8 + q];
+    wt[q] = g.d2wt[e * 8 + q];
+  }
 }
 
 // reference trisk.cu:48-59
@@ -55,110 +75,179 @@ __device__ __forceinline__ double mass_cell(const GridDev &g, const double *__re
   return m;
 }
 
-// P1 for (row y, cell i); with_mass: compute M1 here (rows of tracer 0 store it) instead of reading it
-__device__ __forceinline__ void tr_p1(const TransportDev &T, const TrArgs &a, int order, bool with_mass, int y, int i) {
+// P1 for (tracer j, cell i), every layer; with_mass: compute M1 here (tracer 0 stores it) instead of reading it
+template <int L>
+__device__ __forceinline__ void tr_p1(const TransportDev &T, const TrArgs &a, int order, bool with_mass, int j, int i) {
   const GridDev &g = T.g;
-  const int l = y % a.L, j = y / a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *p = a.tr[j] + (size_t)l * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
-  double m1;
-  if (with_mass) {
-    m1 = mass_cell(g, a.M0, Fml, l, i);
-    if (j == 0) a.M1[om] = m1;
-  } else {
-    m1 = a.M1[om];
+  const int N = g.N, E = g.E;
+  CellEdges c;
+  load_edges(g, i, c);
+  double m1[L], td[L], s[L], mx[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i;
+    const double m0 = a.M0[om], pi = a.tr[j][om];
+    T.psi0[(size_t)(j * L + l) * N + i] = pi;
+    m1[l] = m0;
+    td[l] = m0 * pi;
+    s[l] = m0 * pi;
+    mx[l] = m0;
   }
-  const double pi = p[i];
-  T.psi0[o] = pi;
-  const double m0 = a.M0[om];
-  double td = m0 * pi;
-  double s = m0 * pi, mx = m0;
   const double frac = 1.0 / 3.0;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const bool out = g.eI[e] == i;
-    const double fu = upwind(Fml, p, g.eI, g.eJ, e);
-    if (out) td -= fu; else td += fu;
-    if (order != 1) {
-      const double f = frac * hoflux(g, Fml, p, e, a.beta);
-      const double m = frac * Fml[e];
-      if (out) { s -= f; mx -= m; } else { s += f; mx += m; }
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int e = c.e[q];
+    if (e >= 0) {
+      const bool out = c.a[q] == i;
+      int idx[8];
+      double wt[8];
+      if (order != 1) load_stencil(g, e, idx, wt);
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const double *p = a.tr[j] + (size_t)l * N;
+        const double f = a.Fm[(size_t)l * E + e];
+        if (with_mass) { if (out) m1[l] -= f; else m1[l] += f; }
+        const double fu = upwind_v(f, p[c.a[q]], p[c.b[q]]);
+        if (out) td[l] -= fu; else td[l] += fu;
+        if (order != 1) {
+          const double hf = frac * hoflux_s(f, p, idx, wt, c.a[q], c.b[q], a.beta);
+          const double m = frac * f;
+          if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
+        }
+      }
     }
   }
-  T.td[o] = td / m1;
-  if (order != 1) T.p1[o] = s / mx;
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
+    double mm = m1[l];
+    if (with_mass) { if (j == 0) a.M1[om] = mm; }
+    else mm = a.M1[om];
+    T.td[o] = td[l] / mm;
+    if (order != 1) T.p1[o] = s[l] / mx[l];
+  }
 }
 
-__device__ __forceinline__ void tr_p2(const TransportDev &T, const TrArgs &a, int y, int i) {
+template <int L>
+__device__ __forceinline__ void tr_p2(const TransportDev &T, const TrArgs &a, int j, int i) {
   const GridDev &g = T.g;
-  const int l = y % a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *p1 = T.p1 + (size_t)y * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
+  const int N = g.N, E = g.E;
+  CellEdges c;
+  load_edges(g, i, c);
+  double s[L], mx[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
+    s[l] = a.M0[om] * T.psi0[o];
+    mx[l] = a.M0[om];
+  }
   const double frac = 1.0 / 2.0;
-  double s = a.M0[om] * T.psi0[o], mx = a.M0[om];
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double f = frac * hoflux(g, Fml, p1, e, a.beta);
-    const double m = frac * Fml[e];
-    if (g.eI[e] == i) { s -= f; mx -= m; } else { s += f; mx += m; }
-  }
-  T.p2[o] = s / mx;
-}
-
-__device__ __forceinline__ void tr_p3(const TransportDev &T, const TrArgs &a, int y, int i) {
-  const GridDev &g = T.g;
-  const int l = y % a.L;
-  const double *p = T.psi0 + (size_t)y * g.N;
-  const double *tt = T.td + (size_t)y * g.N;
-  const double *p2 = T.p2 + (size_t)y * g.N;
-  const double *Fml = a.Fm + (size_t)l * g.E;
-  double hi = fmax(p[i], tt[i]), lo = fmin(p[i], tt[i]);
-  for (int k = 0; k < 6; k++) {
-    const int j = g.nbr[i * 6 + k];
-    if (j < 0) break;
-    hi = fmax(hi, fmax(p[j], tt[j]));
-    lo = fmin(lo, fmin(p[j], tt[j]));
-  }
-  const double m1 = a.M1[(size_t)l * g.N + i];
-  const double qmax = (hi - tt[i]) * m1, qmin = (tt[i] - lo) * m1;
-  double Pp = 0, Pm = 0;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double A = hoflux(g, Fml, p2, e, a.beta) - upwind(Fml, p, g.eI, g.eJ, e);
-    if (g.eI[e] == i) {
-      T.A[(size_t)y * g.E + e] = A;
-      if (A > 0) Pm += A; else Pp -= A;
-    } else {
-      if (A > 0) Pp += A; else Pm -= A;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int e = c.e[q];
+    if (e >= 0) {
+      const bool out = c.a[q] == i;
+      int idx[8];
+      double wt[8];
+      load_stencil(g, e, idx, wt);
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const double *p1 = T.p1 + (size_t)(j * L + l) * N;
+        const double f = a.Fm[(size_t)l * E + e];
+        const double hf = frac * hoflux_s(f, p1, idx, wt, c.a[q], c.b[q], a.beta);
+        const double m = frac * f;
+        if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
+      }
     }
   }
-  T.Rp[(size_t)y * g.N + i] = Pp > 0 ? fmin(1.0, qmax / Pp) : 0.0;
-  T.Rm[(size_t)y * g.N + i] = Pm > 0 ? fmin(1.0, qmin / Pm) : 0.0;
+#pragma unroll
+  for (int l = 0; l < L; l++) T.p2[(size_t)(j * L + l) * N + i] = s[l] / mx[l];
 }
 
-__device__ __forceinline__ void tr_p4(const TransportDev &T, const TrArgs &a, int y, int i) {
+template <int L>
+__device__ __forceinline__ void tr_p3(const TransportDev &T, const TrArgs &a, int j, int i) {
   const GridDev &g = T.g;
-  const int l = y % a.L, j = y / a.L;
-  const size_t o = (size_t)y * g.N + i, om = (size_t)l * g.N + i;
-  const double *Al = T.A + (size_t)y * g.E;
-  const double *rp = T.Rp + (size_t)y * g.N;
-  const double *rm = T.Rm + (size_t)y * g.N;
-  const double m1 = a.M1[om];
-  double s = T.td[o] * m1;
-  for (int k = 0; k < 6; k++) {
-    const int e = g.cellEdgeAsc[i * 6 + k];
-    if (e < 0) break;
-    const double A = Al[e];
-    const int ea = g.eI[e], eb = g.eJ[e];
-    const double c = A > 0 ? fmin(rp[eb], rm[ea]) : fmin(rp[ea], rm[eb]);
-    if (ea == i) s -= c * A; else s += c * A;
+  const int N = g.N, E = g.E;
+  CellEdges c;
+  load_edges(g, i, c);
+  int nb[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) nb[q] = g.nbr[i * 6 + q];
+  double Pp[L], Pm[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) { Pp[l] = 0; Pm[l] = 0; }
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int e = c.e[q];
+    if (e >= 0) {
+      const bool out = c.a[q] == i;
+      int idx[8];
+      double wt[8];
+      load_stencil(g, e, idx, wt);
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const size_t row = (size_t)(j * L + l);
+        const double *p = T.psi0 + row * N;
+        const double *p2 = T.p2 + row * N;
+        const double f = a.Fm[(size_t)l * E + e];
+        const double A = hoflux_s(f, p2, idx, wt, c.a[q], c.b[q], a.beta) - upwind_v(f, p[c.a[q]], p[c.b[q]]);
+        if (out) {
+          T.A[row * E + e] = A;
+          if (A > 0) Pm[l] += A; else Pp[l] -= A;
+        } else {
+          if (A > 0) Pp[l] += A; else Pm[l] -= A;
+        }
+      }
+    }
   }
-  a.tr[j][(size_t)l * g.N + i] = s / m1;
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t row = (size_t)(j * L + l);
+    const double *p = T.psi0 + row * N;
+    const double *tt = T.td + row * N;
+    const double ti = tt[i];
+    double hi = fmax(p[i], ti), lo = fmin(p[i], ti);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int jn = nb[q];
+      if (jn >= 0) {
+        hi = fmax(hi, fmax(p[jn], tt[jn]));
+        lo = fmin(lo, fmin(p[jn], tt[jn]));
+      }
+    }
+    const double m1 = a.M1[(size_t)l * N + i];
+    const double qmax = (hi - ti) * m1, qmin = (ti - lo) * m1;
+    T.Rp[row * N + i] = Pp[l] > 0 ? fmin(1.0, qmax / Pp[l]) : 0.0;
+    T.Rm[row * N + i] = Pm[l] > 0 ? fmin(1.0, qmin / Pm[l]) : 0.0;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void tr_p4(const TransportDev &T, const TrArgs &a, int j, int i) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  CellEdges c;
+  load_edges(g, i, c);
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t row = (size_t)(j * L + l), om = (size_t)l * N + i;
+    const double *Al = T.A + row * E;
+    const double *rp = T.Rp + row * N;
+    const double *rm = T.Rm + row * N;
+    const double m1 = a.M1[om];
+    double s = T.td[row * N + i] * m1;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int e = c.e[q];
+      if (e >= 0) {
+        const double A = Al[e];
+        const int ea = c.a[q], eb = c.b[q];
+        const double cc = A > 0 ? fmin(rp[eb], rm[ea]) : fmin(rp[ea], rm[eb]);
+        if (ea == i) s -= cc * A; else s += cc * A;
+      }
+    }
+    a.tr[j][om] = s / m1;
+  }
 }
 
 }  // namespace fp64

@@ -41,9 +41,16 @@ class Batch:
         _lib.check(_lib.isw_batch_remove(self._h, int(slot)))
         self._keep.pop(slot, None)
 
-    def config(self, tiles=True, tile_k=4):
-        """The fast loop in shared-memory tiles exchanging every tile_k sub-steps (or grid-wide passes)."""
+    def config(self, tiles=True, tile_k=8):
+        """The fast loop in shared-memory tiles exchanging every k <= tile_k sub-steps (the largest that fits), or
+        grid-wide passes."""
         _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k)))
+
+    def info(self):
+        """(stacks, tiles, exchange interval k, tile shared memory bytes) of the current layout."""
+        st, ti, k, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        _lib.check(_lib.isw_batch_info(self._h, ctypes.byref(st), ctypes.byref(ti), ctypes.byref(k), ctypes.byref(sm)))
+        return dict(stacks=st.value, tiles=ti.value, tile_k=k.value, smem=sm.value)
 
     def step(self, stream=None):
         _lib.check(_lib.isw_batch_step(self._h, stream_of(self.device, stream)))

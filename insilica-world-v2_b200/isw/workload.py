@@ -81,7 +81,14 @@ class Member:
         return [a for s in self.stacks for a in s.state()]
 
     def launches(self):
-        return 1 if self.batch is not None else sum(s.launches() for s in self.stacks)
+        """Kernels one step launches (in the batched case, the step graph's kernels, shared with the batch's other
+        members)."""
+        if self.batch is None:
+            return sum(s.launches() for s in self.stacks)
+        info = self.batch.info()
+        n = sum(max(1, int(np.ceil(c * self.stacks[0].nfast))) for c in (1 / 3, 1 / 2, 1.0))
+        nu4 = any(s.core.nu4 for s in self.stacks)
+        return 1 + (3 if nu4 else 0) + 3 * 5 + (3 if info['tiles'] else 2 * n) + 4
 
 
 def planet_grid(g, omega=cases.OMEGA_EARTH):

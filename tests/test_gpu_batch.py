@@ -155,6 +155,8 @@ def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
     tiled.config(tiles=True, tile_k=k)
     flat.config(tiles=False)
     a, b, c = Member(dg, 9, batch=tiled), Member(dg, 9, batch=flat), Member(dg, 9)
+    info = tiled.info()
+    assert info['tiles'] > 0 and 1 <= info['tile_k'] <= k
     for _ in range(3):
         tiled.step()
         flat.step()
