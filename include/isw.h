@@ -110,6 +110,12 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
 
 /* Deterministic sum of x[0..n) (or of x * y): the reference's fixed tree; synchronises `stream`, writes *out. */
 int isw_dsum(const double *x, const double *y, long long n, double *out, void *stream);
+/* The same sum (bit-identical to isw_dsum) for callers that cannot allocate device memory at the call: no counterpart in
+ * the reference. It allocates nothing: its pass scratch is a fixed file-scope device array, so n is limited to
+ * 134217728 values (larger n is rejected with ISW_EINVAL). *out is a DEVICE pointer, written on `stream` without
+ * synchronising. The first call on each device looks up the array's device address (make it before any stream
+ * capture); calls share the array, so calls that overlap on the GPU race and must be serialised. */
+int isw_dsum_static(const double *x, const double *y, long long n, double *out, void *stream);
 
 /* Batched step: stacks (a Layers handle with its state h, u, Fm, and optionally a Transport with M, M1 and tracers)
  * registered once, then advanced together by isw_batch_step in ONE persistent cooperative launch per step: the RK3 step,

@@ -3,6 +3,8 @@
 // x[base + t + 256 k] for k = 0..7 in order, then the 256 partial sums halve pairwise, s[t] += s[t + h] for
 // h = 128, 64, 32 through shared memory and h = 16 .. 1 by warp shuffles (the same additions in the same order).
 // Passes repeat over the block sums until one value remains; all passes are queued at once (the sizes are known).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace isw {
@@ -88,6 +90,63 @@ extern "C" int isw_dsum(const double *x, const double *y, long long n, double *o
     }
     ISW_CUDA(cudaFreeAsync(buf, st));
     ISW_CUDA(cudaStreamSynchronize(st));
+    return ISW_OK;
+  } catch (const Error &e) {
+    set_last_error(e.msg);
+    return e.status;
+  }
+}
+
+// ---- The deterministic sum without any allocation ----
+//
+// For callers that cannot allocate device memory when they sum: code running while a CUDA graph is being captured
+// (an allocation there is either refused or recorded into the graph), hosts that reserve all device memory up front
+// and forbid later cudaMalloc calls (an embedding framework with its own memory pool, a real-time loop that must not
+// stall on the allocator), and plugins whose host owns the device heap. The passes' partial sums live in one file-scope
+// device array of a fixed size, sized for sums of up to 134,217,728 values (2^27). Every GPU that loads this library
+// holds the array until the process exits.
+//
+// In host code `g_dsum_static` is only a host-side stand-in for the device array, never a device address: the address
+// is looked up with cudaGetSymbolAddress once per device, on the first call made with that device current (so that first
+// call should come before any stream capture). Every call shares the array and finds in it what the last call left:
+// each pass writes every partial sum it later reads, so nothing needs clearing, but calls whose work overlaps on the
+// GPU (different streams, or different host threads on one device) race on the array and must be serialised.
+namespace isw {
+namespace {
+
+constexpr long long DSUM_STATIC_MAX_N = 1LL << 27;                // 134,217,728 values
+constexpr long long DSUM_STATIC_SCRATCH = 65536 + 32 + 8;          // dsum_scratch(DSUM_STATIC_MAX_N), with room to spare
+constexpr int DSUM_STATIC_DEVICES = 64;
+
+static __device__ __align__(256) double g_dsum_static[DSUM_STATIC_SCRATCH];
+
+std::mutex g_dsum_static_mu;
+double *g_dsum_static_addr[DSUM_STATIC_DEVICES] = {};
+
+double *dsum_static_scratch() {
+  int dev = -1;
+  ISW_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= DSUM_STATIC_DEVICES) fail(ISW_EINVAL, "dsum_static: device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_dsum_static_mu);
+  if (!g_dsum_static_addr[dev]) {
+    double *p = nullptr;
+    ISW_CUDA(cudaGetSymbolAddress((void **)&p, g_dsum_static));
+    if (!p) fail(ISW_ECUDA, "dsum_static: no device address for the scratch array");
+    g_dsum_static_addr[dev] = p;
+  }
+  return g_dsum_static_addr[dev];
+}
+
+}  // namespace
+}  // namespace isw
+
+extern "C" int isw_dsum_static(const double *x, const double *y, long long n, double *out, void *stream) {
+  try {
+    if (!x || !out) fail(ISW_EINVAL, "dsum_static: null argument");
+    if (n < 1) fail(ISW_EINVAL, "dsum_static: n must be >= 1");
+    if (n > DSUM_STATIC_MAX_N) fail(ISW_EINVAL, "dsum_static: n exceeds the 134217728 values its fixed scratch holds; use isw_dsum");
+    if (dsum_scratch(n) > DSUM_STATIC_SCRATCH) fail(ISW_EINVAL, "dsum_static: scratch too small for n");
+    dsum_enqueue(x, y, n, dsum_static_scratch(), out, (cudaStream_t)stream);
     return ISW_OK;
   } catch (const Error &e) {
     set_last_error(e.msg);

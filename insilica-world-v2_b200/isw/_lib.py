@@ -54,6 +54,7 @@ isw_transport_destroy = _sig('isw_transport_destroy', I, [P])
 isw_transport_mass_after = _sig('isw_transport_mass_after', I, [P, P, P, P, P])
 isw_transport_step_many = _sig('isw_transport_step_many', I, [P, P, P, P, ctypes.POINTER(P), I, I, P])
 isw_dsum = _sig('isw_dsum', I, [P, P, LL, ctypes.POINTER(D), P])
+isw_dsum_static = _sig('isw_dsum_static', I, [P, P, LL, P, P])
 isw_mesh_build = _sig('isw_mesh_build', I, [I, I, I, I, P, ctypes.POINTER(P)])
 isw_mesh_get = _sig('isw_mesh_get', I, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(I)])
 isw_mesh_destroy = _sig('isw_mesh_destroy', I, [P])
