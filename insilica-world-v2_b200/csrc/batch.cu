@@ -33,12 +33,12 @@
 namespace isw {
 namespace {
 
-constexpr int FAST_THREADS = 512;
 
 struct TileSetDev {
   int P, k;
   const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt, *eown;
   const int16_t *cedge, *eIl, *eJl;
+  const double *ade, *ale, *aarea;            // d_e, l_e per local edge and the area per local cell, in local order
 };
 
 struct StackDesc {
@@ -241,9 +241,10 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
 // Exchange buffers (the owned values each round publishes, double-buffered by round parity): eta / eta_prev for the
 // surface and ub2 / F for the barotropic wind (F, the layer fluxes, is not in use during the fast loop). The final
 // barotropic wind and its accumulated sum go to ub and acc, which no round reads.
-__global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
-                                                         int rounds, GridBarrier *bar, int *status, long long timeout_ns,
-                                                         int fault_block) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
+                                                    int rounds, GridBarrier *bar, int *status, long long timeout_ns,
+                                                    int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileRef tr = refs[blockIdx.x];
   const StackDesc &d = S[tr.s];
@@ -277,17 +278,16 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
     const int gi = cells[c];
     eta[c] = M.eta0[gi];
-    area[c] = g.areaCell[gi];
+    area[c] = T.aarea[c0 + c];
     gc[c] = M.Gc[gi];
-#pragma unroll
-    for (int s = 0; s < 6; s++) cedge[c * 6 + s] = T.cedge[(size_t)(c0 + c) * 6 + s];
   }
+  for (int w = threadIdx.x; w < nc * 6; w += blockDim.x) cedge[w] = T.cedge[(size_t)c0 * 6 + w];
   for (int e = threadIdx.x; e < ne; e += blockDim.x) {
     const int ge = edges[e];
     ub[e] = M.ub0[ge];
     G[e] = M.G[ge];
-    de[e] = g.de[ge];
-    lh[e] = g.le[ge] * M.He[ge];
+    de[e] = T.ade[e0 + e];
+    lh[e] = T.ale[e0 + e] * M.He[ge];
     if (e < eown) acc[e] = 0.0;
     eIl[e] = T.eIl[e0 + e];
     eJl[e] = T.eJl[e0 + e];
@@ -300,8 +300,9 @@ __global__ void __launch_bounds__(FAST_THREADS, 2) k_fast(const StackDesc *__res
       if (K > 0) {                         // round r reads what round r - 1 published: buffer (r - 1) & 1
         const double *xe = ((r - 1) & 1) ? M.eta_prev : M.eta;
         const double *xu = ((r - 1) & 1) ? M.F : M.ub2;
-        for (int c = threadIdx.x; c < nc; c += blockDim.x) eta[c] = xe[cells[c]];
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) ub[e] = xu[edges[e]];
+        // only the halo: the owned cells and edges already hold exactly what was published
+        for (int c = nown + threadIdx.x; c < nc; c += blockDim.x) eta[c] = xe[cells[c]];
+        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) ub[e] = xu[edges[e]];
       }
     }
     __syncthreads();
@@ -383,6 +384,7 @@ struct isw_batch {
   int lmax = 1, nstacks = 0, ntiles = 0, rounds[3] = {0, 0, 0}, nsub[3] = {0, 0, 0}, kused = 0;
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0;
   size_t fast_smem = 0;
+  int fast_bps = 2;                           // tile blocks per SM: 2 (512 threads each) or 1 (1024 threads)
   GridBarrier *bar = nullptr;
   int *status = nullptr;
   int tile_k = 8;
@@ -454,6 +456,12 @@ TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k) {
   t.cedge = dupload(c->allocs, h.cedge);
   t.eIl = dupload(c->allocs, h.eIl);
   t.eJl = dupload(c->allocs, h.eJl);
+  std::vector<double> ade(h.edges.size()), ale(h.edges.size()), aarea(h.cells.size());
+  for (size_t q = 0; q < h.edges.size(); q++) { ade[q] = g->h_de[h.edges[q]]; ale[q] = g->h_le[h.edges[q]]; }
+  for (size_t q = 0; q < h.cells.size(); q++) aarea[q] = g->h_areaCell[h.cells[q]];
+  t.ade = dupload(c->allocs, ade);
+  t.ale = dupload(c->allocs, ale);
+  t.aarea = dupload(c->allocs, aarea);
   TileCache *out = c.get();
   b->tiles[key] = std::move(c);
   return out;
@@ -489,7 +497,7 @@ void rebuild(isw_batch *b) {
   for (auto &sl : b->slots)
     if (sl.used) { cells_total += sl.layers->grid->d.N; used++; }
   std::vector<int> Pbest(b->slots.size(), 0);
-  int kbest = 0;
+  int kbest = 0, bps_best = 2;
   if (b->tiles_enabled && used > 0) {
     for (int bps = 2; bps >= 1; bps--) {
       const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
@@ -511,6 +519,7 @@ void rebuild(isw_batch *b) {
       }
       if (any && kmin > kbest) {
         kbest = kmin;
+        bps_best = bps;
         Pbest = P;
       }
     }
@@ -599,10 +608,12 @@ void rebuild(isw_batch *b) {
   sc.nrows = (int)rows.size();
   b->ntiles = (int)refs.size();
   b->fast_smem = fast_smem;
+  b->fast_bps = bps_best;
   if (b->ntiles > 0) {                      // every tile block must be resident at once (cooperative launch)
-    if (fast_smem > 48 * 1024) ISW_CUDA(cudaFuncSetAttribute(k_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_smem));
+    const void *fn = bps_best == 2 ? (const void *)k_fast<512, 2> : (const void *)k_fast<1024, 1>;
+    if (fast_smem > 48 * 1024) ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_smem));
     int per = 0;
-    ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fast, FAST_THREADS, fast_smem));
+    ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, bps_best == 2 ? 512 : 1024, fast_smem));
     if ((long long)per * b->sms < b->ntiles) {
       b->ntiles = 0;
       any_untiled = 1;
@@ -641,7 +652,7 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
   ISW_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), st));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)b->ntiles);
-  cfg.blockDim = dim3(FAST_THREADS);
+  cfg.blockDim = dim3(b->fast_bps == 2 ? 512 : 1024);
   cfg.dynamicSmemBytes = b->fast_smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -649,8 +660,12 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast, (const StackDesc *)b->d_desc, (const TileRef *)b->d_refs, stage, b->rounds[stage],
-                              b->bar, b->status, timeout_ns, fault_block));
+  if (b->fast_bps == 2)
+    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<512, 2>, (const StackDesc *)b->d_desc, (const TileRef *)b->d_refs, stage,
+                                b->rounds[stage], b->bar, b->status, timeout_ns, fault_block));
+  else
+    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<1024, 1>, (const StackDesc *)b->d_desc, (const TileRef *)b->d_refs, stage,
+                                b->rounds[stage], b->bar, b->status, timeout_ns, fault_block));
 }
 
 // The launches of one step, in order.
@@ -685,8 +700,6 @@ void enqueue(isw_batch *b, cudaStream_t st) {
 
 void prepare(isw_batch *b) {
   if (b->dirty) rebuild(b);
-  if (b->fast_smem > 48 * 1024)
-    ISW_CUDA(cudaFuncSetAttribute(k_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->fast_smem));
 }
 
 void step(isw_batch *b, cudaStream_t st) {

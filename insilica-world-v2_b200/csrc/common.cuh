@@ -73,4 +73,5 @@ struct isw_grid {
   double dmin;                   // smallest edge spacing (Layers.dmin)
   std::vector<int32_t> h_nbr, h_cellEdge, h_eI, h_eJ;   // host copies the fast-loop tiles are built from
   std::vector<int8_t> h_cellSign;
+  std::vector<double> h_de, h_le, h_areaCell;
 };

@@ -138,8 +138,12 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
   check_range(h->eoe, nE2, 0, E, false, "eoe");
   for (int i = 0; i < N; i++)
     if (h->deg[i] < 3 || h->deg[i] > 6) fail(ISW_EINVAL, "grid: deg outside [3, 6]");
-  for (int e = 0; e < E; e++)
+  for (int e = 0; e < E; e++) {
     if (h->eKi[e] >= h->deg[h->eI[e]] || h->eKj[e] >= h->deg[h->eJ[e]]) fail(ISW_EINVAL, "grid: eKi/eKj outside the cell's slots");
+    // each edge sits at its cells' slots eKi, eKj (the transport stencil relies on it: [eI, eJ, ... | eJ, eI, ...])
+    if (h->nbr[h->eI[e] * 6 + h->eKi[e]] != h->eJ[e] || h->nbr[h->eJ[e] * 6 + h->eKj[e]] != h->eI[e])
+      fail(ISW_EINVAL, "grid: nbr at eKi/eKj does not name the edge's other cell");
+  }
   for (int i = 0; i < N; i++)     // the stencil reads nbr at slots < deg
     for (int k = 0; k < h->deg[i]; k++)
       if (h->nbr[i * 6 + k] < 0) fail(ISW_EINVAL, "grid: nbr pad inside deg");
@@ -185,6 +189,9 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
     g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);
     g->h_cellSign.assign(h->cellSign, h->cellSign + (size_t)N * 6);
+    g->h_de.assign(h->de, h->de + E);
+    g->h_le.assign(h->le, h->le + E);
+    g->h_areaCell.assign(h->areaCell, h->areaCell + N);
     g->h_eI.assign(h->eI, h->eI + E);
     g->h_eJ.assign(h->eJ, h->eJ + E);
     double dmin = h->de[0];

@@ -32,13 +32,36 @@ namespace fp64 {
 
 __device__ __forceinline__ double upwind_v(double f, double pi, double pj) { return f * (f >= 0 ? pi : pj); }
 
-// The 3rd-order flux of edge e (reference fused.cu:131-138, FP64 form: the stencil reads the 64-bit field itself),
-// given the edge's stencil cells idx[8] and weights wt[8].
-__device__ __forceinline__ double hoflux_s(double f, const double *__restrict__ ps, const int *idx, const double *wt, int a, int b,
+// The 3rd-order stencil of an edge (csrc/grid.cu d2_stencil, reference gpu.py:86-108) is, by construction,
+// [eI, eJ, o1, o2 | eJ, eI, o1', o2']: each side's cell, the other cell, and two cells opposite (the same cell twice
+// on a hexagon, its weight split in halves). So an edge's flux needs the field at eI, eJ and at most four other cells;
+// each distinct value is loaded once and enters the reference's expression in the reference's positions.
+struct Stencil {
+  int o[4];          // idx[2], idx[3], idx[6], idx[7]
+  double wt[8];
+};
+
+__device__ __forceinline__ void load_stencil(const GridDev &g, int e, Stencil &st) {
+  st.o[0] = g.d2idx[e * 8 + 2];
+  st.o[1] = g.d2idx[e * 8 + 3];
+  st.o[2] = g.d2idx[e * 8 + 6];
+  st.o[3] = g.d2idx[e * 8 + 7];
+#pragma unroll
+  for (int q = 0; q < 8; q++) st.wt[q] = g.d2wt[e * 8 + q];
+}
+
+// The 3rd-order flux of an edge (reference fused.cu:131-138, FP64 form: the stencil reads the 64-bit field itself):
+// f (mean - a - b) + |f| (b - a) beta, with pa = field at eI, pb = field at eJ.
+__device__ __forceinline__ double hoflux_s(double f, const double *__restrict__ ps, const Stencil &st, double pa, double pb,
                                            double beta) {
-  const double x = wt[0] * ps[idx[0]] + wt[1] * ps[idx[1]] + wt[2] * ps[idx[2]] + wt[3] * ps[idx[3]];
-  const double y = wt[4] * ps[idx[4]] + wt[5] * ps[idx[5]] + wt[6] * ps[idx[6]] + wt[7] * ps[idx[7]];
-  return f * (0.5 * (ps[a] + ps[b]) - (x + y)) + fabs(f) * ((y - x) * beta);
+  const double q0 = ps[st.o[0]];
+  const double q1 = st.o[1] == st.o[0] ? q0 : ps[st.o[1]];
+  const double q2 = ps[st.o[2]];
+  const double q3 = st.o[3] == st.o[2] ? q2 : ps[st.o[3]];
+  const double* w = st.wt;
+  const double x = w[0] * pa + w[1] * pb + w[2] * q0 + w[3] * q1;
+  const double y = w[4] * pb + w[5] * pa + w[6] * q2 + w[7] * q3;
+  return f * (0.5 * (pa + pb) - (x + y)) + fabs(f) * ((y - x) * beta);
 }
 
 // A cell's edges in ascending edge order (cellEdgeAsc), with their two cells.
@@ -53,14 +76,6 @@ __device__ __forceinline__ void load_edges(const GridDev &g, int i, CellEdges &c
     c.e[s] = e;
     c.a[s] = e >= 0 ? g.eI[e] : 0;
     c.b[s] = e >= 0 ? g.eJ[e] : 0;
-  }
-}
-
-__device__ __forceinline__ void load_stencil(const GridDev &g, int e, int *idx, double *wt) {
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    idx[q] = g.d2idx[e * 8 + q];
-    wt[q] = g.d2wt[e * 8 + q];
   }
 }
 
@@ -99,18 +114,18 @@ __device__ __forceinline__ void tr_p1(const TransportDev &T, const TrArgs &a, in
     const int e = c.e[q];
     if (e >= 0) {
       const bool out = c.a[q] == i;
-      int idx[8];
-      double wt[8];
-      if (order != 1) load_stencil(g, e, idx, wt);
+      Stencil stn;
+      if (order != 1) load_stencil(g, e, stn);
 #pragma unroll
       for (int l = 0; l < L; l++) {
         const double *p = a.tr[j] + (size_t)l * N;
         const double f = a.Fm[(size_t)l * E + e];
         if (with_mass) { if (out) m1[l] -= f; else m1[l] += f; }
-        const double fu = upwind_v(f, p[c.a[q]], p[c.b[q]]);
+        const double pa = p[c.a[q]], pb = p[c.b[q]];
+        const double fu = upwind_v(f, pa, pb);
         if (out) td[l] -= fu; else td[l] += fu;
         if (order != 1) {
-          const double hf = frac * hoflux_s(f, p, idx, wt, c.a[q], c.b[q], a.beta);
+          const double hf = frac * hoflux_s(f, p, stn, pa, pb, a.beta);
           const double m = frac * f;
           if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
         }
@@ -147,14 +162,13 @@ __device__ __forceinline__ void tr_p2(const TransportDev &T, const TrArgs &a, in
     const int e = c.e[q];
     if (e >= 0) {
       const bool out = c.a[q] == i;
-      int idx[8];
-      double wt[8];
-      load_stencil(g, e, idx, wt);
+      Stencil stn;
+      load_stencil(g, e, stn);
 #pragma unroll
       for (int l = 0; l < L; l++) {
         const double *p1 = T.p1 + (size_t)(j * L + l) * N;
         const double f = a.Fm[(size_t)l * E + e];
-        const double hf = frac * hoflux_s(f, p1, idx, wt, c.a[q], c.b[q], a.beta);
+        const double hf = frac * hoflux_s(f, p1, stn, p1[c.a[q]], p1[c.b[q]], a.beta);
         const double m = frac * f;
         if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
       }
@@ -181,16 +195,15 @@ __device__ __forceinline__ void tr_p3(const TransportDev &T, const TrArgs &a, in
     const int e = c.e[q];
     if (e >= 0) {
       const bool out = c.a[q] == i;
-      int idx[8];
-      double wt[8];
-      load_stencil(g, e, idx, wt);
+      Stencil stn;
+      load_stencil(g, e, stn);
 #pragma unroll
       for (int l = 0; l < L; l++) {
         const size_t row = (size_t)(j * L + l);
         const double *p = T.psi0 + row * N;
         const double *p2 = T.p2 + row * N;
         const double f = a.Fm[(size_t)l * E + e];
-        const double A = hoflux_s(f, p2, idx, wt, c.a[q], c.b[q], a.beta) - upwind_v(f, p[c.a[q]], p[c.b[q]]);
+        const double A = hoflux_s(f, p2, stn, p2[c.a[q]], p2[c.b[q]], a.beta) - upwind_v(f, p[c.a[q]], p[c.b[q]]);
         if (out) {
           T.A[row * E + e] = A;
           if (A > 0) Pm[l] += A; else Pp[l] -= A;
