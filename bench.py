@@ -122,6 +122,7 @@ def cpu_member(g, seed, backend):
             s['tr'].mass_after(s['M'], s['Fm'], s['M1'])
             s['tr'].step_many(s['M'], s['M1'], s['Fm'], s['trc'], order=3)
             s['M'], s['M1'] = s['M1'], s['M']
+    step.state = lambda: [a for s in stacks for a in [s['h'], s['u'], s['M']] + s['trc']]   # Member.state() order
     return step, dt
 
 
