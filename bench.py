@@ -179,6 +179,7 @@ def main():
     ap.add_argument('--level', type=int, default=6)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
+    ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -203,45 +204,58 @@ def main():
     from isw.batch import Batch
     from isw.gpu import DeviceGrid, set_precision
     from isw.workload import Member
-    set_precision('double')
     dev = torch.device(f'cuda:{local}')
     torch.cuda.set_device(dev)
     g, t_grid = build_grid(args.level, local)
-    dg = DeviceGrid(g, device=local)
-    batch = None if args.percall else Batch(local)
-    member = Member(dg, seed=rank, batch=batch)
-    layout = batch.info() if batch is not None else None
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
-    for _ in range(args.warmup):
-        member.step()
-    torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    def make(precision):
+        set_precision(precision)
+        try:
+            dg = DeviceGrid(g, device=local)
+            batch = None if args.percall else Batch(local)
+            m = Member(dg, seed=rank, batch=batch)
+        finally:
+            set_precision('double')
+        return m, (batch.info() if batch is not None else None)
+
+    def timed(m):
+        """Mean device ms per step over exactly args.steps steps (after the warm-up), max over ranks."""
+        for _ in range(args.warmup):
+            m.step()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
         t_soak = time.time()                     # keep the GPU busy ~1 s so the clock samples cover load, then time
         while time.time() - t_soak < 1.0:
             for _ in range(20):
-                member.step()
+                m.step()
             torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()                        # the L2 holds no state from the previous step
             starts[k].record(stream)
-            member.step()
+            m.step()
             ends[k].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+        if dist:
+            dist.barrier()
+        t = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+        if dist:
+            x = torch.tensor([t], device=dev)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            t = float(x.item())
+        return t
+
+    member, layout = make('double')
+    mixed, layout_m = (None, None) if args.no_mixed else make('mixed')
+    with ClockSampler(local) as clk:
+        ms = timed(member)
+        ms_m = timed(mixed) if mixed is not None else None
     finite = all(bool(torch.isfinite(a).all()) for a in member.state())
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     dt = member.dt
     value = world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
 
@@ -293,6 +307,12 @@ def main():
                e2e=dict(value=world * (dt / SECONDS_PER_DAY) / (e2e_ms / 1e3), unit='model days/s',
                         h2d_bytes_per_step=io_bytes, d2h_bytes_per_step=io_bytes),
                gpu_launches=member.launches() * args.steps, clocks=clk.summary(), finite=finite, grid_build_s=t_grid)
+    if mixed is not None:
+        vm = world * (dt / SECONDS_PER_DAY) / (ms_m / 1e3)
+        out['mixed'] = dict(value=vm, unit='model days/s', ms_per_step=ms_m, speedup_vs_fp64=vm / value, steps=args.steps,
+                            dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets',
+                            tiles=layout_m, finite=all(bool(torch.isfinite(a).all()) for a in mixed.state()),
+                            gpu_launches=mixed.launches() * args.steps)
 
     if rank == 0 and world == 1 and not args.no_cpu:
         ensure_oracle()

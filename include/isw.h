@@ -42,7 +42,12 @@ enum {
   ISW_ENOTFINITE = 6     /* reserved: a NaN/Inf budget */
 };
 
-enum { ISW_FP64 = 0, ISW_MIXED = 1 };   /* precision forms: plain FP64 (reference parity) or mixed FP32/FP64 */
+/* Precision forms. ISW_FP64: plain FP64, the reference's FP64 path bit for bit (1e-12 where exp() enters). ISW_MIXED:
+ * momentum, the TRiSK operators, the slow tendencies and the FCT curvature corrections in FP32; thicknesses, masses, the
+ * layer fluxes, the fast loop's sub-step sum and the final wind update in FP64 (state arrays stay FP64). A mixed Layers
+ * handle steps through the batched kernels (isw_layers_step uses a private one-stack batch); a mixed Transport handle's
+ * per-call isw_transport_step_many runs the FP64 arithmetic, and the mixed FCT runs inside isw_batch_step. */
+enum { ISW_FP64 = 0, ISW_MIXED = 1 };
 
 typedef struct isw_grid isw_grid;
 typedef struct isw_layers isw_layers;
@@ -118,21 +123,27 @@ int isw_dsum(const double *x, const double *y, long long n, double *out, void *s
 int isw_dsum_static(const double *x, const double *y, long long n, double *out, void *stream);
 
 /* Batched step: stacks (a Layers handle with its state h, u, Fm, and optionally a Transport with M, M1 and tracers)
- * registered once, then advanced together by isw_batch_step in ONE persistent cooperative launch per step: the RK3 step,
- * the receiving masses M1, the FCT step of every tracer, and M <- M1. Stacks may use different grids and layer counts;
- * each stack's result is bit-identical to stepping it alone. Registered pointers are borrowed until removed. */
+ * registered once, then advanced together by isw_batch_step as ONE CUDA graph per step (one kernel per phase over every
+ * stack; the barotropic sub-steps in shared-memory tiles, one cooperative kernel per stage): the RK3 step, the receiving
+ * masses M1, the FCT step of every tracer, and M <- M1. Stacks may use different grids and layer counts; all stacks of a
+ * batch share one precision form (ISW_EINVAL otherwise). Each stack's result is bit-identical to stepping it alone.
+ * Registered pointers are borrowed until removed. */
 int isw_batch_create(int device, isw_batch **out);
 int isw_batch_destroy(isw_batch *b);
 int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *M, double *M1,
                   double *const *tracers, int ntr, double dt, int nfast, int *slot);
 int isw_batch_remove(isw_batch *b, int slot);
 int isw_batch_step(isw_batch *b, void *stream);
-/* Tuning: the barotropic fast loop in shared-memory tiles (tiles_enabled != 0, the default) exchanging every k
- * sub-steps, k the largest up to tile_k (1..32, default 8) whose tiles fit in shared memory; or as grid-wide passes.
- * Results are the same either way. */
-int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k);
-/* The batch's layout: registered stacks, fast-loop tiles, the exchange interval in use, tile shared memory (bytes). */
-int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes);
+/* Tuning (the autotuner's knobs; results are the same under every setting). The barotropic fast loop runs in
+ * shared-memory tiles (tiles_enabled != 0, the default) exchanging every k sub-steps, k the largest up to tile_k (1..8,
+ * default 8) whose tiles fit in shared memory, or as grid-wide passes. layout: 0 choose, 1 shared (one cooperative launch,
+ * every stack cut in proportion to its cells so the tiles fill the SMs), 2 packed (tiles of about tile_cells owned cells,
+ * 64..4096, 0 = by blocks per SM; stacks packed into cooperative launches of at most SMs x blocks-per-SM tiles).
+ * blocks_per_sm: 0 choose, 1 (1024-thread tiles) or 2 (512-thread tiles). */
+int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, int tile_cells, int blocks_per_sm);
+/* The batch's layout: registered stacks, fast-loop tiles, the exchange interval in use, the largest tile's shared memory
+ * (bytes), the cooperative launches per stage, tile blocks per SM (0 when untiled). */
+int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes, int *groups, int *blocks_per_sm);
 /* The batch's device status word (ISW_OK, or ISW_ETIMEOUT after a grid barrier's bounded wait ran out); synchronises
  * `stream`; reset != 0 clears it. */
 int isw_batch_status(isw_batch *b, void *stream, int reset);

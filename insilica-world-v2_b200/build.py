@@ -4,7 +4,7 @@
 
 FP64 sources compile with -fmad=false (no fused multiply-add: every product rounds as the reference's --fmad=false
 kernels do); host code with -ffp-contract=off for the same reason (the transport stencil's weights are computed on the
-host). --check adds -DISW_CHECK (device-side bounds checks on gathered indices, for debugging).
+host). The mixed form's kernels (batch_mixed.cu) compile with fused multiply-adds. --check adds -DISW_CHECK (device-side bounds checks on gathered indices, for debugging).
 """
 import argparse
 import os
@@ -26,6 +26,7 @@ SOURCES = [  # (file, extra flags)
     ('mesh.cu', ['-fmad=false', '-Xcompiler', '-fopenmp']),
     ('tiles.cu', ['-fmad=false']),
     ('batch.cu', ['-fmad=false']),
+    ('batch_mixed.cu', ['-fmad=true']),     # the mixed form: fused multiply-adds allowed
 ]
 
 

@@ -14,9 +14,8 @@
 //
 // The tile kernel's grid barrier waits with an iteration-bounded, time-bounded spin (globaltimer): if a wait runs out
 // it records ISW_ETIMEOUT in the batch's status word and every block returns; the host reads the status.
-#include <cuda/atomic>
-
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -24,6 +23,7 @@
 #include <tuple>
 #include <vector>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "handles.cuh"
 #include "layers_fp64.cuh"
@@ -31,141 +31,9 @@
 #include "transport_fp64.cuh"
 
 namespace isw {
+using namespace bt;
 namespace {
 
-
-struct TileSetDev {
-  int P, k;
-  const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt, *eown;
-  const int16_t *cedge, *eIl, *eJl;
-  const double *ade, *ale, *aarea;            // d_e, l_e per local edge and the area per local cell, in local order
-};
-
-struct StackDesc {
-  LayersDev M;
-  TransportDev T;
-  TrArgs tr;                 // M0 = the stack's M, M1, Fm, tracers, L, rows, beta
-  double *h, *u, *Fm, *Mm;
-  double dt;
-  int L, has_tr, tiled;
-  int n[3];
-  double cdt[3], tau[3], inv_n[3];
-  TileSetDev tiles;
-};
-
-struct Chunk {
-  int s, begin, end;
-};
-
-struct TileRef {
-  int s, p;
-};
-
-struct Sched {
-  const Chunk *cell, *edge, *vert, *rows;
-  int ncell, nedge, nvert, nrows;
-};
-
-struct GridBarrier {
-  unsigned count, gen;
-};
-
-__device__ __forceinline__ long long globaltimer() {
-  long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Block-wide grid barrier with a bounded wait. Returns false once any block has recorded a failure.
-__device__ bool grid_sync(GridBarrier *b, int *status, long long timeout_ns, int skip_arrive) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(b->gen), cnt(b->count);
-    cuda::atomic_ref<int, cuda::thread_scope_device> st(*status);
-    const unsigned g0 = gen.load(cuda::memory_order_acquire);
-    __threadfence();
-    if (!skip_arrive && cnt.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
-      cnt.store(0u, cuda::memory_order_relaxed);
-      gen.fetch_add(1u, cuda::memory_order_release);
-    } else {
-      const long long t0 = globaltimer();
-      unsigned it = 0;
-      while (gen.load(cuda::memory_order_acquire) == g0) {
-        ++it;
-        if ((it & 63) == 0) {
-          if (st.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
-          if (globaltimer() - t0 > timeout_ns) {
-            int z = 0;
-            st.compare_exchange_strong(z, (int)ISW_ETIMEOUT, cuda::memory_order_relaxed);
-            ok = 0;
-            break;
-          }
-        }
-        if (it > (1u << 30)) { ok = 0; break; }
-      }
-    }
-    __threadfence();
-    if (st.load(cuda::memory_order_relaxed) != 0) ok = 0;
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
-#define ISW_BATCH_L(LV, LMAXK, CALL)                                                            \
-  do {                                                                                          \
-    switch (LV) {                                                                               \
-      case 1: { constexpr int LL = 1; CALL; } break;                                            \
-      case 2: if (LMAXK >= 2) { constexpr int LL = 2 <= LMAXK ? 2 : 1; CALL; } break;           \
-      case 3: if (LMAXK >= 3) { constexpr int LL = 3 <= LMAXK ? 3 : 1; CALL; } break;           \
-      case 4: if (LMAXK >= 4) { constexpr int LL = 4 <= LMAXK ? 4 : 1; CALL; } break;           \
-      case 5: if (LMAXK >= 5) { constexpr int LL = 5 <= LMAXK ? 5 : 1; CALL; } break;           \
-      case 6: if (LMAXK >= 6) { constexpr int LL = 6 <= LMAXK ? 6 : 1; CALL; } break;           \
-      case 7: if (LMAXK >= 7) { constexpr int LL = 7 <= LMAXK ? 7 : 1; CALL; } break;           \
-      case 8: if (LMAXK >= 8) { constexpr int LL = 8 <= LMAXK ? 8 : 1; CALL; } break;           \
-      default: break;                                                                           \
-    }                                                                                           \
-  } while (0)
-
-__device__ __forceinline__ StageArgs stage_args(const StackDesc &d, int st) {
-  StageArgs a;
-  a.h0 = d.h;
-  a.u0 = d.u;
-  a.hs = st == 0 ? d.h : st == 1 ? d.M.h1 : d.M.h2;
-  a.us = st == 0 ? d.u : st == 1 ? d.M.u1 : d.M.u2;
-  a.hn = st == 0 ? d.M.h1 : st == 1 ? d.M.h2 : d.h;
-  a.un = st == 0 ? d.M.u1 : st == 1 ? d.M.u2 : d.u;
-  a.Fm = st == 2 ? d.Fm : nullptr;
-  a.cdt = d.cdt[st];
-  a.dt = d.dt;
-  a.tau = d.tau[st];
-  a.inv_n = d.inv_n[st];
-  a.n = d.n[st];
-  return a;
-}
-
-// The block's stack descriptor, staged in shared memory (one chunk per block, so one stack per block).
-__device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s) {
-  __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
-  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(S + s);
-  unsigned long long *dst = reinterpret_cast<unsigned long long *>(buf);
-  for (int w = threadIdx.x; w < (int)(sizeof(StackDesc) / 8); w += blockDim.x) dst[w] = src[w];
-  __syncthreads();
-  return *reinterpret_cast<const StackDesc *>(buf);
-}
-
-enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4 };
-
-// Domains of a phase, in block order: which chunk tables its blocks walk.
-template <int PH>
-struct Dom {
-  static constexpr bool cell = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A || PH == PH_ETA || PH == PH_C || PH == PH_D;
-  static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
-                               PH == PH_D || PH == PH_POST;
-  static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
-  static constexpr bool rows = PH == PH_POST || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
-};
 
 template <int PH, int LMAXK>
 __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
@@ -367,6 +235,12 @@ struct BatchSlot {
   int nfast = 0;
 };
 
+struct FastGroup {
+  int begin = 0, count = 0;
+  size_t smem = 0;
+  int rounds[3] = {0, 0, 0};
+};
+
 struct TileCache {
   TileSetDev dev{};
   TileSetHost host;
@@ -381,7 +255,8 @@ struct isw_batch {
   Chunk *d_chunks = nullptr;
   TileRef *d_refs = nullptr;
   Sched sc{};
-  int lmax = 1, nstacks = 0, ntiles = 0, rounds[3] = {0, 0, 0}, nsub[3] = {0, 0, 0}, kused = 0;
+  int lmax = 1, nstacks = 0, ntiles = 0, nsub[3] = {0, 0, 0}, kused = 0;
+  std::vector<FastGroup> groups;              // cooperative launches of the fast loop (tiles [begin, begin + count))
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0;
   size_t fast_smem = 0;
   int fast_bps = 2;                           // tile blocks per SM: 2 (512 threads each) or 1 (1024 threads)
@@ -389,6 +264,10 @@ struct isw_batch {
   int *status = nullptr;
   int tile_k = 8;
   int tiles_enabled = 1;
+  int mixed = -1;                             // the stacks' precision form (all alike): -1 before the first add
+  int tile_cells = 0;                         // packed layout's owned cells per tile (0: by blocks per SM)
+  int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
+  int layout = 0;                             // 0: choose; 1 shared; 2 packed
   std::map<std::tuple<const isw_grid *, int, int>, std::unique_ptr<TileCache>> tiles;
   std::map<std::pair<const isw_grid *, int>, std::vector<int32_t>> parts;
   cudaStream_t cap = nullptr;
@@ -462,68 +341,146 @@ TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k) {
   t.ade = dupload(c->allocs, ade);
   t.ale = dupload(c->allocs, ale);
   t.aarea = dupload(c->allocs, aarea);
+  std::vector<float> rde32(h.edges.size()), le32(h.edges.size()), rA32(h.cells.size());
+  for (size_t q = 0; q < h.edges.size(); q++) { rde32[q] = (float)(1.0 / ade[q]); le32[q] = (float)ale[q]; }
+  for (size_t q = 0; q < h.cells.size(); q++) rA32[q] = (float)(1.0 / aarea[q]);
+  t.arde32 = dupload(c->allocs, rde32);
+  t.ale32 = dupload(c->allocs, le32);
+  t.arA32 = dupload(c->allocs, rA32);
   TileCache *out = c.get();
   b->tiles[key] = std::move(c);
   return out;
 }
 
+size_t smem_of(size_t nc, size_t ne, size_t nown, bool mixed) {
+  return mixed ? tile_smem_bytes_mixed(nc, ne, nown) : tile_smem_bytes(nc, ne, nown);
+}
+
 // The largest k' <= the probe's k whose largest tile fits `budget` bytes of shared memory (0 if none).
-int fitting_k(const TileSetHost &h, size_t budget) {
+int fitting_k(const TileSetHost &h, size_t budget, bool mixed) {
   for (int kk = h.k; kk >= 1; kk--) {
     size_t worst = 0;
     for (int p = 0; p < h.P; p++) {
       const size_t nc = h.ncnt[(size_t)p * (h.k + 1) + kk], ne = h.ecnt[(size_t)p * (h.k + 1) + kk];
-      worst = std::max(worst, tile_smem_bytes(nc, ne, h.eown[p]));
+      worst = std::max(worst, smem_of(nc, ne, h.eown[p], mixed));
     }
     if (worst <= budget) return kk;
   }
   return 0;
 }
 
+// Dynamic shared memory of the largest tile of a tile set.
+size_t tiles_smem(const TileSetHost &h, bool mixed) {
+  size_t worst = 0;
+  for (int p = 0; p < h.P; p++)
+    worst = std::max(worst, smem_of(h.cell_off[p + 1] - h.cell_off[p], h.edge_off[p + 1] - h.edge_off[p], h.eown[p], mixed));
+  return worst;
+}
+
 int kernel_lmax(int L) { return L <= 2 ? 2 : L <= 3 ? 3 : L <= 5 ? 5 : 8; }
+
+// The fast-loop tiling of the registered stacks. Two layouts, and the one with the larger exchange interval k wins:
+//  - shared: one cooperative group over all stacks, each stack cut into tiles in proportion to its share of the cells,
+//    filling the SMs (small batches: one member, a few members);
+//  - packed: each stack cut into tiles of about tile_cells owned cells (a fixed size per grid, so tile sets are reused
+//    as stacks come and go), the stacks packed in order into groups of at most SMs x blocks-per-SM tiles, one
+//    cooperative launch per group and stage (large ensembles, serving).
+// Stacks whose tiles would not fit in shared memory at all take the grid-wide sub-step kernels.
+struct Tiling {
+  int k = 0, bps = 2;
+  std::vector<int> P;                          // tiles per slot (0: untiled)
+  std::vector<int> group;                      // group per slot
+};
+
+Tiling plan_shared(isw_batch *b, int bps) {
+  Tiling t;
+  t.bps = bps;
+  t.P.assign(b->slots.size(), 0);
+  t.group.assign(b->slots.size(), 0);
+  const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
+  const int slots = b->sms * bps;
+  long long cells_total = 0;
+  for (auto &sl : b->slots)
+    if (sl.used) cells_total += sl.layers->grid->d.N;
+  int kmin = b->tile_k;
+  bool any = false;
+  for (size_t q = 0; q < b->slots.size(); q++) {
+    const BatchSlot &sl = b->slots[q];
+    if (!sl.used) continue;
+    const int N = sl.layers->grid->d.N;
+    const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
+    if (Pq * 16 > N) return Tiling{};          // tiles of at least 16 owned cells, for every stack
+    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1);
+    if (kf == 0) return Tiling{};
+    t.P[q] = Pq;
+    kmin = std::min(kmin, kf);
+    any = true;
+  }
+  t.k = any ? kmin : 0;
+  return t;
+}
+
+Tiling plan_packed(isw_batch *b, int bps) {
+  Tiling t;
+  t.bps = bps;
+  t.P.assign(b->slots.size(), 0);
+  t.group.assign(b->slots.size(), 0);
+  const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
+  const int cap = b->sms * bps;
+  const int cells = b->tile_cells > 0 ? b->tile_cells : (bps == 2 ? 384 : 768);
+  int kmin = b->tile_k;
+  bool any = false;
+  for (size_t q = 0; q < b->slots.size(); q++) {
+    const BatchSlot &sl = b->slots[q];
+    if (!sl.used) continue;
+    const int N = sl.layers->grid->d.N;
+    const int Pq = std::min(cap, std::max(1, (N + cells - 1) / cells));
+    if (Pq * 16 > N) continue;
+    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1);
+    if (kf == 0) continue;
+    t.P[q] = Pq;
+    kmin = std::min(kmin, kf);
+    any = true;
+  }
+  if (!any) return Tiling{};
+  t.k = kmin;
+  int g = 0, fill = 0;
+  for (size_t q = 0; q < b->slots.size(); q++) {
+    if (t.P[q] == 0) continue;
+    if (fill + t.P[q] > cap) { g++; fill = 0; }
+    t.group[q] = g;
+    fill += t.P[q];
+  }
+  return t;
+}
 
 void rebuild(isw_batch *b) {
   std::vector<StackDesc> desc;
   std::vector<Chunk> cell, edge, vert, rows;
-  std::vector<TileRef> refs;
   int nsub[3] = {0, 0, 0};
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
-  size_t fast_smem = 0;
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
-  // the tiling: per stack P tiles (its share of the tile slots by cell count) and one exchange interval k for all
-  // stacks, the largest that fits the shared memory of one or of two tile blocks per SM
-  long long cells_total = 0;
   int used = 0;
-  for (auto &sl : b->slots)
-    if (sl.used) { cells_total += sl.layers->grid->d.N; used++; }
-  std::vector<int> Pbest(b->slots.size(), 0);
-  int kbest = 0, bps_best = 2;
+  for (auto &sl : b->slots) used += sl.used ? 1 : 0;
+  Tiling best;
   if (b->tiles_enabled && used > 0) {
     for (int bps = 2; bps >= 1; bps--) {
-      const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
-      const int slots = b->sms * bps;
-      std::vector<int> P(b->slots.size(), 0);
-      int kmin = b->tile_k;
-      bool any = false;
-      for (size_t q = 0; q < b->slots.size(); q++) {
-        const BatchSlot &sl = b->slots[q];
-        if (!sl.used) continue;
-        const int N = sl.layers->grid->d.N;
-        const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
-        if (Pq * 16 > N) continue;             // tiles of at least 16 owned cells
-        const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget);
-        if (kf == 0) continue;
-        P[q] = Pq;
-        kmin = std::min(kmin, kf);
-        any = true;
+      if (b->force_bps && bps != b->force_bps) continue;
+      if (b->layout != 2) {
+        Tiling t = plan_shared(b, bps);
+        if (t.k > best.k) best = t;
       }
-      if (any && kmin > kbest) {
-        kbest = kmin;
-        bps_best = bps;
-        Pbest = P;
+      if (b->layout != 1) {
+        Tiling t = plan_packed(b, bps);
+        if (t.k > best.k || (b->layout == 2 && t.k > 0 && best.k == 0)) best = t;
       }
     }
   }
+  const int kbest = best.k;
+  const int ngroups = kbest > 0 ? 1 + *std::max_element(best.group.begin(), best.group.end()) : 0;
+  std::vector<std::vector<TileRef>> grefs(ngroups);
+  std::vector<size_t> gsmem(ngroups, 0);
+  std::vector<std::array<int, 3>> gsub(ngroups, std::array<int, 3>{0, 0, 0});
   for (auto &sl : b->slots) {
     if (!sl.used) continue;
     StackDesc d;
@@ -554,12 +511,14 @@ void rebuild(isw_batch *b) {
     const int s = (int)desc.size();
     d.tiled = 0;
     const size_t q = (size_t)(&sl - &b->slots[0]);
-    if (kbest > 0 && Pbest[q] > 0) {
-      TileCache *tc = tiles_for(b, sl.layers->grid, Pbest[q], kbest);
+    if (kbest > 0 && best.P[q] > 0) {
+      TileCache *tc = tiles_for(b, sl.layers->grid, best.P[q], kbest);
+      const int g = best.group[q];
       d.tiled = 1;
       d.tiles = tc->dev;
-      fast_smem = std::max(fast_smem, tc->host.smem);
-      for (int p = 0; p < Pbest[q]; p++) refs.push_back(TileRef{s, p});
+      gsmem[g] = std::max(gsmem[g], tiles_smem(tc->host, b->mixed == 1));
+      for (int p = 0; p < best.P[q]; p++) grefs[g].push_back(TileRef{s, p});
+      for (int st = 0; st < 3; st++) gsub[g][st] = std::max(gsub[g][st], d.n[st]);
     }
     if (!d.tiled) any_untiled = 1;
     auto chunks = [&](std::vector<Chunk> &v, int n) {
@@ -578,6 +537,8 @@ void rebuild(isw_batch *b) {
   b->d_desc = nullptr;
   b->d_chunks = nullptr;
   b->d_refs = nullptr;
+  b->groups.clear();
+  b->ntiles = 0;
   if (b->exec) {
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
@@ -590,9 +551,36 @@ void rebuild(isw_batch *b) {
   all.insert(all.end(), vert.begin(), vert.end());
   all.insert(all.end(), rows.begin(), rows.end());
   ISW_CUDA(cudaMalloc(&b->d_desc, sizeof(StackDesc) * desc.size()));
-  ISW_CUDA(cudaMemcpy(b->d_desc, desc.data(), sizeof(StackDesc) * desc.size(), cudaMemcpyHostToDevice));
   ISW_CUDA(cudaMalloc(&b->d_chunks, sizeof(Chunk) * all.size()));
   ISW_CUDA(cudaMemcpy(b->d_chunks, all.data(), sizeof(Chunk) * all.size(), cudaMemcpyHostToDevice));
+  std::vector<TileRef> refs;
+  for (int g = 0; g < ngroups; g++) {
+    FastGroup fg;
+    fg.begin = (int)refs.size();
+    fg.count = (int)grefs[g].size();
+    fg.smem = gsmem[g];
+    for (int st = 0; st < 3; st++) fg.rounds[st] = (gsub[g][st] + kbest - 1) / kbest;
+    refs.insert(refs.end(), grefs[g].begin(), grefs[g].end());
+    b->groups.push_back(fg);
+  }
+  b->fast_bps = best.bps;
+  if (!refs.empty()) {                       // every tile block of a group must be resident at once (cooperative launch)
+    const void *fn = b->mixed == 1 ? fast_kernel_mixed(best.bps)
+                     : best.bps == 2 ? (const void *)k_fast<512, 2> : (const void *)k_fast<1024, 1>;
+    size_t smax = 0;
+    int cmax = 0;
+    for (auto &fg : b->groups) { smax = std::max(smax, fg.smem); cmax = std::max(cmax, fg.count); }
+    if (smax > 48 * 1024) ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+    int per = 0;
+    ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, best.bps == 2 ? 512 : 1024, smax));
+    if ((long long)per * b->sms < cmax) {
+      refs.clear();
+      b->groups.clear();
+      any_untiled = 1;
+      for (auto &d : desc) d.tiled = 0;
+    }
+  }
+  ISW_CUDA(cudaMemcpy(b->d_desc, desc.data(), sizeof(StackDesc) * desc.size(), cudaMemcpyHostToDevice));
   if (!refs.empty()) {
     ISW_CUDA(cudaMalloc(&b->d_refs, sizeof(TileRef) * refs.size()));
     ISW_CUDA(cudaMemcpy(b->d_refs, refs.data(), sizeof(TileRef) * refs.size(), cudaMemcpyHostToDevice));
@@ -607,25 +595,11 @@ void rebuild(isw_batch *b) {
   sc.rows = sc.vert + sc.nvert;
   sc.nrows = (int)rows.size();
   b->ntiles = (int)refs.size();
-  b->fast_smem = fast_smem;
-  b->fast_bps = bps_best;
-  if (b->ntiles > 0) {                      // every tile block must be resident at once (cooperative launch)
-    const void *fn = bps_best == 2 ? (const void *)k_fast<512, 2> : (const void *)k_fast<1024, 1>;
-    if (fast_smem > 48 * 1024) ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_smem));
-    int per = 0;
-    ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, bps_best == 2 ? 512 : 1024, fast_smem));
-    if ((long long)per * b->sms < b->ntiles) {
-      b->ntiles = 0;
-      any_untiled = 1;
-      for (auto &d : desc) d.tiled = 0;
-      ISW_CUDA(cudaMemcpy(b->d_desc, desc.data(), sizeof(StackDesc) * desc.size(), cudaMemcpyHostToDevice));
-    }
-  }
-  for (int st = 0; st < 3; st++) {
-    b->nsub[st] = nsub[st];
-    b->rounds[st] = kbest > 0 ? (nsub[st] + kbest - 1) / kbest : 0;
-  b->kused = kbest;
-  }
+  size_t smax = 0;
+  for (auto &fg : b->groups) smax = std::max(smax, fg.smem);
+  b->fast_smem = smax;
+  for (int st = 0; st < 3; st++) b->nsub[st] = nsub[st];
+  b->kused = b->ntiles > 0 ? kbest : 0;
   b->any_nu4 = any_nu4;
   b->any_vmix = any_vmix;
   b->any_tr = any_tr;
@@ -639,6 +613,10 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j) {
   const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
                  (Dom<PH>::rows ? sc.nrows : 0);
   if (nb == 0) return;
+  if (b->mixed == 1) {
+    launch_phase_mixed(PH, b->lmax, nb, st, b->d_desc, sc, stage, j);
+    return;
+  }
   switch (b->lmax) {
     case 2: k_phase<PH, 2><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
     case 3: k_phase<PH, 3><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
@@ -648,24 +626,30 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j) {
 }
 
 void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns, int fault_block) {
-  if (b->ntiles == 0) return;
-  ISW_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), st));
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)b->ntiles);
-  cfg.blockDim = dim3(b->fast_bps == 2 ? 512 : 1024);
-  cfg.dynamicSmemBytes = b->fast_smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (b->fast_bps == 2)
-    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<512, 2>, (const StackDesc *)b->d_desc, (const TileRef *)b->d_refs, stage,
-                                b->rounds[stage], b->bar, b->status, timeout_ns, fault_block));
-  else
-    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<1024, 1>, (const StackDesc *)b->d_desc, (const TileRef *)b->d_refs, stage,
-                                b->rounds[stage], b->bar, b->status, timeout_ns, fault_block));
+  for (const FastGroup &fg : b->groups) {
+    if (fg.count == 0) continue;
+    ISW_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)fg.count);
+    cfg.blockDim = dim3(b->fast_bps == 2 ? 512 : 1024);
+    cfg.dynamicSmemBytes = fg.smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const TileRef *refs = b->d_refs + fg.begin;
+    const StackDesc *desc = b->d_desc;
+    const int rounds = fg.rounds[stage];
+    if (b->mixed == 1)
+      launch_fast_mixed(b->fast_bps, cfg, desc, refs, stage, rounds, b->bar, b->status, timeout_ns, fault_block);
+    else if (b->fast_bps == 2)
+      ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<512, 2>, desc, refs, stage, rounds, b->bar, b->status, timeout_ns, fault_block));
+    else
+      ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast<1024, 1>, desc, refs, stage, rounds, b->bar, b->status, timeout_ns, fault_block));
+    if (fault_block >= 0) break;             // the failure test runs the first group only
+  }
 }
 
 // The launches of one step, in order.
@@ -782,7 +766,12 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
       if (!M || !M1 || !tracers) fail(ISW_EINVAL, "batch.add: transport needs M, M1 and the tracers");
       if (ntr < 1 || ntr > tr->T) fail(ISW_EINVAL, "batch.add: ntr outside 1..tracers of the transport");
       if (tr->L != layers->d.L || tr->grid != layers->grid) fail(ISW_EINVAL, "batch.add: transport and layers differ in grid or L");
+      if (tr->precision != layers->d.precision) fail(ISW_EINVAL, "batch.add: transport and layers differ in precision form");
     }
+    const int mixed = layers->d.precision == ISW_MIXED ? 1 : 0;
+    bool any = false;
+    for (auto &q : b->slots) any = any || q.used;
+    if (any && b->mixed != mixed) fail(ISW_EINVAL, "batch.add: a batch holds stacks of one precision form");
     BatchSlot sl;
     sl.used = true;
     sl.layers = layers;
@@ -799,6 +788,7 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     while (k < b->slots.size() && b->slots[k].used) k++;
     if (k == b->slots.size()) b->slots.push_back(sl);
     else b->slots[k] = sl;
+    b->mixed = mixed;
     b->dirty = true;
     *slot = (int)k;
   });
@@ -812,25 +802,33 @@ int isw_batch_remove(isw_batch *b, int slot) {
   });
 }
 
-int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k) {
+int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, int tile_cells, int blocks_per_sm) {
   return guarded([&] {
     if (!b) fail(ISW_EINVAL, "batch.config: null handle");
-    if (tile_k < 1 || tile_k > 32) fail(ISW_EINVAL, "batch.config: tile_k outside 1..32");
+    if (tile_k < 1 || tile_k > K_PROBE) fail(ISW_EINVAL, "batch.config: tile_k outside 1..8");
+    if (layout < 0 || layout > 2) fail(ISW_EINVAL, "batch.config: layout must be 0 (choose), 1 (shared) or 2 (packed)");
+    if (tile_cells != 0 && (tile_cells < 64 || tile_cells > 4096)) fail(ISW_EINVAL, "batch.config: tile_cells outside 64..4096");
+    if (blocks_per_sm < 0 || blocks_per_sm > 2) fail(ISW_EINVAL, "batch.config: blocks_per_sm must be 0 (choose), 1 or 2");
     b->tiles_enabled = tiles_enabled ? 1 : 0;
     b->tile_k = tile_k;
+    b->layout = layout;
+    b->tile_cells = tile_cells;
+    b->force_bps = blocks_per_sm;
     b->dirty = true;
   });
 }
 
-int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes) {
+int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes, int *groups, int *blocks_per_sm) {
   return guarded([&] {
-    if (!b || !stacks || !tiles || !tile_k || !smem_bytes) fail(ISW_EINVAL, "batch.info: null argument");
+    if (!b || !stacks || !tiles || !tile_k || !smem_bytes || !groups || !blocks_per_sm) fail(ISW_EINVAL, "batch.info: null argument");
     ISW_CUDA(cudaSetDevice(b->device));
     prepare(b);
     *stacks = b->nstacks;
     *tiles = b->ntiles;
     *tile_k = b->ntiles > 0 ? b->kused : 0;
     *smem_bytes = (long long)b->fast_smem;
+    *groups = (int)b->groups.size();
+    *blocks_per_sm = b->ntiles > 0 ? b->fast_bps : 0;
   });
 }
 
@@ -863,7 +861,7 @@ int isw_batch_fault_test(isw_batch *b, long long timeout_ns, void *stream) {
     ISW_CUDA(cudaSetDevice(b->device));
     prepare(b);
     if (b->ntiles == 0) fail(ISW_EUNSUPPORTED, "batch.fault_test: no tiled stack in the batch");
-    if (b->rounds[2] < 2) fail(ISW_EUNSUPPORTED, "batch.fault_test: the last stage has no grid barrier");
+    if (b->groups.empty() || b->groups[0].rounds[2] < 2) fail(ISW_EUNSUPPORTED, "batch.fault_test: the last stage has no grid barrier");
     launch_fast(b, (cudaStream_t)stream, 2, timeout_ns, 0);
   });
 }

@@ -1,0 +1,154 @@
+// Definitions shared by the batched step's translation units (batch.cu: plain FP64 phases and the step's host side;
+// batch_mixed.cu: the mixed form's phases, compiled with fused multiply-adds): the stack descriptor, chunk tables,
+// tiles, the bounded grid barrier, the phase list.
+#pragma once
+#include <cuda/atomic>
+
+#include "common.cuh"
+#include "transport_fp64.cuh"
+
+namespace isw {
+namespace bt {
+
+struct TileSetDev {
+  int P, k;
+  const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt, *eown;
+  const int16_t *cedge, *eIl, *eJl;
+  const double *ade, *ale, *aarea;            // d_e, l_e per local edge and the area per local cell, in local order
+  const float *arde32, *ale32, *arA32;        // the mixed form's: 1 / d_e, l_e, 1 / area, in local order
+};
+
+struct StackDesc {
+  LayersDev M;
+  TransportDev T;
+  TrArgs tr;                 // M0 = the stack's M, M1, Fm, tracers, L, rows, beta
+  double *h, *u, *Fm, *Mm;
+  double dt;
+  int L, has_tr, tiled;
+  int n[3];
+  double cdt[3], tau[3], inv_n[3];
+  TileSetDev tiles;
+};
+
+struct Chunk {
+  int s, begin, end;
+};
+
+struct TileRef {
+  int s, p;
+};
+
+struct Sched {
+  const Chunk *cell, *edge, *vert, *rows;
+  int ncell, nedge, nvert, nrows;
+};
+
+struct GridBarrier {
+  unsigned count, gen;
+};
+
+__device__ __forceinline__ long long globaltimer() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Block-wide grid barrier with a bounded wait. Returns false once any block has recorded a failure.
+__device__ inline bool grid_sync(GridBarrier *b, int *status, long long timeout_ns, int skip_arrive) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(b->gen), cnt(b->count);
+    cuda::atomic_ref<int, cuda::thread_scope_device> st(*status);
+    const unsigned g0 = gen.load(cuda::memory_order_acquire);
+    __threadfence();
+    if (!skip_arrive && cnt.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.fetch_add(1u, cuda::memory_order_release);
+    } else {
+      const long long t0 = globaltimer();
+      unsigned it = 0;
+      while (gen.load(cuda::memory_order_acquire) == g0) {
+        ++it;
+        if ((it & 63) == 0) {
+          if (st.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
+          if (globaltimer() - t0 > timeout_ns) {
+            int z = 0;
+            st.compare_exchange_strong(z, (int)ISW_ETIMEOUT, cuda::memory_order_relaxed);
+            ok = 0;
+            break;
+          }
+        }
+        if (it > (1u << 30)) { ok = 0; break; }
+      }
+    }
+    __threadfence();
+    if (st.load(cuda::memory_order_relaxed) != 0) ok = 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+#define ISW_BATCH_L(LV, LMAXK, CALL)                                                            \
+  do {                                                                                          \
+    switch (LV) {                                                                               \
+      case 1: { constexpr int LL = 1; CALL; } break;                                            \
+      case 2: if (LMAXK >= 2) { constexpr int LL = 2 <= LMAXK ? 2 : 1; CALL; } break;           \
+      case 3: if (LMAXK >= 3) { constexpr int LL = 3 <= LMAXK ? 3 : 1; CALL; } break;           \
+      case 4: if (LMAXK >= 4) { constexpr int LL = 4 <= LMAXK ? 4 : 1; CALL; } break;           \
+      case 5: if (LMAXK >= 5) { constexpr int LL = 5 <= LMAXK ? 5 : 1; CALL; } break;           \
+      case 6: if (LMAXK >= 6) { constexpr int LL = 6 <= LMAXK ? 6 : 1; CALL; } break;           \
+      case 7: if (LMAXK >= 7) { constexpr int LL = 7 <= LMAXK ? 7 : 1; CALL; } break;           \
+      case 8: if (LMAXK >= 8) { constexpr int LL = 8 <= LMAXK ? 8 : 1; CALL; } break;           \
+      default: break;                                                                           \
+    }                                                                                           \
+  } while (0)
+
+__device__ __forceinline__ StageArgs stage_args(const StackDesc &d, int st) {
+  StageArgs a;
+  a.h0 = d.h;
+  a.u0 = d.u;
+  a.hs = st == 0 ? d.h : st == 1 ? d.M.h1 : d.M.h2;
+  a.us = st == 0 ? d.u : st == 1 ? d.M.u1 : d.M.u2;
+  a.hn = st == 0 ? d.M.h1 : st == 1 ? d.M.h2 : d.h;
+  a.un = st == 0 ? d.M.u1 : st == 1 ? d.M.u2 : d.u;
+  a.Fm = st == 2 ? d.Fm : nullptr;
+  a.cdt = d.cdt[st];
+  a.dt = d.dt;
+  a.tau = d.tau[st];
+  a.inv_n = d.inv_n[st];
+  a.n = d.n[st];
+  return a;
+}
+
+// The block's stack descriptor, staged in shared memory (one chunk per block, so one stack per block).
+__device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s) {
+  __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(S + s);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(buf);
+  for (int w = threadIdx.x; w < (int)(sizeof(StackDesc) / 8); w += blockDim.x) dst[w] = src[w];
+  __syncthreads();
+  return *reinterpret_cast<const StackDesc *>(buf);
+}
+
+enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4 };
+
+// Domains of a phase, in block order: which chunk tables its blocks walk.
+template <int PH>
+struct Dom {
+  static constexpr bool cell = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A || PH == PH_ETA || PH == PH_C || PH == PH_D;
+  static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
+                               PH == PH_D || PH == PH_POST;
+  static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
+  static constexpr bool rows = PH == PH_POST || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
+};
+
+
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j);
+const void *fast_kernel_mixed(int bps);
+void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
+                       GridBarrier *bar, int *status, long long timeout_ns, int fault_block);
+
+}  // namespace bt
+}  // namespace isw

@@ -1,0 +1,271 @@
+// The batched step's kernels for stacks in the mixed form (layers_mixed.cuh, transport_mixed.cuh): the same phase list,
+// chunk tables and tiles as the plain FP64 kernels in batch.cu, compiled with fused multiply-adds (this file alone).
+// The tile kernel runs the fast loop in deviation form (deta, dub in FP32, their FP64 sum acc) in shared memory.
+#include "batch.cuh"
+#include "layers_mixed.cuh"
+#include "transport_mixed.cuh"
+
+namespace isw {
+namespace bt {
+namespace {
+
+__device__ __forceinline__ mixed::MStageArgs mstage_args(const StackDesc &d, int st) {
+  const LayersDev &M = d.M;
+  mixed::MStageArgs a;
+  a.h0 = d.h;
+  a.u0 = d.u;
+  a.u0f = M.u32;
+  a.hs = st == 0 ? d.h : st == 1 ? M.h1 : M.h2;
+  a.us = st == 0 ? M.u32 : st == 1 ? M.u1f : M.u2f;
+  a.hn = st == 0 ? M.h1 : st == 1 ? M.h2 : d.h;
+  a.un = st == 2 ? d.u : nullptr;
+  a.unf = st == 0 ? M.u1f : st == 1 ? M.u2f : nullptr;
+  a.Fm = st == 2 ? d.Fm : nullptr;
+  a.cdt = d.cdt[st];
+  a.dt = d.dt;
+  a.tau = (float)d.tau[st];
+  a.inv_n = d.inv_n[st];
+  a.n = d.n[st];
+  return a;
+}
+
+template <int PH, int LMAXK>
+__global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
+  int b = blockIdx.x;
+  int kind = -1;
+  Chunk ch{0, 0, 0};
+  if (Dom<PH>::cell) { if (b < sc.ncell) { kind = 0; ch = sc.cell[b]; } else b -= sc.ncell; }
+  if (kind < 0 && Dom<PH>::edge) { if (b < sc.nedge) { kind = 1; ch = sc.edge[b]; } else b -= sc.nedge; }
+  if (kind < 0 && Dom<PH>::vert) { if (b < sc.nvert) { kind = 2; ch = sc.vert[b]; } else b -= sc.nvert; }
+  if (kind < 0 && Dom<PH>::rows) { if (b < sc.nrows) { kind = 3; ch = sc.rows[b]; } else b -= sc.nrows; }
+  if (kind < 0) return;
+  const StackDesc &d = stage_desc(S, ch.s);
+  const int i = ch.begin + (int)threadIdx.x;
+  if (i >= ch.end) return;
+  const LayersDev &M = d.M;
+  if (PH == PH_INIT) {
+    if (kind == 0) {
+      ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
+      if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, (mixed::div_cell<LL, double>(M, d.u, i)));
+    } else if (kind == 1) {
+      ISW_BATCH_L(d.L, LMAXK, mixed::ubar0_edge<LL>(M, d.h, d.u, i));
+    } else if (M.nu4 != 0) {
+      ISW_BATCH_L(d.L, LMAXK, (mixed::curl_vertex<LL, double>(M, d.u, i)));
+    }
+  } else if (PH == PH_LAPE1 || PH == PH_LAPE2) {
+    if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, mixed::lap_edge<LL>(M, PH == PH_LAPE1 ? M.L1f : M.L2f, i));
+  } else if (PH == PH_LAPCV) {
+    if (M.nu4 != 0) {
+      if (kind == 0) ISW_BATCH_L(d.L, LMAXK, (mixed::div_cell<LL, float>(M, M.L1f, i)));
+      else ISW_BATCH_L(d.L, LMAXK, (mixed::curl_vertex<LL, float>(M, M.L1f, i)));
+    }
+  } else if (PH == PH_A) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, mixed::bern_cell<LL>(M, a.hs, a.us, i));
+    else ISW_BATCH_L(d.L, LMAXK, mixed::pv_vertex<LL>(M, a.hs, a.us, i));
+  } else if (PH == PH_E) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, mixed::edge_hq<LL>(M, a.hs, a.us, i));
+  } else if (PH == PH_S) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, mixed::slow_edge<LL>(M, a.us, a.cdt, i));
+  } else if (PH == PH_ETA) {
+    if (!d.tiled && j < d.n[st]) mixed::bt_eta_cell(M, (float)d.tau[st], j, i);
+  } else if (PH == PH_U) {
+    if (!d.tiled && j < d.n[st]) mixed::bt_u_edge(M, (float)d.tau[st], i);
+  } else if (PH == PH_C) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, mixed::scale_cell<LL>(M, a, i));
+  } else if (PH == PH_D) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, mixed::h_cell<LL>(M, a, i));
+    else ISW_BATCH_L(d.L, LMAXK, mixed::u_edge<LL>(M, a, i));
+  } else if (PH == PH_POST) {
+    if (kind == 1) {
+      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
+    } else {
+      ISW_BATCH_L(d.L, LMAXK, mixed::tr_p1<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+    }
+  } else if (PH == PH_P2) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_p2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P3) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_p3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P4) {
+    const int jj = i / M.g.N, c = i % M.g.N;
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_p4<LL>(d.T, d.tr, jj, c));
+    if (jj == 0)
+      for (int l = 0; l < d.L; l++) d.Mm[(size_t)l * M.g.N + c] = d.tr.M1[(size_t)l * M.g.N + c];
+  }
+}
+
+// The fast loop of stage `st` over every tiled stack in the mixed form (the tile scheme of batch.cu's k_fast): per cell
+// deta, its previous value, 1/area, Gc and c0 = sum sign l_e H_e ubar0 (FP32); per edge dub, G', 1/d_e and l_e H_e
+// (FP32); per owned edge acc (FP64). Exchange buffers xeta[r & 1] and xdub[r & 1]; the final dub and acc go to dub and
+// acc, which no round reads.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
+                                                      int rounds, GridBarrier *bar, int *status, long long timeout_ns,
+                                                      int fault_block) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const TileRef tr = refs[blockIdx.x];
+  const StackDesc &d = S[tr.s];
+  const LayersDev &M = d.M;
+  const TileSetDev &T = d.tiles;
+  const int p = tr.p, k = T.k;
+  const int c0i = T.cell_off[p], nc = T.cell_off[p + 1] - c0i;
+  const int e0 = T.edge_off[p], ne = T.edge_off[p + 1] - e0;
+  const int eown = T.eown[p];
+  const int *cells = T.cells + c0i;
+  const int *edges = T.edges + e0;
+  const int *ncnt = T.ncnt + (size_t)p * (k + 1);
+  const int *ecnt = T.ecnt + (size_t)p * (k + 1);
+  double *acc = reinterpret_cast<double *>(smem);        // owned edges only
+  float *deta = reinterpret_cast<float *>(acc + eown);
+  float *dprev = deta + nc;
+  float *rA = dprev + nc;
+  float *gc = rA + nc;
+  float *cz = gc + nc;
+  float *dub = cz + nc;
+  float *G = dub + ne;
+  float *rde = G + ne;
+  float *lh = rde + ne;
+  int16_t *cedge = reinterpret_cast<int16_t *>(lh + ne);
+  int16_t *eIl = cedge + (size_t)nc * 6;
+  int16_t *eJl = eIl + ne;
+  const int skip = (int)blockIdx.x == fault_block;
+  const int n = d.n[st];
+  const float tau = (float)d.tau[st], gam = (float)M.div_damp;
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    deta[c] = 0.f;
+    rA[c] = T.arA32[c0i + c];
+    gc[c] = M.Gc32[cells[c]];
+  }
+  for (int w = threadIdx.x; w < nc * 6; w += blockDim.x) cedge[w] = T.cedge[(size_t)c0i * 6 + w];
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    const int ge = edges[e];
+    dub[e] = (float)M.ub0[ge];              // ubar0 for the c0 pass below; then zero
+    G[e] = M.G32[ge];
+    rde[e] = T.arde32[e0 + e];
+    lh[e] = T.ale32[e0 + e] * M.He32[ge];
+    if (e < eown) acc[e] = 0.0;
+    eIl[e] = T.eIl[e0 + e];
+    eJl[e] = T.eJl[e0 + e];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int v = cedge[c * 6 + q];
+      if (v == 0) continue;
+      const int le_ = (v > 0 ? v : -v) - 1;
+      s += (v > 0 ? lh[le_] : -lh[le_]) * dub[le_];
+    }
+    cz[c] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) dub[e] = 0.f;
+  const int nown = ncnt[0];
+  for (int r = 0; r < rounds; r++) {
+    const int K = min(k, n - r * k);
+    if (r > 0) {
+      if (!grid_sync(bar, status, timeout_ns, skip)) return;
+      if (K > 0) {
+        const float *xe = M.xeta[(r - 1) & 1];
+        const float *xu = M.xdub[(r - 1) & 1];
+        for (int c = nown + threadIdx.x; c < nc; c += blockDim.x) deta[c] = xe[cells[c]];
+        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) dub[e] = xu[edges[e]];
+      }
+    }
+    __syncthreads();
+    for (int m = 1; m <= K; m++) {
+      const int cn = ncnt[K - m + 1];
+      for (int c = threadIdx.x; c < cn; c += blockDim.x) {
+        const float d0 = deta[c];
+        dprev[c] = d0;
+        float div = cz[c];
+        int vs[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) vs[q] = cedge[c * 6 + q];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+          const int v = vs[q];
+          if (v == 0) continue;
+          const int le_ = (v > 0 ? v : -v) - 1;
+          div += (v > 0 ? lh[le_] : -lh[le_]) * dub[le_];
+        }
+        deta[c] = d0 - tau * div * rA[c];
+      }
+      __syncthreads();
+      const int en = ecnt[K - m];
+      for (int e = threadIdx.x; e < en; e += blockDim.x) {
+        const float v = dub[e];
+        if (e < eown) acc[e] += (double)v;
+        const int i = eIl[e], jj = eJl[e];
+        const float xj = deta[jj] + gam * (deta[jj] - dprev[jj]);
+        const float xi = deta[i] + gam * (deta[i] - dprev[i]);
+        dub[e] = v + tau * (G[e] - (gc[jj] * xj - gc[i] * xi) * rde[e]);
+      }
+      __syncthreads();
+    }
+    if (r + 1 < rounds && K > 0) {
+      float *xe = M.xeta[r & 1];
+      float *xu = M.xdub[r & 1];
+      for (int c = threadIdx.x; c < nown; c += blockDim.x) xe[cells[c]] = deta[c];
+      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = dub[e];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < eown; e += blockDim.x) {
+    M.dub[edges[e]] = dub[e];
+    M.acc[edges[e]] = acc[e];
+  }
+}
+
+template <int PH>
+void launch_m(int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j) {
+  switch (lmax) {
+    case 2: k_phase_m<PH, 2><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
+    case 3: k_phase_m<PH, 3><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
+    case 5: k_phase_m<PH, 5><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
+    default: k_phase_m<PH, 8><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
+  }
+}
+
+}  // namespace
+
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j) {
+  switch (ph) {
+    case PH_INIT: launch_m<PH_INIT>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_LAPE1: launch_m<PH_LAPE1>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_LAPCV: launch_m<PH_LAPCV>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_LAPE2: launch_m<PH_LAPE2>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_A: launch_m<PH_A>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_E: launch_m<PH_E>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_S: launch_m<PH_S>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_U: launch_m<PH_U>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_C: launch_m<PH_C>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_D: launch_m<PH_D>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_POST: launch_m<PH_POST>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P2: launch_m<PH_P2>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P3: launch_m<PH_P3>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P4: launch_m<PH_P4>(lmax, nb, st, desc, sc, stage, j); break;
+    default: break;
+  }
+}
+
+const void *fast_kernel_mixed(int bps) {
+  return bps == 2 ? (const void *)k_fast_m<512, 2> : (const void *)k_fast_m<1024, 1>;
+}
+
+void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
+                       GridBarrier *bar, int *status, long long timeout_ns, int fault_block) {
+  if (bps == 2)
+    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_m<512, 2>, desc, refs, stage, rounds, bar, status, timeout_ns, fault_block));
+  else
+    ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_m<1024, 1>, desc, refs, stage, rounds, bar, status, timeout_ns, fault_block));
+}
+
+}  // namespace bt
+}  // namespace isw

@@ -32,7 +32,7 @@ struct GridDev {
   const int *eI, *eJ, *nbr, *cellEdge, *cellEdgeAsc, *ev1, *ev2, *vEdge, *vCell, *eoeStart, *eoe, *d2idx;
   const int8_t *cellSign, *vEdgeSign, *vSlot;
   const double *le, *de, *areaCell, *areaV, *fV, *kite, *w, *d2wt;
-  const float *w32, *d2wt32, *le32, *de32, *rde32, *rA32, *rAV32, *kite32;
+  const float *w32, *d2wt32, *le32, *de32, *rde32, *rle32, *rA32, *rAV32, *kite32;
   const double *rA, *rde, *rAV;   // FP64 reciprocals (mixed form multiplies where the reference divides)
 };
 
@@ -46,8 +46,12 @@ struct LayersDev {
   double *B, *q, *Tp, *F, *scale, *G, *He, *ubs, *ub0, *ub, *acc, *eta0, *eta, *eta_prev;
   double *h1, *h2, *u1, *u2, *D1, *Z1, *L1, *L2, *hedge, *diss, *pk;
   double *ub2;                               // second exchange buffer of the tiled fast loop
-  float *q32, *B32, *Tp32, *G32, *pk32;      // mixed-form scratch
   double *red;                               // reduction scratch (substeps)
+  // mixed-form scratch (allocated for ISW_MIXED only): FP32 stage winds and operators; the fast loop in deviation form
+  // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)
+  float *u32, *u1f, *u2f, *D1f, *Z1f, *L1f, *L2f, *q32, *Tp32, *G32, *He32, *ubs32, *Gc32;
+  float *c0, *dub, *deta, *deprev, *xeta[2], *xdub[2];
+  float4 *pk4;
 };
 
 // Arguments of one RK3 stage (reference layers.py:129-183).

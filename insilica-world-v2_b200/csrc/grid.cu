@@ -185,6 +185,9 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     d.w32 = upload_f32(g, h->w, nE2); d.d2wt32 = upload_f32(g, d2w.data(), d2w.size());
     d.le32 = upload_f32(g, h->le, E); d.de32 = upload_f32(g, h->de, E); d.rde32 = upload_f32(g, rde.data(), E);
     d.rA32 = upload_f32(g, rA.data(), N); d.rAV32 = upload_f32(g, rAV.data(), NV);
+    std::vector<double> rle(E);
+    for (int e = 0; e < E; e++) rle[e] = 1.0 / h->le[e];
+    d.rle32 = upload_f32(g, rle.data(), E);
     d.kite32 = upload_f32(g, h->kite, (size_t)N * 6);
     g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
     g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);

@@ -13,6 +13,8 @@ struct GraphEntry {
   cudaGraphExec_t exec;
 };
 
+struct isw_batch;
+
 struct isw_layers {
   isw_grid *grid;
   isw::LayersDev d;
@@ -21,6 +23,11 @@ struct isw_layers {
   std::list<GraphEntry> graphs;     // most recent first
   int colmax_blocks;
   int *nonfinite;
+  // the mixed form steps call by call through a private one-stack batch (its step graph and tiles)
+  isw_batch *solo = nullptr;
+  int solo_slot = -1;
+  GraphEntry solo_key{};
+  double *solo_Fm = nullptr;        // Fm when the caller passes none
 };
 
 struct isw_transport {

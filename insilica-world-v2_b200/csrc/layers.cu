@@ -148,6 +148,15 @@ double *dalloc(isw_layers *s, size_t n) {
   return (double *)p;
 }
 
+template <class T>
+T *talloc_t(isw_layers *s, size_t n) {
+  void *p = nullptr;
+  ISW_CUDA(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+  s->allocs.push_back(p);
+  ISW_CUDA(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
+  return (T *)p;
+}
+
 // The step's kernels in order on `st` (reference layers.py:185-212, Boussinesq branch).
 void enqueue_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
   const LayersDev &M = s->d;
@@ -197,7 +206,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
   if (!g || !p) fail(ISW_EINVAL, "layers: null grid or parameters");
   if (p->L < 1 || p->L > LMAX) fail(ISW_EINVAL, "layers: L must be in 1..8");
   if (p->L > 1 && !p->gprime) fail(ISW_EINVAL, "layers: gprime needs L - 1 values");
-  if (p->precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers: the mixed form is not built yet");
+  if (p->precision != ISW_FP64 && p->precision != ISW_MIXED) fail(ISW_EINVAL, "layers: precision must be ISW_FP64 or ISW_MIXED");
   ISW_CUDA(cudaSetDevice(g->device));
   isw_layers *s = new isw_layers();
   s->grid = g;
@@ -241,6 +250,18 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.D1 = dalloc(s, (size_t)L * N); d.Z1 = dalloc(s, (size_t)L * NV); d.L1 = dalloc(s, (size_t)L * E); d.L2 = dalloc(s, (size_t)L * E);
     d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
     d.ub2 = dalloc(s, E);
+    if (p->precision == ISW_MIXED) {
+      auto f = [&](size_t n) { return talloc_t<float>(s, n); };
+      d.u32 = f((size_t)L * E); d.u1f = f((size_t)L * E); d.u2f = f((size_t)L * E);
+      d.D1f = f((size_t)L * N); d.Z1f = f((size_t)L * NV); d.L1f = f((size_t)L * E); d.L2f = f((size_t)L * E);
+      d.q32 = f((size_t)L * NV); d.Tp32 = f((size_t)L * E); d.G32 = f(E); d.He32 = f(E); d.ubs32 = f(E);
+      d.c0 = f(N); d.dub = f(E); d.deta = f(N); d.deprev = f(N);
+      d.xeta[0] = f(N); d.xeta[1] = f(N); d.xdub[0] = f(E); d.xdub[1] = f(E);
+      d.pk4 = talloc_t<float4>(s, (size_t)L * E);
+      std::vector<float> gc32(N, (float)p->grav);
+      d.Gc32 = f(N);
+      ISW_CUDA(cudaMemcpy(d.Gc32, gc32.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    }
     s->colmax_blocks = blocks_for(N) < 1024 ? blocks_for(N) : 1024;
     d.red = dalloc(s, s->colmax_blocks + 1);
     void *nf = nullptr;
@@ -258,16 +279,41 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
 
 void layers_destroy(isw_layers *s) {
   cudaSetDevice(s->grid->device);
+  if (s->solo) isw_batch_destroy(s->solo);
   for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);
   if (s->cap) cudaStreamDestroy(s->cap);
   for (void *p : s->allocs) cudaFree(p);
   delete s;
 }
 
+// The mixed form call by call: a private batch holding this one stack (rebuilt when the arrays, dt or nfast change).
+void layers_step_mixed(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
+  auto ok = [](int rc) { if (rc != ISW_OK) fail(rc, isw_last_error()); };
+  if (!s->solo) ok(isw_batch_create(s->grid->device, &s->solo));
+  if (!Fm) {
+    if (!s->solo_Fm) s->solo_Fm = dalloc(s, (size_t)s->d.L * s->d.g.E);
+    Fm = s->solo_Fm;
+  }
+  GraphEntry &k = s->solo_key;
+  if (s->solo_slot < 0 || k.h != h || k.u != u || k.Fm != Fm || k.dt != dt || k.nfast != nfast) {
+    if (s->solo_slot >= 0) ok(isw_batch_remove(s->solo, s->solo_slot));
+    s->solo_slot = -1;
+    int slot = -1;
+    ok(isw_batch_add(s->solo, s, nullptr, h, u, Fm, nullptr, nullptr, nullptr, 0, dt, nfast, &slot));
+    s->solo_slot = slot;
+    k = GraphEntry{h, u, Fm, dt, nfast, nullptr};
+  }
+  ok(isw_batch_step(s->solo, st));
+}
+
 void layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
   if (!h || !u) fail(ISW_EINVAL, "layers.step: null h or u");
   if (nfast < 1) fail(ISW_EINVAL, "layers.step: nfast must be >= 1");
   if (!(dt > 0) || !std::isfinite(dt)) fail(ISW_EINVAL, "layers.step: dt must be positive and finite");
+  if (s->d.precision == ISW_MIXED) {
+    layers_step_mixed(s, h, u, Fm, dt, nfast, st);
+    return;
+  }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   ISW_CUDA(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) {   // the caller is capturing a graph of its own: just queue the kernels

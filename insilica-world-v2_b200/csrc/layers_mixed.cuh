@@ -1,0 +1,372 @@
+// Phase functions of the time-split RK3 step, mixed form: the same phases as layers_fp64.cuh (reference layers.py:129-212),
+// with momentum, the TRiSK operators and the slow tendencies in FP32 and the quantities whose size dwarfs their change
+// in FP64, so that FP32 rounding only ever lands on small numbers:
+//   FP64  thicknesses h (stage and final), the layer fluxes F and the limiter, the Montgomery potential B, the free
+//         surface eta0, the barotropic wind at the step start ubar0 and the sub-step sum acc, the final wind u = u0 +
+//         dt T' + (ubar - ubar0), the interfacial stress (vmix);
+//   FP32  the stage winds u1, u2 (and u's FP32 copy for stage 1), q, the packed neighbour record, the PV flux, KE, the
+//         Laplacians, T' and the column force, H_e, and the fast loop's state.
+// The fast loop runs in deviation form: deta = eta - eta0 and dub = ubar - ubar0, both zero at each stage's start and
+// small, with eta0's gradient folded into the column force once per stage (G' = G - (Gc_J eta0_J - Gc_I eta0_I) / d_e)
+// and ubar0's divergence once per cell (c0 = sum sign l_e H_e ubar0); acc sums dub in FP64, so the mean barotropic wind
+// is ubar0 + acc / n. Division by a fixed grid quantity multiplies by its stored reciprocal (as the reference's mixed
+// form does, layers.cu:15-21). Mass stays exact to FP64 rounding: each edge's flux is one FP64 value used by both cells.
+#pragma once
+#include "common.cuh"
+#include "layers_fp64.cuh"
+
+namespace isw {
+namespace mixed {
+
+// Stage arguments of the mixed form: stage winds in FP32; the final stage writes the caller's FP64 u.
+struct MStageArgs {
+  const double *hs, *h0, *u0;
+  const float *us, *u0f;
+  double *hn, *un, *Fm;        // un: the final stage only
+  float *unf;                  // stages 1 and 2
+  double cdt, dt, inv_n;
+  float tau;
+  int n;
+};
+
+// ---- init: u's FP32 copy with the column wind ubar0 (FP64), and the Laplacian passes in FP32 ----
+template <int L>
+__device__ __forceinline__ void ubar0_edge(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int e) {
+  const int N = M.g.N, E = M.g.E;
+  const int a = M.g.eI[e], b = M.g.eJ[e];
+  double H = 0, U = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double he = 0.5 * (h[(size_t)k * N + a] + h[(size_t)k * N + b]);
+    const double ue = u[(size_t)k * E + e];
+    H += he;
+    U += he * ue;
+    M.u32[(size_t)k * E + e] = (float)ue;
+  }
+  M.ub0[e] = U / H;
+}
+
+template <int L, class T>
+__device__ __forceinline__ void div_cell(const LayersDev &M, const T *__restrict__ u, int i) {
+  const GridDev &g = M.g;
+  int es[6];
+  float c[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdge[i * 6 + s];
+    es[s] = e;
+    c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] : 0.f;
+  }
+  const float rA = g.rA32[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const T *ul = u + (size_t)k * g.E;
+    float s = 0;
+#pragma unroll
+    for (int t = 0; t < 6; t++)
+      if (es[t] >= 0) s += c[t] * (float)ul[es[t]];
+    M.D1f[(size_t)k * g.N + i] = s * rA;
+  }
+}
+
+template <int L, class T>
+__device__ __forceinline__ void curl_vertex(const LayersDev &M, const T *__restrict__ u, int v) {
+  const GridDev &g = M.g;
+  int es[3];
+  float c[3];
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const int e = g.vEdge[v * 3 + s];
+    es[s] = e;
+    c[s] = (float)g.vEdgeSign[v * 3 + s] * g.de32[e];
+  }
+  const float rA = g.rAV32[v];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const T *ul = u + (size_t)k * g.E;
+    float z = 0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) z += c[s] * (float)ul[es[s]];
+    M.Z1f[(size_t)k * g.NV + v] = z * rA;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void lap_edge(const LayersDev &M, float *__restrict__ out, int e) {
+  const GridDev &g = M.g;
+  const int a = g.eI[e], b = g.eJ[e], v1 = g.ev1[e], v2 = g.ev2[e];
+  const float rde = g.rde32[e], rle = g.rle32[e];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const float *Dl = M.D1f + (size_t)k * g.N;
+    const float *Zl = M.Z1f + (size_t)k * g.NV;
+    out[(size_t)k * g.E + e] = (Dl[b] - Dl[a]) * rde - (Zl[v2] - Zl[v1]) * rle;
+  }
+}
+
+// ---- stage phase A: B (FP64 Montgomery part plus FP32 kinetic energy), q (FP32) ----
+template <int L>
+__device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__restrict__ h, const float *__restrict__ u, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double z[L];
+  double s = M.b[i];
+#pragma unroll
+  for (int k = L - 1; k >= 0; k--) { s += h[(size_t)k * N + i]; z[k] = s; }
+  int es[6];
+  float c[6];
+#pragma unroll
+  for (int t = 0; t < 6; t++) {
+    const int e = g.cellEdge[i * 6 + t];
+    es[t] = e;
+    c[t] = e >= 0 ? g.le32[e] * g.de32[e] * 0.25f : 0.f;
+  }
+  const float rA = g.rA32[i];
+  double Mp = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    if (k > 0) Mp += M.gp[k - 1] * z[k];
+    const float *ul = u + (size_t)k * E;
+    float ke = 0;
+#pragma unroll
+    for (int t = 0; t < 6; t++)
+      if (es[t] >= 0) {
+        const float ue = ul[es[t]];
+        ke += c[t] * ue * ue;
+      }
+    M.B[(size_t)k * N + i] = Mp + (double)(ke * rA);
+  }
+  M.deta[i] = 0.f;                       // the grid-wide fast loop's start (tiles start from zero themselves)
+}
+
+template <int L>
+__device__ __forceinline__ void pv_vertex(const LayersDev &M, const double *__restrict__ h, const float *__restrict__ u, int v) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E, NV = g.NV;
+  int cs[3], es[3];
+  float kw[3], c[3];
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const int cc = g.vCell[v * 3 + s];
+    cs[s] = cc;
+    kw[s] = g.kite32[cc * 6 + g.vSlot[v * 3 + s]];
+    const int e = g.vEdge[v * 3 + s];
+    es[s] = e;
+    c[s] = (float)g.vEdgeSign[v * 3 + s] * g.de32[e];
+  }
+  const float rAv = g.rAV32[v], f = (float)M.fV[v];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double *hl = h + (size_t)k * N;
+    const float *ul = u + (size_t)k * E;
+    float hv = 0, z = 0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) hv += kw[s] * (float)hl[cs[s]];
+#pragma unroll
+    for (int s = 0; s < 3; s++) z += c[s] * ul[es[s]];
+    M.q32[(size_t)k * NV + v] = (z * rAv + f) / (hv * rAv);
+  }
+}
+
+// ---- stage phase E: the packed neighbour record (h_e, u, q_e) per edge and layer; fast-loop accumulators to zero ----
+template <int L>
+__device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__restrict__ h, const float *__restrict__ u, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E, NV = g.NV;
+  const int a = g.eI[e], b = g.eJ[e], v1 = g.ev1[e], v2 = g.ev2[e];
+  float4 *pp = M.pk4 + (size_t)e * L;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const float hv = (float)(0.5 * (h[(size_t)k * N + a] + h[(size_t)k * N + b]));
+    const float qv = 0.5f * (M.q32[(size_t)k * NV + v1] + M.q32[(size_t)k * NV + v2]);
+    pp[k] = make_float4(hv, u[(size_t)k * E + e], qv, 0.f);
+  }
+  M.dub[e] = 0.f;
+  M.acc[e] = 0.0;
+}
+
+// ---- stage phase S: slow tendencies in FP32; the pressure gradient from the FP64 B ----
+template <int L>
+__device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__restrict__ u, double dts, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  float he[L], cap[L], qf[L], Q[L];
+  const float thin = (float)M.thin;
+  const float4 *pe = M.pk4 + (size_t)e * L;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const float4 p = pe[k];
+    he[k] = p.x;
+    cap[k] = thin * p.x;
+    qf[k] = p.z;
+    Q[k] = 0.f;
+  }
+  const int m0 = g.eoeStart[e], m1 = g.eoeStart[e + 1];
+  for (int m = m0; m < m1; m++) {
+    const float wm = g.w32[m];
+    const float4 *pp = M.pk4 + (size_t)g.eoe[m] * L;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const float4 p = pp[k];
+      Q[k] += wm * (fminf(p.x, cap[k]) * p.y) * 0.5f * (qf[k] + p.z);
+    }
+  }
+  const int a = g.eI[e], b = g.eJ[e];
+  const double rde = g.rde[e];
+  const float fdts = (float)dts, flo = (float)M.floor_, nu4 = (float)M.nu4;
+  float T[L];
+  float H = 0, U = 0, GT = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const float ue = u[(size_t)k * E + e];
+    const double *Bl = M.B + (size_t)k * N;
+    float d = Q[k] - (float)((Bl[b] - Bl[a]) * rde) - (float)M.drag[k] * ue;
+    const float ck = (float)M.stress[k];
+    if (ck != 0.f) {
+      const float r = ck / fmaxf(he[k], flo);
+      const float rd = r * fdts;
+      d -= (rd > 1e-8f ? -expm1f(-rd) / fdts : r) * ue;     // exact exponential decay over the stage
+    }
+    if (nu4 != 0.f) d -= nu4 * M.L2f[(size_t)k * E + e];
+    T[k] = d;
+    H += he[k];
+    U += he[k] * ue;
+  }
+#pragma unroll
+  for (int k = 0; k < L; k++) GT += he[k] * T[k];
+  const float gm = GT / H;
+#pragma unroll
+  for (int k = 0; k < L; k++) M.Tp32[(size_t)k * E + e] = T[k] - gm;
+  const double gb = (M.Gc[b] * M.eta0[b] - M.Gc[a] * M.eta0[a]) * rde;   // eta0's gradient, FP64
+  M.G32[e] = (float)((double)gm - gb);
+  M.He32[e] = H;
+  M.ubs32[e] = U / H;
+}
+
+// ---- fast loop, grid-wide form (stacks without tiles): deviation variables ----
+__device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int i) {
+  const GridDev &g = M.g;
+  int es[6];
+  float c[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = g.cellEdge[i * 6 + s];
+    es[s] = e;
+    c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] * M.He32[e] : 0.f;
+  }
+  float c0;
+  if (j == 0) {
+    c0 = 0.f;
+#pragma unroll
+    for (int s = 0; s < 6; s++)
+      if (es[s] >= 0) c0 += c[s] * (float)M.ub0[es[s]];
+    M.c0[i] = c0;
+  } else {
+    c0 = M.c0[i];
+  }
+  const float d0 = M.deta[i];
+  M.deprev[i] = d0;
+  float div = c0;
+#pragma unroll
+  for (int s = 0; s < 6; s++)
+    if (es[s] >= 0) div += c[s] * M.dub[es[s]];
+  M.deta[i] = d0 - tau * div * g.rA32[i];
+}
+
+__device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) {
+  const GridDev &g = M.g;
+  const float v = M.dub[e];
+  M.acc[e] += (double)v;
+  const int i = g.eI[e], j = g.eJ[e];
+  const float gam = (float)M.div_damp;
+  const float xj = M.deta[j] + gam * (M.deta[j] - M.deprev[j]);
+  const float xi = M.deta[i] + gam * (M.deta[i] - M.deprev[i]);
+  M.dub[e] = v + tau * (M.G32[e] - (M.Gc32[j] * xj - M.Gc32[i] * xi) * g.rde32[e]);
+}
+
+// ---- stage phase C: layer fluxes (FP64) and the floor limiter ----
+template <int L>
+__device__ __forceinline__ void scale_cell(const LayersDev &M, const MStageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double out[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) out[k] = 0;
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdgeAsc[i * 6 + s];
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = es[s];
+    if (e < 0) continue;
+    const int ea = g.eI[e], eb = g.eJ[e];
+    const bool mine = ea == i;
+    const float ubs = M.ubs32[e];
+    const double ubm = M.ub0[e] + M.acc[e] * a.inv_n, le = g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const double he = 0.5 * (a.hs[(size_t)k * N + ea] + a.hs[(size_t)k * N + eb]);
+      const double F = he * ((double)(a.us[(size_t)k * E + e] - ubs) + ubm);
+      if (mine) M.F[(size_t)k * E + e] = F;
+      const double f = F * le * a.cdt;
+      if (mine) { if (f > 0) out[k] += f; }
+      else if (!(f > 0)) out[k] -= f;
+    }
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double avail = a.h0[(size_t)k * N + i] - M.floor_;
+    const double cap = (avail > 0 ? avail : 0.0) * A;
+    M.scale[(size_t)k * N + i] = out[k] > cap ? cap / out[k] : 1.0;
+  }
+}
+
+// ---- stage phase D: h (FP64) and the stage wind ----
+template <int L>
+__device__ __forceinline__ void h_cell(const LayersDev &M, const MStageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N;
+  double div[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) div[k] = 0;
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = es[s];
+    if (e < 0) continue;
+    const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) div[k] += c * fp64::limited(M, k, e);
+  }
+  const double rA = g.rA[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const size_t o = (size_t)k * N + i;
+    a.hn[o] = a.h0[o] - a.cdt * div[k] * rA;
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void u_edge(const LayersDev &M, const MStageArgs &a, int e) {
+  const GridDev &g = M.g;
+  const int E = g.E;
+  const float dub = M.dub[e];
+  const double le = g.le[e];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const size_t o = (size_t)k * E + e;
+    const float tp = M.Tp32[o];
+    if (a.un) {
+      if (a.Fm) a.Fm[o] = fp64::limited(M, k, e) * le * a.dt;
+      a.un[o] = a.u0[o] + (a.cdt * (double)tp + (double)dub);
+    } else {
+      a.unf[o] = a.u0f[o] + ((float)a.cdt * tp + dub);
+    }
+  }
+}
+
+}  // namespace mixed
+}  // namespace isw

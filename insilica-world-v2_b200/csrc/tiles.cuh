@@ -32,6 +32,9 @@ struct TileSetHost {
 // Per-tile shared-memory bytes: per cell eta, eta_prev, area, Gc (8 B each) and 6 signed local edge ids (2 B); per
 // edge ubar, G, d_e, l_e H_e (8 B each) and two local cell ids (2 B); per owned edge the sub-step sum acc (8 B).
 inline size_t tile_smem_bytes(size_t nc, size_t ne, size_t nown) { return nc * (4 * 8 + 6 * 2) + ne * (4 * 8 + 2 * 2) + nown * 8 + 64; }
+// The mixed form's tile: per cell deta, its previous value, 1/area, Gc, c0 (4 B each) and the edge ids; per edge dub,
+// G', 1/d_e, l_e H_e (4 B each) and the cell ids; per owned edge acc (8 B).
+inline size_t tile_smem_bytes_mixed(size_t nc, size_t ne, size_t nown) { return nc * (5 * 4 + 6 * 2) + ne * (4 * 4 + 2 * 2) + nown * 8 + 64; }
 
 // Compact balanced partition of the N cells into P regions (owner per cell).
 std::vector<int32_t> partition_cells(int N, const int32_t *nbr, int P);

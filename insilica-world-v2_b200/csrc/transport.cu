@@ -114,7 +114,7 @@ int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int preci
     if (!g || !out) fail(ISW_EINVAL, "transport: null grid or output handle");
     if (L < 1 || L > LMAX) fail(ISW_EINVAL, "transport: L must be in 1..8");
     if (tracers < 1 || tracers > TRMAX) fail(ISW_EINVAL, "transport: tracers must be in 1..16");
-    if (precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "transport: the mixed form is not built yet");
+    if (precision != ISW_FP64 && precision != ISW_MIXED) fail(ISW_EINVAL, "transport: precision must be ISW_FP64 or ISW_MIXED");
     ISW_CUDA(cudaSetDevice(g->device));
     isw_transport *t = new isw_transport();
     t->grid = g;
@@ -127,6 +127,10 @@ int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int preci
       t->d.g = g->d;
       t->d.psi0 = talloc(t, R * N); t->d.td = talloc(t, R * N); t->d.p1 = talloc(t, R * N); t->d.p2 = talloc(t, R * N);
       t->d.Rp = talloc(t, R * N); t->d.Rm = talloc(t, R * N); t->d.A = talloc(t, R * E);
+      if (precision == ISW_MIXED) {            // the batched step's mixed FCT: FP32 stage fields, fluxes and ratios
+        auto f = [&](size_t n) { return reinterpret_cast<float *>(talloc(t, (n + 1) / 2)); };
+        t->d.p1f = f(R * N); t->d.p2f = f(R * N); t->d.Af = f(R * E); t->d.Rpf = f(R * N); t->d.Rmf = f(R * N);
+      }
     } catch (...) {
       for (void *p : t->allocs) cudaFree(p);
       delete t;

@@ -17,6 +17,7 @@ namespace isw {
 struct TransportDev {
   GridDev g;
   double *psi0, *td, *p1, *p2, *A, *Rp, *Rm;   // rows x N (A rows x E); psi0 holds the tracers as they came in
+  float *p1f, *p2f, *Af, *Rpf, *Rmf;           // the mixed form's FP32 stage fields, antidiffusive fluxes and ratios
 };
 
 // Per-call arguments: the masses, the fluxes and the caller's tracer arrays.

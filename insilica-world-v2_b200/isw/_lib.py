@@ -63,8 +63,9 @@ isw_batch_destroy = _sig('isw_batch_destroy', I, [P])
 isw_batch_add = _sig('isw_batch_add', I, [P, P, P, P, P, P, P, P, ctypes.POINTER(P), I, D, I, ctypes.POINTER(I)])
 isw_batch_remove = _sig('isw_batch_remove', I, [P, I])
 isw_batch_step = _sig('isw_batch_step', I, [P, P])
-isw_batch_config = _sig('isw_batch_config', I, [P, I, I])
-isw_batch_info = _sig('isw_batch_info', I, [P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(LL)])
+isw_batch_config = _sig('isw_batch_config', I, [P, I, I, I, I, I])
+isw_batch_info = _sig('isw_batch_info', I, [P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(LL),
+                                             ctypes.POINTER(I), ctypes.POINTER(I)])
 isw_batch_status = _sig('isw_batch_status', I, [P, P, I])
 isw_batch_fault_test = _sig('isw_batch_fault_test', I, [P, LL, P])
 

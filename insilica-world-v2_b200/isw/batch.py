@@ -1,7 +1,9 @@
-"""Batched persistent steps (the reference's Ensemble, src/insilica/ensemble.py, as one launch): stacks registered once
-and advanced together, each RK3 step + receiving masses + FCT transport + M <- M1 of every stack in ONE cooperative
-kernel launch per step. A stack's results are bit-identical to stepping it alone through Layers/Transport."""
+"""Batched steps (the reference's Ensemble, src/insilica/ensemble.py, as one CUDA graph): stacks registered once and
+advanced together, each RK3 step + receiving masses + FCT transport + M <- M1 of every stack in one graph launch per
+step (one kernel per phase over all stacks, the barotropic sub-steps in shared-memory tiles). A stack's results are
+bit-identical to stepping it alone through Layers/Transport. `autotune` picks the tile layout by timing the batch."""
 import ctypes
+import itertools
 
 from . import _lib
 from .gpu import device_ptr, stream_of
@@ -41,16 +43,65 @@ class Batch:
         _lib.check(_lib.isw_batch_remove(self._h, int(slot)))
         self._keep.pop(slot, None)
 
-    def config(self, tiles=True, tile_k=8):
+    LAYOUTS = {'auto': 0, 'shared': 1, 'packed': 2}
+
+    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0):
         """The fast loop in shared-memory tiles exchanging every k <= tile_k sub-steps (the largest that fits), or
-        grid-wide passes."""
-        _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k)))
+        grid-wide passes; layout 'shared' (one cooperative launch, tiles in proportion to each stack's cells), 'packed'
+        (tiles of about tile_cells owned cells, stacks packed into launches) or 'auto'; blocks_per_sm 1, 2 or 0 (auto)."""
+        self._config = dict(tiles=tiles, tile_k=tile_k, layout=layout, tile_cells=tile_cells, blocks_per_sm=blocks_per_sm)
+        _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k), self.LAYOUTS[layout], int(tile_cells),
+                                         int(blocks_per_sm)))
 
     def info(self):
-        """(stacks, tiles, exchange interval k, tile shared memory bytes) of the current layout."""
-        st, ti, k, sm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
-        _lib.check(_lib.isw_batch_info(self._h, ctypes.byref(st), ctypes.byref(ti), ctypes.byref(k), ctypes.byref(sm)))
-        return dict(stacks=st.value, tiles=ti.value, tile_k=k.value, smem=sm.value)
+        """The current layout: stacks, tiles, exchange interval k, the largest tile's shared memory (bytes), cooperative
+        launches per stage (groups), tile blocks per SM."""
+        v = [ctypes.c_int() for _ in range(3)] + [ctypes.c_longlong()] + [ctypes.c_int() for _ in range(2)]
+        _lib.check(_lib.isw_batch_info(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(stacks=v[0].value, tiles=v[1].value, tile_k=v[2].value, smem=v[3].value, groups=v[4].value,
+                    blocks_per_sm=v[5].value)
+
+    def autotune(self, steps=5, candidates=None, stream=None):
+        """Choose the fast-loop layout by timing: each candidate configuration (layout, blocks per SM, exchange interval,
+        tile size; or no tiles) runs `steps` batched steps after one warm-up step, timed with CUDA events; the fastest
+        stays configured. Every registered array is restored afterwards, so the stacks' states are as before. Returns
+        (best configuration, {configuration: ms per step})."""
+        import torch
+        arrays = []
+        for keep in self._keep.values():
+            core, tr, h, u, Fm, M, M1, tracers = keep
+            arrays += [a for a in (h, u, Fm, M, M1) + tuple(tracers) if a is not None]
+        saved = [a.clone() for a in arrays]
+        if candidates is None:
+            candidates = [dict(tiles=False)]
+            for layout, bps, k in itertools.product(('shared', 'packed'), (1, 2), (2, 4, 8)):
+                cells = (0,) if layout == 'shared' else ((256, 512) if bps == 2 else (512, 1024))
+                for c in cells:
+                    candidates.append(dict(tiles=True, layout=layout, blocks_per_sm=bps, tile_k=k, tile_cells=c))
+        dev = torch.device(f'cuda:{self.device}')
+        st = torch.cuda.current_stream(dev) if stream is None else stream
+        times, seen = {}, set()
+        for cand in candidates:
+            self.config(**cand)
+            lay = self.info()
+            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'])
+            if key in seen:                       # the same layout as an earlier candidate
+                continue
+            seen.add(key)
+            self.step(st)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                self.step(st)
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+            times[tuple(sorted(cand.items()))] = e0.elapsed_time(e1) / steps
+        best = dict(min(times, key=times.get))
+        self.config(**best)
+        for a, b in zip(arrays, saved):
+            a.copy_(b)
+        torch.cuda.synchronize(dev)
+        return best, times
 
     def step(self, stream=None):
         _lib.check(_lib.isw_batch_step(self._h, stream_of(self.device, stream)))

@@ -143,7 +143,7 @@ def test_barrier_timeout_reports_and_recovers(dev, grid4):
         assert torch.equal(x, y)
 
 
-@pytest.mark.parametrize('k', [1, 2, 3, 4, 7, 11])
+@pytest.mark.parametrize('k', [1, 2, 3, 4, 7, 8])
 def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
     """The barotropic sub-steps in shared-memory tiles (exchanging every k sub-steps) give the grid-wide passes' result
     bit for bit, and so does the call-by-call path."""
@@ -165,3 +165,58 @@ def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
     assert tiled.status() == 0 and flat.status() == 0
     for x, y, z in zip(a.state(), b.state(), c.state()):
         assert torch.equal(x, y) and torch.equal(x, z)
+
+
+@pytest.mark.parametrize('precision', ['double', 'mixed'])
+def test_packed_groups_equal_shared(dev, grid4, precision):
+    """Eight members in the packed layout (tiles of about 64 owned cells, more tiles than one cooperative launch holds,
+    so the fast loop runs as several launches per stage) give the shared layout's result bit for bit; in FP64 also the
+    grid-wide passes' result."""
+    from isw import gpu
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    gpu.set_precision(precision)
+    try:
+        dg = DeviceGrid(planet_grid(grid4))
+        packed, shared, flat = Batch(0), Batch(0), Batch(0)
+        packed.config(tiles=True, tile_k=4, layout='packed', tile_cells=64, blocks_per_sm=2)
+        shared.config(tiles=True, tile_k=4, layout='shared')
+        flat.config(tiles=False)
+        ms = [[Member(dg, 20 + i, ntracers=2, batch=bt) for i in range(8)] for bt in (packed, shared, flat)]
+    finally:
+        gpu.set_precision('double')
+    info = packed.info()
+    assert info['groups'] >= 2 and info['tiles'] > 296, info
+    for _ in range(3):
+        for bt in (packed, shared, flat):
+            bt.step()
+    torch.cuda.synchronize()
+    for bt in (packed, shared, flat):
+        assert bt.status() == 0
+    for a, b, c in zip(*ms):
+        for x, y, z in zip(a.state(), b.state(), c.state()):
+            assert torch.equal(x, y)
+            if precision == 'double':
+                assert torch.equal(x, z)
+            else:
+                assert float(torch.max(torch.abs(x - z)) / torch.max(torch.abs(z))) <= 1e-5
+
+
+def test_autotune_keeps_state(dev, grid4):
+    """The autotuner times candidate layouts on the live batch and restores every registered array: the stepped result
+    afterwards equals an untuned batch's bit for bit."""
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg = DeviceGrid(planet_grid(grid4))
+    tuned, plain = Batch(0), Batch(0)
+    a, b = Member(dg, 5, batch=tuned), Member(dg, 5, batch=plain)
+    best, times = tuned.autotune(steps=2)
+    assert best in [dict(k) for k in times] and len(times) >= 2
+    for _ in range(3):
+        tuned.step()
+        plain.step()
+    torch.cuda.synchronize()
+    for x, y in zip(a.state(), b.state()):
+        assert torch.equal(x, y)
