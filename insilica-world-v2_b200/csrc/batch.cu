@@ -105,19 +105,22 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
 }
 
 // The barotropic fast loop of stage `st` for every tiled stack (reference layers.cu:366-388, layers.py:168-175), one
-// block per tile, all tiles co-resident (cooperative launch). Same arithmetic as fp64::bt_eta_cell / bt_u_edge.
-// Exchange buffers (the owned values each round publishes, double-buffered by round parity): eta / eta_prev for the
-// surface and ub2 / F for the barotropic wind (F, the layer fluxes, is not in use during the fast loop). The final
-// barotropic wind and its accumulated sum go to ub and acc, which no round reads.
+// block per tile, all tiles of a group co-resident (cooperative launch). Same arithmetic as fp64::bt_eta_cell /
+// bt_u_edge: the cell pass also forms each updated cell's Y = Gc (eta + gamma (eta - eta_prev)), the expression the
+// reference's edge pass evaluates for each of an edge's two cells, so the edge pass reads two values per edge and no
+// eta_prev is kept. Shared memory per edge: (l_e H_e, ubar) and (G, d_e) as 16-byte pairs; per cell its 8 edge slots
+// as one 16-byte word. Exchange buffers (the owned values each round publishes, double-buffered by round parity):
+// eta / eta_prev for the surface and ub2 / F for the barotropic wind (F, the layer fluxes, is not in use during the fast
+// loop). The final barotropic wind and its accumulated sum go to ub and acc, which no round reads.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
                                                     int rounds, GridBarrier *bar, int *status, long long timeout_ns,
                                                     int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int cnt[2 * (FAST_KMAX + 1)];
   const TileRef tr = refs[blockIdx.x];
   const StackDesc &d = S[tr.s];
   const LayersDev &M = d.M;
-  const GridDev &g = M.g;
   const TileSetDev &T = d.tiles;
   const int p = tr.p, k = T.k;
   const int c0 = T.cell_off[p], nc = T.cell_off[p + 1] - c0;
@@ -125,42 +128,39 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
   const int eown = T.eown[p];
   const int *cells = T.cells + c0;
   const int *edges = T.edges + e0;
-  const int *ncnt = T.ncnt + (size_t)p * (k + 1);
-  const int *ecnt = T.ecnt + (size_t)p * (k + 1);
-  // shared memory: doubles first, then 16-bit ids
-  double *eta = reinterpret_cast<double *>(smem);
-  double *eprev = eta + nc;
-  double *area = eprev + nc;
+  double2 *EA = reinterpret_cast<double2 *>(smem);        // (l_e H_e, ubar)
+  double2 *EB = EA + ne;                                   // (G, d_e)
+  uint4 *cedge = reinterpret_cast<uint4 *>(EB + ne);       // 8 slots of +-(local edge + 1)
+  double *acc = reinterpret_cast<double *>(cedge + nc);    // owned edges only
+  double *eta = acc + eown;
+  double *Y = eta + nc;
+  double *area = Y + nc;
   double *gc = area + nc;
-  double *ub = gc + nc;
-  double *G = ub + ne;
-  double *de = G + ne;
-  double *lh = de + ne;                    // l_e H_e: with the cell's sign, the reference's (sign * l_e) * H_e
-  double *acc = lh + ne;                   // owned edges only
-  int16_t *cedge = reinterpret_cast<int16_t *>(acc + eown);
-  int16_t *eIl = cedge + (size_t)nc * 6;
-  int16_t *eJl = eIl + ne;
+  short2 *eij = reinterpret_cast<short2 *>(gc + nc);
   const int skip = (int)blockIdx.x == fault_block;
   const int n = d.n[st];
   const double tau = d.tau[st], gam = M.div_damp;
+  if (threadIdx.x <= k) {
+    cnt[threadIdx.x] = T.ncnt[(size_t)p * (k + 1) + threadIdx.x];
+    cnt[FAST_KMAX + 1 + threadIdx.x] = T.ecnt[(size_t)p * (k + 1) + threadIdx.x];
+  }
+  const uint4 *gcedge = reinterpret_cast<const uint4 *>(T.cedge) + c0;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
     const int gi = cells[c];
     eta[c] = M.eta0[gi];
     area[c] = T.aarea[c0 + c];
     gc[c] = M.Gc[gi];
+    cedge[c] = gcedge[c];
   }
-  for (int w = threadIdx.x; w < nc * 6; w += blockDim.x) cedge[w] = T.cedge[(size_t)c0 * 6 + w];
   for (int e = threadIdx.x; e < ne; e += blockDim.x) {
     const int ge = edges[e];
-    ub[e] = M.ub0[ge];
-    G[e] = M.G[ge];
-    de[e] = T.ade[e0 + e];
-    lh[e] = T.ale[e0 + e] * M.He[ge];
+    EA[e] = make_double2(T.ale[e0 + e] * M.He[ge], M.ub0[ge]);
+    EB[e] = make_double2(M.G[ge], T.ade[e0 + e]);
     if (e < eown) acc[e] = 0.0;
-    eIl[e] = T.eIl[e0 + e];
-    eJl[e] = T.eJl[e0 + e];
+    eij[e] = make_short2(T.eIl[e0 + e], T.eJl[e0 + e]);
   }
-  const int nown = ncnt[0];
+  __syncthreads();
+  const int nown = cnt[0];
   for (int r = 0; r < rounds; r++) {
     const int K = min(k, n - r * k);        // sub-steps of this stack in this round (<= 0: idle, barriers only)
     if (r > 0) {
@@ -170,38 +170,37 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
         const double *xu = ((r - 1) & 1) ? M.F : M.ub2;
         // only the halo: the owned cells and edges already hold exactly what was published
         for (int c = nown + threadIdx.x; c < nc; c += blockDim.x) eta[c] = xe[cells[c]];
-        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) ub[e] = xu[edges[e]];
+        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) EA[e].y = xu[edges[e]];
       }
     }
     __syncthreads();
     for (int m = 1; m <= K; m++) {
-      const int cn = ncnt[K - m + 1];
+      const int cn = cnt[K - m + 1];
       for (int c = threadIdx.x; c < cn; c += blockDim.x) {
         const double e0v = eta[c];
-        eprev[c] = e0v;
+        const uint4 w = cedge[c];
+        const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
+                           (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
         double div = 0;
-        int vs[6];
 #pragma unroll
-        for (int s = 0; s < 6; s++) vs[s] = cedge[c * 6 + s];
-#pragma unroll
-        for (int s = 0; s < 6; s++) {
-          const int v = vs[s];
+        for (int q = 0; q < 6; q++) {
+          const int v = vs[q];
           if (v == 0) continue;
-          const int le_ = (v > 0 ? v : -v) - 1;
-          const double cf = v > 0 ? lh[le_] : -lh[le_];
-          div += cf * ub[le_];
+          const double2 pr = EA[(v > 0 ? v : -v) - 1];
+          div += (v > 0 ? pr.x : -pr.x) * pr.y;
         }
-        eta[c] = e0v - (tau * div) / area[c];
+        const double en = e0v - (tau * div) / area[c];
+        eta[c] = en;
+        Y[c] = gc[c] * (en + gam * (en - e0v));
       }
       __syncthreads();
-      const int en = ecnt[K - m];
+      const int en = cnt[FAST_KMAX + 1 + K - m];
       for (int e = threadIdx.x; e < en; e += blockDim.x) {
-        const double v = ub[e];
+        const double v = EA[e].y;
+        const double2 gb = EB[e];
+        const short2 ij = eij[e];
         if (e < eown) acc[e] += v;
-        const int i = eIl[e], jj = eJl[e];
-        const double ej = gc[jj] * (eta[jj] + gam * (eta[jj] - eprev[jj]));
-        const double ei = gc[i] * (eta[i] + gam * (eta[i] - eprev[i]));
-        ub[e] = v + tau * ((-(ej - ei)) / de[e] + G[e]);
+        EA[e].y = v + tau * ((-(Y[ij.y] - Y[ij.x])) / gb.y + gb.x);
       }
       __syncthreads();
     }
@@ -209,12 +208,12 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
       double *xe = (r & 1) ? M.eta_prev : M.eta;
       double *xu = (r & 1) ? M.F : M.ub2;
       for (int c = threadIdx.x; c < nown; c += blockDim.x) xe[cells[c]] = eta[c];
-      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = ub[e];
+      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = EA[e].y;
     }
   }
   __syncthreads();
   for (int e = threadIdx.x; e < eown; e += blockDim.x) {
-    M.ub[edges[e]] = ub[e];
+    M.ub[edges[e]] = EA[e].y;
     M.acc[edges[e]] = acc[e];
   }
 }
@@ -294,7 +293,7 @@ int guarded(F f) {
 constexpr long long DEFAULT_TIMEOUT_NS = 2000000000LL;   // 2 s: far beyond any stage; only a broken grid reaches it
 constexpr size_t SMEM_TWO = 112 * 1024;                  // per tile block when two share an SM
 constexpr size_t SMEM_ONE = 224 * 1024;                  // per tile block alone on an SM
-constexpr int K_PROBE = 8;                               // the largest exchange interval considered
+constexpr int K_PROBE = FAST_KMAX;                       // the largest exchange interval considered
 
 template <class T>
 T *dupload(std::vector<void *> &allocs, const std::vector<T> &v) {

@@ -10,6 +10,8 @@
 namespace isw {
 namespace bt {
 
+constexpr int FAST_KMAX = 8;                  // the largest exchange interval of the tiled fast loop
+
 struct TileSetDev {
   int P, k;
   const int *cell_off, *edge_off, *cells, *edges, *ncnt, *ecnt, *eown;

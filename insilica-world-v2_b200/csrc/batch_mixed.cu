@@ -99,14 +99,15 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
 }
 
 // The fast loop of stage `st` over every tiled stack in the mixed form (the tile scheme of batch.cu's k_fast): per cell
-// deta, its previous value, 1/area, Gc and c0 = sum sign l_e H_e ubar0 (FP32); per edge dub, G', 1/d_e and l_e H_e
-// (FP32); per owned edge acc (FP64). Exchange buffers xeta[r & 1] and xdub[r & 1]; the final dub and acc go to dub and
-// acc, which no round reads.
+// deta, Y = Gc (deta + gamma (deta - deta_prev)), 1/area, Gc and c0 = sum sign l_e H_e ubar0 (FP32) and its 8 edge slots
+// (16 bytes); per edge (l_e H_e, dub, G', 1/d_e) as one 16-byte record; per owned edge acc (FP64). Exchange buffers
+// xeta[r & 1] and xdub[r & 1]; the final dub and acc go to dub and acc, which no round reads.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
                                                       int rounds, GridBarrier *bar, int *status, long long timeout_ns,
                                                       int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int cnt[2 * (FAST_KMAX + 1)];
   const TileRef tr = refs[blockIdx.x];
   const StackDesc &d = S[tr.s];
   const LayersDev &M = d.M;
@@ -117,55 +118,55 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
   const int eown = T.eown[p];
   const int *cells = T.cells + c0i;
   const int *edges = T.edges + e0;
-  const int *ncnt = T.ncnt + (size_t)p * (k + 1);
-  const int *ecnt = T.ecnt + (size_t)p * (k + 1);
-  double *acc = reinterpret_cast<double *>(smem);        // owned edges only
+  float4 *EF = reinterpret_cast<float4 *>(smem);           // (l_e H_e, dub, G', 1/d_e)
+  const float2 *EF2 = reinterpret_cast<const float2 *>(EF);
+  uint4 *cedge = reinterpret_cast<uint4 *>(EF + ne);
+  double *acc = reinterpret_cast<double *>(cedge + nc);    // owned edges only
   float *deta = reinterpret_cast<float *>(acc + eown);
-  float *dprev = deta + nc;
-  float *rA = dprev + nc;
+  float *Y = deta + nc;
+  float *rA = Y + nc;
   float *gc = rA + nc;
   float *cz = gc + nc;
-  float *dub = cz + nc;
-  float *G = dub + ne;
-  float *rde = G + ne;
-  float *lh = rde + ne;
-  int16_t *cedge = reinterpret_cast<int16_t *>(lh + ne);
-  int16_t *eIl = cedge + (size_t)nc * 6;
-  int16_t *eJl = eIl + ne;
+  short2 *eij = reinterpret_cast<short2 *>(cz + nc);
   const int skip = (int)blockIdx.x == fault_block;
   const int n = d.n[st];
   const float tau = (float)d.tau[st], gam = (float)M.div_damp;
+  if (threadIdx.x <= k) {
+    cnt[threadIdx.x] = T.ncnt[(size_t)p * (k + 1) + threadIdx.x];
+    cnt[FAST_KMAX + 1 + threadIdx.x] = T.ecnt[(size_t)p * (k + 1) + threadIdx.x];
+  }
+  const uint4 *gcedge = reinterpret_cast<const uint4 *>(T.cedge) + c0i;
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
     deta[c] = 0.f;
     rA[c] = T.arA32[c0i + c];
     gc[c] = M.Gc32[cells[c]];
+    cedge[c] = gcedge[c];
   }
-  for (int w = threadIdx.x; w < nc * 6; w += blockDim.x) cedge[w] = T.cedge[(size_t)c0i * 6 + w];
   for (int e = threadIdx.x; e < ne; e += blockDim.x) {
     const int ge = edges[e];
-    dub[e] = (float)M.ub0[ge];              // ubar0 for the c0 pass below; then zero
-    G[e] = M.G32[ge];
-    rde[e] = T.arde32[e0 + e];
-    lh[e] = T.ale32[e0 + e] * M.He32[ge];
+    // dub holds ubar0 for the c0 pass below, then zero
+    EF[e] = make_float4(T.ale32[e0 + e] * M.He32[ge], (float)M.ub0[ge], M.G32[ge], T.arde32[e0 + e]);
     if (e < eown) acc[e] = 0.0;
-    eIl[e] = T.eIl[e0 + e];
-    eJl[e] = T.eJl[e0 + e];
+    eij[e] = make_short2(T.eIl[e0 + e], T.eJl[e0 + e]);
   }
   __syncthreads();
   for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    const uint4 w = cedge[c];
+    const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
+                       (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
     float s = 0.f;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-      const int v = cedge[c * 6 + q];
+      const int v = vs[q];
       if (v == 0) continue;
-      const int le_ = (v > 0 ? v : -v) - 1;
-      s += (v > 0 ? lh[le_] : -lh[le_]) * dub[le_];
+      const float2 pr = EF2[2 * ((v > 0 ? v : -v) - 1)];
+      s += (v > 0 ? pr.x : -pr.x) * pr.y;
     }
     cz[c] = s;
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) dub[e] = 0.f;
-  const int nown = ncnt[0];
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) EF[e].y = 0.f;
+  const int nown = cnt[0];
   for (int r = 0; r < rounds; r++) {
     const int K = min(k, n - r * k);
     if (r > 0) {
@@ -174,37 +175,36 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
         const float *xe = M.xeta[(r - 1) & 1];
         const float *xu = M.xdub[(r - 1) & 1];
         for (int c = nown + threadIdx.x; c < nc; c += blockDim.x) deta[c] = xe[cells[c]];
-        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) dub[e] = xu[edges[e]];
+        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) EF[e].y = xu[edges[e]];
       }
     }
     __syncthreads();
     for (int m = 1; m <= K; m++) {
-      const int cn = ncnt[K - m + 1];
+      const int cn = cnt[K - m + 1];
       for (int c = threadIdx.x; c < cn; c += blockDim.x) {
         const float d0 = deta[c];
-        dprev[c] = d0;
+        const uint4 w = cedge[c];
+        const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
+                           (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
         float div = cz[c];
-        int vs[6];
-#pragma unroll
-        for (int q = 0; q < 6; q++) vs[q] = cedge[c * 6 + q];
 #pragma unroll
         for (int q = 0; q < 6; q++) {
           const int v = vs[q];
           if (v == 0) continue;
-          const int le_ = (v > 0 ? v : -v) - 1;
-          div += (v > 0 ? lh[le_] : -lh[le_]) * dub[le_];
+          const float2 pr = EF2[2 * ((v > 0 ? v : -v) - 1)];
+          div += (v > 0 ? pr.x : -pr.x) * pr.y;
         }
-        deta[c] = d0 - tau * div * rA[c];
+        const float dn = d0 - tau * div * rA[c];
+        deta[c] = dn;
+        Y[c] = gc[c] * (dn + gam * (dn - d0));
       }
       __syncthreads();
-      const int en = ecnt[K - m];
+      const int en = cnt[FAST_KMAX + 1 + K - m];
       for (int e = threadIdx.x; e < en; e += blockDim.x) {
-        const float v = dub[e];
-        if (e < eown) acc[e] += (double)v;
-        const int i = eIl[e], jj = eJl[e];
-        const float xj = deta[jj] + gam * (deta[jj] - dprev[jj]);
-        const float xi = deta[i] + gam * (deta[i] - dprev[i]);
-        dub[e] = v + tau * (G[e] - (gc[jj] * xj - gc[i] * xi) * rde[e]);
+        const float4 f = EF[e];
+        const short2 ij = eij[e];
+        if (e < eown) acc[e] += (double)f.y;
+        EF[e].y = f.y + tau * (f.z - (Y[ij.y] - Y[ij.x]) * f.w);
       }
       __syncthreads();
     }
@@ -212,12 +212,12 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
       float *xe = M.xeta[r & 1];
       float *xu = M.xdub[r & 1];
       for (int c = threadIdx.x; c < nown; c += blockDim.x) xe[cells[c]] = deta[c];
-      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = dub[e];
+      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = EF[e].y;
     }
   }
   __syncthreads();
   for (int e = threadIdx.x; e < eown; e += blockDim.x) {
-    M.dub[edges[e]] = dub[e];
+    M.dub[edges[e]] = EF[e].y;
     M.acc[edges[e]] = acc[e];
   }
 }

@@ -114,6 +114,8 @@ TileSetHost build_tiles(int N, int E, const int32_t *nbr, const int32_t *cellEdg
         const int v = e < 0 ? 0 : le.at(e) + 1;
         t.cedge.push_back((int16_t)(cellSign[(size_t)c * 6 + s] < 0 ? -v : v));
       }
+      t.cedge.push_back(0);                    // two pads: a cell's slots are one 16-byte word
+      t.cedge.push_back(0);
     }
     for (auto &tu : ev) {
       const int e = std::get<2>(tu);

@@ -25,16 +25,17 @@ struct TileSetHost {
   std::vector<int32_t> cells, edges;           // global ids, tile by tile, local order
   std::vector<int32_t> ncnt, ecnt;             // per tile k + 1 prefix counts: cells of ring <= r, edges of ring <= r
   std::vector<int32_t> eown;                   // per tile: owned edges (eI owned), the first of the local edges
-  std::vector<int16_t> cedge;                  // per local cell 6 slots: +-(local edge + 1), sign = cellSign; 0 pads
+  std::vector<int16_t> cedge;                  // per local cell 8 slots: +-(local edge + 1), sign = cellSign; 0 pads
   std::vector<int16_t> eIl, eJl;               // per local edge its local cells (-1 outside the tile)
 };
 
-// Per-tile shared-memory bytes: per cell eta, eta_prev, area, Gc (8 B each) and 6 signed local edge ids (2 B); per
-// edge ubar, G, d_e, l_e H_e (8 B each) and two local cell ids (2 B); per owned edge the sub-step sum acc (8 B).
-inline size_t tile_smem_bytes(size_t nc, size_t ne, size_t nown) { return nc * (4 * 8 + 6 * 2) + ne * (4 * 8 + 2 * 2) + nown * 8 + 64; }
-// The mixed form's tile: per cell deta, its previous value, 1/area, Gc, c0 (4 B each) and the edge ids; per edge dub,
-// G', 1/d_e, l_e H_e (4 B each) and the cell ids; per owned edge acc (8 B).
-inline size_t tile_smem_bytes_mixed(size_t nc, size_t ne, size_t nown) { return nc * (5 * 4 + 6 * 2) + ne * (4 * 4 + 2 * 2) + nown * 8 + 64; }
+// Per-tile shared-memory bytes. FP64 form: per cell eta, Y = Gc (eta + gamma (eta - eta_prev)), area, Gc (8 B each) and
+// its 8 signed local edge ids (16 B); per edge (l_e H_e, ubar) and (G, d_e) (16 B each) and its two local cell ids
+// (4 B); per owned edge the sub-step sum acc (8 B); 64 B of alignment slack.
+inline size_t tile_smem_bytes(size_t nc, size_t ne, size_t nown) { return nc * (4 * 8 + 16) + ne * (2 * 16 + 4) + nown * 8 + 64; }
+// The mixed form's tile: per cell deta, Y, 1/area, Gc, c0 (4 B each) and the edge ids (16 B); per edge (l_e H_e, dub,
+// G', 1/d_e) (16 B) and the cell ids (4 B); per owned edge acc (8 B).
+inline size_t tile_smem_bytes_mixed(size_t nc, size_t ne, size_t nown) { return nc * (5 * 4 + 16) + ne * (16 + 4) + nown * 8 + 64; }
 
 // Compact balanced partition of the N cells into P regions (owner per cell).
 std::vector<int32_t> partition_cells(int N, const int32_t *nbr, int P);
