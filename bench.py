@@ -7,6 +7,8 @@ tracers. dt = 300 s, so a step is 300 s of model time. Synthetic seeded initial 
 spherical-harmonic terrain, 1% perturbations, random tracers); the grid is built on the device (Lloyd to 1e-11 rad).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl isw|reference] [--level 6]
+    python bench.py --workload ensemble    # 64 members (40 at level 5, 16 at 6, 8 at 7), mixed form: member-days/s
+    python bench.py --workload serving     # Poisson request stream with continuous batching: p50/p99, member-days/s
 
 Under torchrun (N > 1) every rank advances its own member (replicas: the members are independent) and rank 0 prints
 one JSON line with the whole job's model days per second (the max step time over ranks). `--impl reference` times
@@ -170,6 +172,114 @@ def run_reference(args, rank):
     print(json.dumps(out), flush=True)
 
 
+def fp64_step_seconds(keys, warmup=3, steps=10):
+    """Seconds per step of ONE member of each (level, layers) key alone on the plain FP64 core (its own batched graph):
+    the sequential baseline of the ensemble and serving workloads."""
+    import torch
+    from isw import gpu
+    from isw.batch import Batch
+    from isw.ensemble import device_grids
+    from isw.workload import Member
+    gpu.set_precision('double')
+    grids = device_grids(sorted({k[0] for k in keys}), 0)
+    out = {}
+    for level, layers in sorted(set(keys)):
+        b = Batch(0)
+        m = Member(grids[level], 0, ntracers=2, perturb=0.005, batch=b, kinds=('air',) if layers == 3 else ('air', 'ocean'),
+                   init_device=torch.device('cuda:0'))
+        for _ in range(warmup):
+            b.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            b.step()
+        e1.record()
+        torch.cuda.synchronize()
+        out[(level, layers)] = e0.elapsed_time(e1) / steps / 1e3
+        del m, b
+    return out
+
+
+def run_ensemble(args):
+    """64 five-layer members (40 at level 5, 16 at level 6, 8 at level 7), seeds base + index, 0.5% perturbations, 2 FCT
+    tracers, mixed precision, in one batch (one CUDA graph per step, tile layout by the autotuner); member-days/s
+    against a sequential loop of the plain FP64 core over the same members."""
+    import torch
+    from isw.ensemble import Ensemble
+    levels = [5] * 40 + [6] * 16 + [7] * 8
+    t = time.time()
+    ens = Ensemble.build(levels, seed=100, perturb=0.005, ntracers=2, precision='mixed', device=0)
+    t_build = time.time() - t
+    best, times = ens.batch.autotune(steps=3)
+    layout = ens.batch.info()
+    for _ in range(args.warmup):
+        ens.step()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            ens.step()
+        e1.record(st)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    finite = all(bool(torch.isfinite(a).all()) for m in ens for a in m.state())
+    value = ens.member_days_per_step() / (ms / 1e3)
+    base = fp64_step_seconds([(n, 5) for n in set(levels)])
+    seq = ens.member_days_per_step() / sum(base[(n, 5)] for n in levels)
+    out = dict(metric='ensemble member-days/s: 64 five-layer members (40 x level 5, 16 x level 6, 8 x level 7), mixed form',
+               value=value, unit='member-days/s', n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
+               higher_is_better=True, scaling='weak', vs_baseline=None,
+               dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
+               impl='isw',
+               config=dict(workload='config-4 ensemble: 64 members, air 3 + ocean 2 layers, 2 tracers, 0.5% perturbations',
+                           members=len(levels), stacks=layout['stacks'], tiles=layout, autotuned=best,
+                           device_bytes=ens.footprint(), l2='state far larger than L2 (no flush needed)'),
+               sequential_fp64=dict(value=seq, unit='member-days/s', ms_per_member_step={f'level{k[0]}': v * 1e3 for k, v in base.items()},
+                                    note='each member stepped alone on the plain FP64 core, one after another'),
+               speedup_vs_sequential_fp64=value / seq, gpu_launches=None, clocks=clk.summary(), finite=finite,
+               build_s=t_build, autotune_ms={str(k): v for k, v in times.items()})
+    print(json.dumps(out), flush=True)
+
+
+def run_serving(args):
+    """Seeded Poisson requests (rate 50 per second of the server's wall clock; level 4..7, horizon 1..30 model days
+    log-uniform, 3 or 5 layers), served with continuous batching in the mixed form under a 150 GB budget; p50/p99
+    time-to-completion and member-days/s, against the plain FP64 core serving the same stream one request at a time."""
+    import torch
+    from isw.serving import Server, poisson_requests, sequential_baseline
+    reqs = poisson_requests(args.requests, 50.0, seed=args.seed, days=(1.0, args.max_days))
+    srv = Server(0, budget_bytes=150e9, precision='mixed', ntracers=2)
+    srv.batch.config(layout='packed')
+    for n in sorted({r.level for r in reqs}):          # grids and the requests' initial states exist before the clock starts
+        srv._grid(n)
+    srv.prepare(reqs)
+    with ClockSampler(0) as clk:
+        results, stats = srv.run(reqs)
+    base = fp64_step_seconds({(r.level, r.layers) for r in reqs})
+    from isw import cases
+    def days_of(r):
+        dt = cases.stack_dt(r.level)
+        n = max(1, int(math.ceil(r.days * SECONDS_PER_DAY / dt - 1e-9)))
+        return n, n * dt / SECONDS_PER_DAY
+    seq = sequential_baseline(reqs, base, days_of)
+    out = dict(metric='serving: p50/p99 time-to-completion (s) and member-days/s, Poisson stream of forecast requests, mixed form',
+               value=stats['member_days_per_s'], unit='member-days/s', p50_s=stats['p50_s'], p99_s=stats['p99_s'],
+               n_gpus=1, steps=stats['batched_steps'], warmup=0, higher_is_better=True, scaling='weak', vs_baseline=None,
+               dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
+               impl='isw',
+               config=dict(workload=f'config-5 serving: {args.requests} requests, Poisson rate 50/s (server wall clock), '
+                                    f'level 4..7, horizon 1..{args.max_days:g} model days log-uniform, 3 or 5 layers, 2 tracers',
+                           budget_bytes=150e9, seed=args.seed),
+               stats=stats,
+               sequential_fp64=dict(seq, note='the same stream served one request at a time (FIFO) on the plain FP64 core, '
+                                              'service times from measured per-step times'),
+               clocks=clk.summary())
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -180,8 +290,15 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
+    ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving'))
+    ap.add_argument('--requests', type=int, default=48, help='serving: requests in the stream')
+    ap.add_argument('--max-days', type=float, default=30.0, help='serving: longest horizon (model days)')
+    ap.add_argument('--seed', type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload != 'member' and args.impl == 'isw':
+        {'ensemble': run_ensemble, 'serving': run_serving}[args.workload](args)
+        return
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

@@ -386,8 +386,9 @@ int kernel_lmax(int L) { return L <= 2 ? 2 : L <= 3 ? 3 : L <= 5 ? 5 : 8; }
 //    cooperative launch per group and stage (large ensembles, serving).
 // Stacks whose tiles would not fit in shared memory at all take the grid-wide sub-step kernels.
 struct Tiling {
-  int k = 0, bps = 2;
+  int k = 0, bps = 2;                          // k: the smallest exchange interval over the stacks (the layout's score)
   std::vector<int> P;                          // tiles per slot (0: untiled)
+  std::vector<int> K;                          // exchange interval per slot
   std::vector<int> group;                      // group per slot
 };
 
@@ -416,6 +417,7 @@ Tiling plan_shared(isw_batch *b, int bps) {
     any = true;
   }
   t.k = any ? kmin : 0;
+  t.K.assign(b->slots.size(), t.k);
   return t;
 }
 
@@ -423,6 +425,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
   Tiling t;
   t.bps = bps;
   t.P.assign(b->slots.size(), 0);
+  t.K.assign(b->slots.size(), 0);
   t.group.assign(b->slots.size(), 0);
   const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
   const int cap = b->sms * bps;
@@ -438,6 +441,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
     const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1);
     if (kf == 0) continue;
     t.P[q] = Pq;
+    t.K[q] = kf;                               // each stack its own interval: a group's rounds follow its slowest
     kmin = std::min(kmin, kf);
     any = true;
   }
@@ -511,13 +515,13 @@ void rebuild(isw_batch *b) {
     d.tiled = 0;
     const size_t q = (size_t)(&sl - &b->slots[0]);
     if (kbest > 0 && best.P[q] > 0) {
-      TileCache *tc = tiles_for(b, sl.layers->grid, best.P[q], kbest);
+      TileCache *tc = tiles_for(b, sl.layers->grid, best.P[q], best.K[q]);
       const int g = best.group[q];
       d.tiled = 1;
       d.tiles = tc->dev;
       gsmem[g] = std::max(gsmem[g], tiles_smem(tc->host, b->mixed == 1));
       for (int p = 0; p < best.P[q]; p++) grefs[g].push_back(TileRef{s, p});
-      for (int st = 0; st < 3; st++) gsub[g][st] = std::max(gsub[g][st], d.n[st]);
+      for (int st = 0; st < 3; st++) gsub[g][st] = std::max(gsub[g][st], (d.n[st] + best.K[q] - 1) / best.K[q]);
     }
     if (!d.tiled) any_untiled = 1;
     auto chunks = [&](std::vector<Chunk> &v, int n) {
@@ -558,7 +562,7 @@ void rebuild(isw_batch *b) {
     fg.begin = (int)refs.size();
     fg.count = (int)grefs[g].size();
     fg.smem = gsmem[g];
-    for (int st = 0; st < 3; st++) fg.rounds[st] = (gsub[g][st] + kbest - 1) / kbest;
+    for (int st = 0; st < 3; st++) fg.rounds[st] = gsub[g][st];
     refs.insert(refs.end(), grefs[g].begin(), grefs[g].end());
     b->groups.push_back(fg);
   }

@@ -111,19 +111,27 @@ def initial_state(g, preset):
 
 # ---- random fields on the sphere ----
 
-def sh_field(g, rng, lmax, spectrum):
+def sh_field(g, rng, lmax, spectrum, device=None):
     """A real random spherical-harmonic field at the cells: sum over l <= lmax, m <= l of 4pi-normalised associated
     Legendre functions times N(0, spectrum(l) / (2l + 1)) coefficients on cos(m lon) and sin(m lon); area-weighted
-    RMS normalised to 1."""
-    x = np.sin(g.lat)
-    c = np.sqrt(np.maximum(0.0, 1 - x * x))
-    lon = g.lon
-    f = np.zeros(g.N)
-    pmm = np.ones(g.N)
+    RMS normalised to 1. device: evaluate the sum with torch on that CUDA device (the same coefficients, drawn in the same
+    order; the sum rounds differently), for the many members of ensembles and serving runs."""
+    if device is not None:
+        import torch
+        xp = torch
+        T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=device)
+        lat, lon = T(g.lat), T(g.lon)
+    else:
+        xp = np
+        lat, lon = g.lat, g.lon
+    x = xp.sin(lat)
+    c = xp.sqrt(xp.clamp(1 - x * x, min=0.0) if xp is not np else np.maximum(0.0, 1 - x * x))
+    f = xp.zeros_like(x)
+    pmm = xp.ones_like(x)
     for m in range(lmax + 1):
         if m > 0:
             pmm = pmm * c * math.sqrt((2 * m + 1) / (2 * m)) * (math.sqrt(2.0) if m == 1 else 1.0)
-        cm, sm = np.cos(m * lon), np.sin(m * lon)
+        cm, sm = xp.cos(m * lon), xp.sin(m * lon)
         p2, p1 = None, pmm
         for l in range(m, lmax + 1):
             if l == m:
@@ -139,21 +147,27 @@ def sh_field(g, rng, lmax, spectrum):
             if l == 0:
                 continue
             s = math.sqrt(spectrum(l) / (2 * l + 1))
-            f += p * (rng.standard_normal() * s * cm + (rng.standard_normal() * s * sm if m > 0 else 0.0))
+            a = rng.standard_normal() * s
+            if m > 0:
+                f += p * (a * cm + (rng.standard_normal() * s) * sm)
+            else:
+                f += p * (a * cm)
+    if device is not None:
+        f = f.cpu().numpy()
     A = g.areaCell / np.sum(g.areaCell)
     f = f - np.sum(A * f)
     return f / math.sqrt(np.sum(A * f * f))
 
 
-def topography(g, seed, lmax=32, rms=2000.0):
+def topography(g, seed, lmax=32, rms=2000.0, device=None):
     """Random spherical-harmonic topography to degree lmax with the given area-weighted RMS (m), flat spectrum."""
-    return rms * sh_field(g, np.random.default_rng(seed), lmax, lambda l: 1.0)
+    return rms * sh_field(g, np.random.default_rng(seed), lmax, lambda l: 1.0, device)
 
 
-def smooth_noise(g, seed, corr=1.0e6, lmax=48):
+def smooth_noise(g, seed, corr=1.0e6, lmax=48, device=None):
     """Unit-RMS smooth random field with a Gaussian correlation of length corr (m)."""
     k = (corr / R_PLANET) ** 2 / 2
-    return sh_field(g, np.random.default_rng(seed), lmax, lambda l: math.exp(-k * l * (l + 1)))
+    return sh_field(g, np.random.default_rng(seed), lmax, lambda l: math.exp(-k * l * (l + 1)), device)
 
 
 # ---- stacked-layer workloads ----
@@ -220,23 +234,24 @@ def compress_peaks(t, knee, cap):
     return np.where(t <= knee, t, knee + w * np.tanh((t - knee) / w))
 
 
-def stack_state(g, kind, seed, perturb=0.01, ntracers=3, topo=None, omega=OMEGA_EARTH):
+def stack_state(g, kind, seed, perturb=0.01, ntracers=3, topo=None, omega=OMEGA_EARTH, device=None):
     """A stacked-layer workload: dict(h (L, N), u (L, E), b (N), gprime, stress, nu4, floor, tracers [T x (L, N)]).
     Topography: random spherical harmonics to degree 32, 2 km RMS (seeded, shared by the stacks of one seed), its peaks
     above 800 m compressed toward 1.5 km, under the air stack; the ocean stack lies on a flat 4 km floor. Each layer's thickness is scaled by
     (1 + perturb r_k), r_k a unit-RMS random field with a 1000 km correlation length. Tracers (per cell and layer,
-    i.i.d.): potential temperature U(250, 310) K, vapour log-normal (median 5e-3, sigma_ln 0.5), a gas U(0, 1)."""
+    i.i.d.): potential temperature U(250, 310) K, vapour log-normal (median 5e-3, sigma_ln 0.5), a gas U(0, 1).
+    device: synthesise the random fields on that CUDA device (faster; equal to the host's to rounding)."""
     c = STACKS[kind]
     L = len(c['H'])
     if c.get('flat'):
         b = np.full(g.N, c['base'])
     else:
-        t = topography(g, seed) if topo is None else topo
+        t = topography(g, seed, device=device) if topo is None else topo
         b = c['base'] + compress_peaks(t, c['knee'], c['cap'])
     ujets = [jet_profile(U) for U in c['U']]
     h, u = balanced_layers(g, c['H'], ujets, c['gprime'], b, c['floor'], omega)
     for k in range(L):
-        h[k] = np.maximum(h[k] * (1 + perturb * smooth_noise(g, seed * 100 + 10 + k)), c['floor'])
+        h[k] = np.maximum(h[k] * (1 + perturb * smooth_noise(g, seed * 100 + 10 + k, device=device)), c['floor'])
     rng = np.random.default_rng(seed * 100 + 50)
     tr = [rng.uniform(250.0, 310.0, (L, g.N)), 5e-3 * np.exp(0.5 * rng.standard_normal((L, g.N))),
           rng.uniform(0.0, 1.0, (L, g.N))][:ntracers]

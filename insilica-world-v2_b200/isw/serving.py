@@ -1,0 +1,192 @@
+"""A forecast server on one GPU with continuous batching: requests (a grid level, a horizon in model days, 3 or 5 layers)
+arrive over time; each is admitted as soon as its device footprint fits the memory budget (and a slot is free), its
+state is created on the device and registered with the server's batch, and from then on every batched step advances it
+together with every other admitted request, each by one of its own steps. A request that reaches its horizon is copied
+back to the host and released at once, and the requests waiting for memory are admitted in arrival order. State stays
+resident on the device from admission to completion; nothing is copied between steps.
+
+A request's result does not depend on what else is in the batch: every stack's arithmetic is its own (the batched
+kernels give each stack the same operations in the same order whatever shares the launch).
+
+The request stream of the benchmark: seeded Poisson arrivals at `rate` requests per second of the server's wall clock,
+the level uniform over 4..7, the horizon log-uniform over 1..30 model days, 3 (air) or 5 (air and ocean) layers, initial
+states as the stacked benchmark member's (seed = request id), carried by the requests (Server.prepare) as a client's
+analysis would be; admission allocates the request's device state and uploads it."""
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import gpu
+from .batch import Batch
+from .ensemble import device_grids
+from .workload import Member, stack_bytes
+
+SECONDS_PER_DAY = 86400.0
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # seconds after the start of the run
+    level: int
+    days: float
+    layers: int             # 3: the air stack; 5: air and ocean
+    seed: int = 0
+    state: list = field(default=None, repr=False)   # the initial stack states (host), as a client sends them
+
+
+@dataclass
+class Result:
+    rid: int
+    level: int
+    layers: int
+    days: float
+    steps: int
+    arrival: float
+    admitted: float
+    done: float
+    state: list = field(default_factory=list, repr=False)   # host copies of h, u (and M, tracers) per stack
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def poisson_requests(n, rate, seed=0, levels=(4, 5, 6, 7), days=(1.0, 30.0), layers=(3, 5)):
+    """n requests: exponential gaps of mean 1/rate seconds, level uniform over `levels`, horizon log-uniform over `days`,
+    layers uniform over `layers` (seeded)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    lv = rng.choice(levels, n)
+    hz = np.exp(rng.uniform(math.log(days[0]), math.log(days[1]), n))
+    ly = rng.choice(layers, n)
+    return [Request(i, float(t[i]), int(lv[i]), float(hz[i]), int(ly[i]), seed=1000 + i) for i in range(n)]
+
+
+def request_bytes(g, layers, ntracers, mixed):
+    kinds = ('air',) if layers == 3 else ('air', 'ocean')
+    return sum(stack_bytes(g, 3 if k == 'air' else 2, ntracers, mixed) for k in kinds)
+
+
+class Server:
+    def __init__(self, device=0, budget_bytes=150e9, precision='mixed', ntracers=2, max_active=256, grids=None,
+                 keep_state=False):
+        self.device = int(device)
+        self.dev = torch.device(f'cuda:{self.device}')
+        self.budget = float(budget_bytes)
+        self.precision = precision
+        self.ntracers = ntracers
+        self.max_active = max_active
+        self.keep_state = keep_state
+        self.grids = grids or {}
+        self.batch = Batch(self.device)
+
+    def _grid(self, level):
+        if level not in self.grids:
+            prev = gpu.PRECISION
+            gpu.set_precision(self.precision)
+            try:
+                self.grids.update(device_grids([level], self.device))
+            finally:
+                gpu.set_precision(prev)
+        return self.grids[level]
+
+    def prepare(self, requests):
+        """Give every request its initial state (the stacked benchmark member's, seeded by the request), synthesised on
+        the device: what a client would send with the request. Done before a timed run."""
+        from . import cases
+        for r in requests:
+            if r.state is None:
+                g = self._grid(r.level).host
+                topo = cases.topography(g, r.seed, device=self.dev)
+                kinds = ('air',) if r.layers == 3 else ('air', 'ocean')
+                r.state = [cases.stack_state(g, k, r.seed, perturb=0.01, ntracers=self.ntracers, topo=topo, device=self.dev)
+                           for k in kinds]
+
+    def footprint(self, req):
+        return request_bytes(self._grid(req.level).host, req.layers, self.ntracers, self.precision == 'mixed')
+
+    def _admit(self, req, now):
+        prev = gpu.PRECISION
+        gpu.set_precision(self.precision)
+        try:
+            if req.state is None:
+                self.prepare([req])
+            m = Member.from_states(self._grid(req.level), req.state, batch=self.batch)
+        finally:
+            gpu.set_precision(prev)
+        steps = max(1, int(math.ceil(req.days * SECONDS_PER_DAY / m.dt - 1e-9)))
+        return dict(req=req, member=m, left=steps, steps=steps, admitted=now, bytes=self.footprint(req))
+
+    def run(self, requests, stream=None, clock=time.perf_counter):
+        """Serve the requests (arrival times relative to the start of the call); returns (results in completion order,
+        stats). A request is done when its final state is on the host."""
+        st = torch.cuda.current_stream(self.dev) if stream is None else stream
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        waiting, active, results = deque(), [], []
+        used = 0.0
+        steps = 0
+        model_days = 0.0
+        t0 = clock()
+        while pending or waiting or active:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            while waiting and len(active) < self.max_active:
+                req = waiting[0]
+                need = self.footprint(req)
+                if used + need > self.budget and active:
+                    break                                   # wait for memory (a lone request is always admitted)
+                waiting.popleft()
+                a = self._admit(req, clock() - t0)
+                used += a['bytes']
+                active.append(a)
+            if not active:
+                if pending:                                 # idle until the next arrival
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
+                continue
+            self.batch.step(st)
+            st.synchronize()
+            steps += 1
+            finished = []
+            for a in active:
+                a['left'] -= 1
+                model_days += a['member'].dt / SECONDS_PER_DAY
+                if a['left'] == 0:
+                    finished.append(a)
+            for a in finished:
+                m, req = a['member'], a['req']
+                m.unregister()
+                state = [x.cpu() for x in m.state()] if self.keep_state else [x.cpu() for x in m.state()[:2]]
+                active.remove(a)
+                used -= a['bytes']
+                results.append(Result(req.rid, req.level, req.layers, req.days, a['steps'], req.arrival, a['admitted'],
+                                      clock() - t0, state if self.keep_state else []))
+                del m, a
+        wall = clock() - t0
+        lat = np.array([r.latency for r in results]) if results else np.zeros(1)
+        stats = dict(requests=len(results), batched_steps=steps, wall_s=wall, model_days=model_days,
+                     member_days_per_s=model_days / wall if wall > 0 else 0.0,
+                     p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)), max_s=float(lat.max()))
+        return results, stats
+
+
+def sequential_baseline(requests, step_seconds, days_of):
+    """The same requests served one at a time in arrival order (FIFO, one server) by a core whose step takes
+    step_seconds[(level, layers)] seconds: completion times by the single-server queue recursion, latencies, and the
+    member-days per second of service time. days_of(req) gives (steps, model days)."""
+    t, lat, busy, days = 0.0, [], 0.0, 0.0
+    for r in sorted(requests, key=lambda r: r.arrival):
+        n, d = days_of(r)
+        service = n * step_seconds[(r.level, r.layers)]
+        t = max(t, r.arrival) + service
+        lat.append(t - r.arrival)
+        busy += service
+        days += d
+    lat = np.array(lat)
+    return dict(p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)), wall_s=t,
+                member_days_per_s=days / busy if busy > 0 else 0.0)

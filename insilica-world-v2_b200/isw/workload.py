@@ -55,20 +55,37 @@ class Stack:
 
 
 class Member:
-    """One benchmark member: the air and ocean stacks of one seed on one grid. batch: an isw.batch.Batch to register the
-    stacks with (they are then advanced by Batch.step, all stacks in one launch); None steps them call by call."""
+    """One benchmark member: the air and ocean stacks of one seed on one grid (kinds=('air',) for the 3-layer form).
+    batch: an isw.batch.Batch to register the stacks with (they are then advanced by Batch.step, all stacks in one
+    launch); None steps them call by call. init_device: synthesise the random initial fields on that CUDA device."""
 
-    def __init__(self, dg, seed, ntracers=3, perturb=0.01, dt=None, nfast=NFAST, batch=None):
+    def __init__(self, dg, seed, ntracers=3, perturb=0.01, dt=None, nfast=NFAST, batch=None, kinds=('air', 'ocean'),
+                 init_device=None):
         g = dg.host
         dt = cases.stack_dt(g.n) if dt is None else dt
-        topo = cases.topography(g, seed)
-        self.stacks = [Stack(dg, cases.stack_state(g, kind, seed, perturb=perturb, ntracers=ntracers, topo=topo), dt, nfast)
-                       for kind in ('air', 'ocean')]
+        topo = cases.topography(g, seed, device=init_device)
+        self.stacks = [Stack(dg, cases.stack_state(g, kind, seed, perturb=perturb, ntracers=ntracers, topo=topo,
+                                                   device=init_device), dt, nfast)
+                       for kind in kinds]
         self.dt = float(dt)
         self.batch, self.slots = batch, []
         if batch is not None:
             for s in self.stacks:
                 self.slots.append(s.register(batch))
+
+    @classmethod
+    def from_states(cls, dg, states, dt=None, nfast=NFAST, batch=None):
+        """A member from prepared stack states (cases.stack_state dicts), e.g. initial conditions that came with a
+        request; nothing is synthesised here."""
+        self = cls.__new__(cls)
+        dt = cases.stack_dt(dg.host.n) if dt is None else dt
+        self.stacks = [Stack(dg, s, dt, nfast) for s in states]
+        self.dt = float(dt)
+        self.batch, self.slots = batch, []
+        if batch is not None:
+            for s in self.stacks:
+                self.slots.append(s.register(batch))
+        return self
 
     def step(self, stream=None):
         if self.batch is not None:
@@ -79,6 +96,16 @@ class Member:
 
     def state(self):
         return [a for s in self.stacks for a in s.state()]
+
+    def unregister(self):
+        if self.batch is not None:
+            for slot in self.slots:
+                self.batch.remove(slot)
+        self.batch, self.slots = None, []
+
+    def footprint(self):
+        """Device bytes this member holds: its state arrays and the scratch of its Layers and Transport objects."""
+        return sum(stack_bytes(s.dg.host, s.L, s.T, s.core.precision == 1) for s in self.stacks)
 
     def launches(self):
         """Kernels one step launches (in the batched case, the step graph's kernels, shared with the batch's other
@@ -95,3 +122,18 @@ def planet_grid(g, omega=cases.OMEGA_EARTH):
     """The grid with the stacked workloads' rotation (fV scaled, as the reference's for_planet does)."""
     from .grid import for_planet
     return for_planet(g, 6.371e6, omega, 9.80616)
+
+
+def stack_bytes(g, L, T, mixed):
+    """Device bytes of one stack on grid g: state (h, u, Fm, M, M1, T tracers), the Layers scratch (csrc/layers.cu
+    layers_create; the mixed form's FP32 scratch too) and the Transport scratch (csrc/transport.cu)."""
+    N, E, NV = g.N, g.E, g.NV
+    R = max(1, T) * L
+    doubles = 3 * L * N + 2 * L * E + T * L * N
+    doubles += 5 * N + NV + 5 * L * N + 2 * L * NV + 10 * L * E + 8 * E
+    doubles += 6 * R * N + R * E
+    floats = 0
+    if mixed:
+        floats += 10 * L * E + L * N + 2 * L * NV + 6 * E + 6 * N
+        floats += 4 * R * N + R * E
+    return 8 * doubles + 4 * floats

@@ -1,0 +1,72 @@
+"""Ensembles and the serving loop in the mixed form: a member of an ensemble of mixed grid levels ends bit for bit where
+it ends alone, and a served request's result is the same whether it was served alone or admitted into a running mix of
+other requests (continuous batching: requests join and leave the batch between steps)."""
+import math
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    return torch.device('cuda:0')
+
+
+@pytest.fixture(scope='module')
+def grids(dev):
+    from isw import gpu
+    from isw.ensemble import device_grids
+    gpu.set_precision('mixed')
+    try:
+        return device_grids([4, 5], 0)
+    finally:
+        gpu.set_precision('double')
+
+
+def test_ensemble_member_equals_alone(dev, grids):
+    from isw.ensemble import Ensemble
+    ens = Ensemble.build([4, 5, 4, 5], seed=40, ntracers=2, precision='mixed', grids=grids)
+    alone = Ensemble.build([5], seed=41, ntracers=2, precision='mixed', grids=grids)
+    assert len(ens) == 4 and ens.member_days_per_step() > 0
+    ens.step(6)
+    alone.step(6)
+    torch.cuda.synchronize()
+    assert ens.batch.status() == 0
+    for x, y in zip(ens.members[1].state(), alone.members[0].state()):
+        assert torch.equal(x, y)
+
+
+def test_served_alone_equals_in_mix(dev, grids):
+    from isw.serving import Request, Server
+    target = Request(0, 0.0, 5, 0.1, 5, seed=77)
+    others = [Request(1, 0.0, 4, 0.3, 3, seed=78), Request(2, 0.0, 5, 0.05, 3, seed=79),
+              Request(3, 0.02, 4, 0.2, 5, seed=80), Request(4, 0.05, 5, 0.15, 3, seed=81)]
+    res = {}
+    for name, reqs in (('alone', [target]), ('mix', [others[0], target] + others[1:])):
+        srv = Server(0, budget_bytes=150e9, precision='mixed', ntracers=2, grids=grids, keep_state=True)
+        srv.batch.config(layout='packed')
+        results, stats = srv.run(reqs)
+        assert stats['requests'] == len(reqs)
+        assert srv.batch.status() == 0
+        for r in results:
+            assert r.done >= r.admitted >= r.arrival >= 0
+            assert r.steps == max(1, math.ceil(r.days * 86400 / (1200.0 * 2.0 ** (4 - r.level)) - 1e-9))
+        res[name] = next(r for r in results if r.rid == 0)
+    assert res['alone'].steps == res['mix'].steps
+    for x, y in zip(res['alone'].state, res['mix'].state):
+        assert torch.equal(x, y)
+
+
+def test_admission_respects_budget(dev, grids):
+    """With a budget that holds one request at a time, requests are served one after another (never two active)."""
+    from isw.serving import Request, Server
+    reqs = [Request(i, 0.0, 4, 0.05, 3, seed=90 + i) for i in range(3)]
+    srv = Server(0, budget_bytes=1.0, precision='mixed', ntracers=2, grids=grids)
+    results, stats = srv.run(reqs)
+    assert [r.rid for r in results] == [0, 1, 2]
+    for a, b in zip(results, results[1:]):
+        assert b.admitted >= a.done - 1e-3
