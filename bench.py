@@ -9,6 +9,7 @@ spherical-harmonic terrain, 1% perturbations, random tracers); the grid is built
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl isw|reference] [--level 6]
     python bench.py --workload ensemble    # 64 members (40 at level 5, 16 at 6, 8 at 7), mixed form: member-days/s
     python bench.py --workload serving     # Poisson request stream with continuous batching: p50/p99, member-days/s
+    python bench.py --workload accuracy    # mixed form against FP64: level-6 member 10 days, level-7 Galewsky 6 days
 
 Under torchrun (N > 1) every rank advances its own member (replicas: the members are independent) and rank 0 prints
 one JSON line with the whole job's model days per second (the max step time over ranks). `--impl reference` times
@@ -280,6 +281,15 @@ def run_serving(args):
     print(json.dumps(out), flush=True)
 
 
+def run_accuracy(args):
+    """The mixed form against the plain FP64 form: the level-6 member over 10 model days and the level-7 Galewsky jet
+    over 6 model days (error norms and mass drifts; no timing)."""
+    from isw import accuracy
+    out = dict(metric='mixed-form accuracy against the FP64 form', impl='isw', data='synthetic',
+               member=accuracy.member(6, args.days_member), galewsky=accuracy.galewsky(7, args.days_galewsky))
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -290,14 +300,16 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
-    ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving'))
+    ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving', 'accuracy'))
+    ap.add_argument('--days-member', type=float, default=10.0, help='accuracy: model days of the level-6 member')
+    ap.add_argument('--days-galewsky', type=float, default=6.0, help='accuracy: model days of the Galewsky jet')
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the stream')
     ap.add_argument('--max-days', type=float, default=30.0, help='serving: longest horizon (model days)')
     ap.add_argument('--seed', type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.workload != 'member' and args.impl == 'isw':
-        {'ensemble': run_ensemble, 'serving': run_serving}[args.workload](args)
+        {'ensemble': run_ensemble, 'serving': run_serving, 'accuracy': run_accuracy}[args.workload](args)
         return
 
     world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -10,7 +10,7 @@
 // alone, whatever else shares the launches.
 //
 // Per step: init (+ first Laplacian pass) | lap e | lap cv | lap e | per stage: A, E, S, fast loop, C, D |
-// vmix + transport P1 (with the receiving masses) | P2 | P3 | P4 (and M <- M1).
+// vmix + FCT stage-1 edge fluxes | P1 (receiving masses, td, p1) | P2E | P2 | P3E | P3 | P4 (and M <- M1).
 //
 // The tile kernel's grid barrier waits with an iteration-bounded, time-bounded spin (globaltimer): if a wait runs out
 // it records ISW_ETIMEOUT in the batch's status word and every block returns; the host reads the status.
@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   if (kind < 0 && Dom<PH>::edge) { if (b < sc.nedge) { kind = 1; ch = sc.edge[b]; } else b -= sc.nedge; }
   if (kind < 0 && Dom<PH>::vert) { if (b < sc.nvert) { kind = 2; ch = sc.vert[b]; } else b -= sc.nvert; }
   if (kind < 0 && Dom<PH>::rows) { if (b < sc.nrows) { kind = 3; ch = sc.rows[b]; } else b -= sc.nrows; }
+  if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
   const int i = ch.begin + (int)threadIdx.x;
@@ -90,16 +91,22 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     if (kind == 1) {
       if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
     } else {
-      ISW_BATCH_L(d.L, LMAXK, fp64::tr_p1<LL>(d.T, d.tr, 3, true, i / M.g.N, i % M.g.N));
+      ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
     }
+  } else if (PH == PH_P1) {
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_c1<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P2E) {
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 2, i / M.g.E, i % M.g.E));
   } else if (PH == PH_P2) {
-    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_c2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P3E) {
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_a_edge<LL>(d.T, d.tr, i / M.g.E, i % M.g.E));
   } else if (PH == PH_P3) {
-    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_c3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
   } else if (PH == PH_P4) {
-    const int j = i / M.g.N, c = i % M.g.N;
-    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p4<LL>(d.T, d.tr, j, c));
-    if (j == 0)
+    const int jj = i / M.g.N, c = i % M.g.N;
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_p4<LL>(d.T, d.tr, jj, c));
+    if (jj == 0)
       for (int l = 0; l < d.L; l++) d.Mm[(size_t)l * M.g.N + c] = d.tr.M1[(size_t)l * M.g.N + c];
   }
 }
@@ -459,7 +466,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
 
 void rebuild(isw_batch *b) {
   std::vector<StackDesc> desc;
-  std::vector<Chunk> cell, edge, vert, rows;
+  std::vector<Chunk> cell, edge, vert, rows, erows;
   int nsub[3] = {0, 0, 0};
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
@@ -531,6 +538,7 @@ void rebuild(isw_batch *b) {
     chunks(edge, d.M.g.E);
     chunks(vert, d.M.g.NV);
     if (d.has_tr) chunks(rows, sl.ntr * d.M.g.N);       // (tracer, cell) pairs
+    if (d.has_tr) chunks(erows, sl.ntr * d.M.g.E);      // (tracer, edge) pairs
     desc.push_back(d);
   }
   b->nstacks = (int)desc.size();
@@ -553,6 +561,7 @@ void rebuild(isw_batch *b) {
   all.insert(all.end(), edge.begin(), edge.end());
   all.insert(all.end(), vert.begin(), vert.end());
   all.insert(all.end(), rows.begin(), rows.end());
+  all.insert(all.end(), erows.begin(), erows.end());
   ISW_CUDA(cudaMalloc(&b->d_desc, sizeof(StackDesc) * desc.size()));
   ISW_CUDA(cudaMalloc(&b->d_chunks, sizeof(Chunk) * all.size()));
   ISW_CUDA(cudaMemcpy(b->d_chunks, all.data(), sizeof(Chunk) * all.size(), cudaMemcpyHostToDevice));
@@ -597,6 +606,8 @@ void rebuild(isw_batch *b) {
   sc.nvert = (int)vert.size();
   sc.rows = sc.vert + sc.nvert;
   sc.nrows = (int)rows.size();
+  sc.erows = sc.rows + sc.nrows;
+  sc.nerows = (int)erows.size();
   b->ntiles = (int)refs.size();
   size_t smax = 0;
   for (auto &fg : b->groups) smax = std::max(smax, fg.smem);
@@ -614,7 +625,7 @@ template <int PH>
 void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j) {
   const Sched &sc = b->sc;
   const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
-                 (Dom<PH>::rows ? sc.nrows : 0);
+                 (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
   if (nb == 0) return;
   if (b->mixed == 1) {
     launch_phase_mixed(PH, b->lmax, nb, st, b->d_desc, sc, stage, j);
@@ -678,7 +689,10 @@ void enqueue(isw_batch *b, cudaStream_t st) {
   }
   if (b->any_vmix || b->any_tr) launch_phase<PH_POST>(b, st, 0, 0);
   if (b->any_tr) {
+    launch_phase<PH_P1>(b, st, 0, 0);
+    launch_phase<PH_P2E>(b, st, 0, 0);
     launch_phase<PH_P2>(b, st, 0, 0);
+    launch_phase<PH_P3E>(b, st, 0, 0);
     launch_phase<PH_P3>(b, st, 0, 0);
     launch_phase<PH_P4>(b, st, 0, 0);
   }

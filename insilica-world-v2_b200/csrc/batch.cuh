@@ -41,8 +41,8 @@ struct TileRef {
 };
 
 struct Sched {
-  const Chunk *cell, *edge, *vert, *rows;
-  int ncell, nedge, nvert, nrows;
+  const Chunk *cell, *edge, *vert, *rows, *erows;   // rows: (tracer, cell) pairs; erows: (tracer, edge) pairs
+  int ncell, nedge, nvert, nrows, nerows;
 };
 
 struct GridBarrier {
@@ -134,7 +134,10 @@ __device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s
   return *reinterpret_cast<const StackDesc *>(buf);
 }
 
-enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4 };
+// The FCT step's passes: POST (edges: interfacial stress; (tracer, edge): stage-1 fluxes), P1 (cells: M1, td, p1),
+// P2E (stage-2 fluxes), P2 (cells: p2), P3E (antidiffusive fluxes), P3 (cells: ratios), P4 (cells: limited update).
+enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4,
+             PH_P1, PH_P2E, PH_P3E };
 
 // Domains of a phase, in block order: which chunk tables its blocks walk.
 template <int PH>
@@ -143,7 +146,8 @@ struct Dom {
   static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
                                PH == PH_D || PH == PH_POST;
   static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
-  static constexpr bool rows = PH == PH_POST || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
+  static constexpr bool rows = PH == PH_P1 || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
+  static constexpr bool erows = PH == PH_POST || PH == PH_P2E || PH == PH_P3E;
 };
 
 

@@ -38,6 +38,7 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
   if (kind < 0 && Dom<PH>::edge) { if (b < sc.nedge) { kind = 1; ch = sc.edge[b]; } else b -= sc.nedge; }
   if (kind < 0 && Dom<PH>::vert) { if (b < sc.nvert) { kind = 2; ch = sc.vert[b]; } else b -= sc.nvert; }
   if (kind < 0 && Dom<PH>::rows) { if (b < sc.nrows) { kind = 3; ch = sc.rows[b]; } else b -= sc.nrows; }
+  if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
   const int i = ch.begin + (int)threadIdx.x;
@@ -84,12 +85,18 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
     if (kind == 1) {
       if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
     } else {
-      ISW_BATCH_L(d.L, LMAXK, mixed::tr_p1<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+      ISW_BATCH_L(d.L, LMAXK, mixed::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
     }
+  } else if (PH == PH_P1) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_c1<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P2E) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_hf_edge<LL>(d.T, d.tr, 2, i / M.g.E, i % M.g.E));
   } else if (PH == PH_P2) {
-    ISW_BATCH_L(d.L, LMAXK, mixed::tr_p2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_c2<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+  } else if (PH == PH_P3E) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_a_edge<LL>(d.T, d.tr, i / M.g.E, i % M.g.E));
   } else if (PH == PH_P3) {
-    ISW_BATCH_L(d.L, LMAXK, mixed::tr_p3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_c3<LL>(d.T, d.tr, i / M.g.N, i % M.g.N));
   } else if (PH == PH_P4) {
     const int jj = i / M.g.N, c = i % M.g.N;
     ISW_BATCH_L(d.L, LMAXK, mixed::tr_p4<LL>(d.T, d.tr, jj, c));
@@ -251,6 +258,9 @@ void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, const StackDe
     case PH_P2: launch_m<PH_P2>(lmax, nb, st, desc, sc, stage, j); break;
     case PH_P3: launch_m<PH_P3>(lmax, nb, st, desc, sc, stage, j); break;
     case PH_P4: launch_m<PH_P4>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P1: launch_m<PH_P1>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, desc, sc, stage, j); break;
     default: break;
   }
 }

@@ -13,6 +13,7 @@ namespace isw {
 constexpr int LMAX = 8;          // layers per column (reference layers.py:30)
 constexpr int TRMAX = 16;        // tracers moved in one transport call
 constexpr int THREADS = 256;     // threads per block of the phase kernels
+constexpr int EOE_MAX = 10;      // TRiSK row length: the other edges of an edge's two cells (5 + 5 on hexagons)
 
 // Thrown inside the library, turned into a status at the C ABI.
 struct Error {

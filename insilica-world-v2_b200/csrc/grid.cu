@@ -134,6 +134,8 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
   if (h->eoeStart[0] != 0) fail(ISW_EINVAL, "grid: eoeStart[0] != 0");
   for (int e = 0; e < E; e++)
     if (h->eoeStart[e + 1] < h->eoeStart[e]) fail(ISW_EINVAL, "grid: eoeStart not ascending");
+  for (int e = 0; e < E; e++)
+    if (h->eoeStart[e + 1] - h->eoeStart[e] > EOE_MAX) fail(ISW_EINVAL, "grid: a TRiSK row (eoe) longer than 10 edges");
   const int nE2 = h->eoeStart[E];
   check_range(h->eoe, nE2, 0, E, false, "eoe");
   for (int i = 0; i < N; i++)

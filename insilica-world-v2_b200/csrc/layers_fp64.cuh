@@ -206,16 +206,24 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
     qf[k] = pe[k * 3 + 2];
     Q[k] = 0;
   }
-  const int m0 = g.eoeStart[e], m1 = g.eoeStart[e + 1];
-  for (int m = m0; m < m1; m++) {
-    const double wm = g.w[m];
-    const double *pp = M.pk + (size_t)g.eoe[m] * L * 3;
+  // the row's neighbour ids and weights first (at most EOE_MAX, validated with the grid), then the gathers, all in
+  // flight together; the sum runs in row order as the reference's loop does
+  const int m0 = g.eoeStart[e], cnt = g.eoeStart[e + 1] - m0;
+  int ix[EOE_MAX];
 #pragma unroll
-    for (int k = 0; k < L; k++) {
-      double h2 = pp[k * 3 + 0];
-      if (h2 > cap[k]) h2 = cap[k];
-      const double F2 = h2 * pp[k * 3 + 1];
-      Q[k] += wm * F2 * 0.5 * (qf[k] + pp[k * 3 + 2]);
+  for (int t = 0; t < EOE_MAX; t++) ix[t] = t < cnt ? g.eoe[m0 + t] : 0;
+#pragma unroll
+  for (int t = 0; t < EOE_MAX; t++) {
+    if (t < cnt) {
+      const double wm = g.w[m0 + t];
+      const double *pp = M.pk + (size_t)ix[t] * L * 3;
+#pragma unroll
+      for (int k = 0; k < L; k++) {
+        double h2 = pp[k * 3 + 0];
+        if (h2 > cap[k]) h2 = cap[k];
+        const double F2 = h2 * pp[k * 3 + 1];
+        Q[k] += wm * F2 * 0.5 * (qf[k] + pp[k * 3 + 2]);
+      }
     }
   }
   const int a = g.eI[e], b = g.eJ[e];

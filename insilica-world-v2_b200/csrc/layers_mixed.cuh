@@ -201,14 +201,20 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
     qf[k] = p.z;
     Q[k] = 0.f;
   }
-  const int m0 = g.eoeStart[e], m1 = g.eoeStart[e + 1];
-  for (int m = m0; m < m1; m++) {
-    const float wm = g.w32[m];
-    const float4 *pp = M.pk4 + (size_t)g.eoe[m] * L;
+  const int m0 = g.eoeStart[e], cnt = g.eoeStart[e + 1] - m0;
+  int ix[EOE_MAX];
 #pragma unroll
-    for (int k = 0; k < L; k++) {
-      const float4 p = pp[k];
-      Q[k] += wm * (fminf(p.x, cap[k]) * p.y) * 0.5f * (qf[k] + p.z);
+  for (int t = 0; t < EOE_MAX; t++) ix[t] = t < cnt ? g.eoe[m0 + t] : 0;
+#pragma unroll
+  for (int t = 0; t < EOE_MAX; t++) {
+    if (t < cnt) {
+      const float wm = g.w32[m0 + t];
+      const float4 *pp = M.pk4 + (size_t)ix[t] * L;
+#pragma unroll
+      for (int k = 0; k < L; k++) {
+        const float4 p = pp[k];
+        Q[k] += wm * (fminf(p.x, cap[k]) * p.y) * 0.5f * (qf[k] + p.z);
+      }
     }
   }
   const int a = g.eI[e], b = g.eJ[e];

@@ -216,5 +216,169 @@ __device__ __forceinline__ void tr_p4(const TransportDev &T, const TrArgs &a, in
   }
 }
 
+
+// ---- The batched step's FCT in the mixed form, as edge passes and cell passes (see transport_fp64.cuh): the stage
+// fluxes of the edge passes are stored in FP64 (T.A), the antidiffusive fluxes rounded to FP32 once (T.Af). ----
+
+template <int L>
+__device__ __forceinline__ void tr_hf_edge(const TransportDev &T, const TrArgs &a, int stage, int j, int e) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  const int ea = g.eI[e], eb = g.eJ[e];
+  const float beta = (float)a.beta;
+  Stencil32 stn;
+  load_stencil(g, e, stn);
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t row = (size_t)(j * L + l);
+    const double f = a.Fm[(size_t)l * E + e];
+    if (stage == 1) {
+      const double *p = a.tr[j] + (size_t)l * N;
+      T.A[row * E + e] = hoflux(f, p, stn, p[ea], p[eb], beta);
+    } else {
+      const float *p = T.p1f + row * N;
+      T.A[row * E + e] = hoflux(f, p, stn, p[ea], p[eb], beta);
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void tr_a_edge(const TransportDev &T, const TrArgs &a, int j, int e) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  const int ea = g.eI[e], eb = g.eJ[e];
+  const float beta = (float)a.beta;
+  Stencil32 stn;
+  load_stencil(g, e, stn);
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t row = (size_t)(j * L + l);
+    const double *p = a.tr[j] + (size_t)l * N;
+    const float *p2 = T.p2f + row * N;
+    const double f = a.Fm[(size_t)l * E + e];
+    T.Af[row * E + e] = (float)(hoflux(f, p2, stn, p2[ea], p2[eb], beta) - fp64::upwind_v(f, p[ea], p[eb]));
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void tr_c1(const TransportDev &T, const TrArgs &a, int j, int i) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  fp64::CellEdges c;
+  fp64::load_edges(g, i, c);
+  double m1[L], td[L], s[L], mx[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i;
+    const double m0 = a.M0[om], pi = a.tr[j][om];
+    m1[l] = m0;
+    td[l] = m0 * pi;
+    s[l] = m0 * pi;
+    mx[l] = m0;
+  }
+  const double frac = 1.0 / 3.0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int e = c.e[q];
+    if (e >= 0) {
+      const bool out = c.a[q] == i;
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const double *p = a.tr[j] + (size_t)l * N;
+        const double f = a.Fm[(size_t)l * E + e];
+        const double fu = fp64::upwind_v(f, p[c.a[q]], p[c.b[q]]);
+        const double hf = frac * T.A[(size_t)(j * L + l) * E + e];
+        const double m = frac * f;
+        if (out) { m1[l] -= f; td[l] -= fu; s[l] -= hf; mx[l] -= m; }
+        else { m1[l] += f; td[l] += fu; s[l] += hf; mx[l] += m; }
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
+    if (j == 0) a.M1[om] = m1[l];
+    T.td[o] = td[l] / m1[l];
+    T.p1f[o] = (float)(s[l] / mx[l]);
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void tr_c2(const TransportDev &T, const TrArgs &a, int j, int i) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  fp64::CellEdges c;
+  fp64::load_edges(g, i, c);
+  double s[L], mx[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t om = (size_t)l * N + i;
+    s[l] = a.M0[om] * a.tr[j][om];
+    mx[l] = a.M0[om];
+  }
+  const double frac = 1.0 / 2.0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const int e = c.e[q];
+    if (e >= 0) {
+      const bool out = c.a[q] == i;
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const double f = a.Fm[(size_t)l * E + e];
+        const double hf = frac * T.A[(size_t)(j * L + l) * E + e];
+        const double m = frac * f;
+        if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < L; l++) T.p2f[(size_t)(j * L + l) * N + i] = (float)(s[l] / mx[l]);
+}
+
+template <int L>
+__device__ __forceinline__ void tr_c3(const TransportDev &T, const TrArgs &a, int j, int i) {
+  const GridDev &g = T.g;
+  const int N = g.N, E = g.E;
+  int es[6], nb[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    es[q] = g.cellEdgeAsc[i * 6 + q];
+    nb[q] = g.nbr[i * 6 + q];
+  }
+  bool out[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) out[q] = es[q] >= 0 && g.eI[es[q]] == i;
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const size_t row = (size_t)(j * L + l);
+    double Pp = 0, Pm = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int e = es[q];
+      if (e >= 0) {
+        const double A = (double)T.Af[row * E + e];
+        if (out[q]) { if (A > 0) Pm += A; else Pp -= A; }
+        else { if (A > 0) Pp += A; else Pm -= A; }
+      }
+    }
+    const double *p = a.tr[j] + (size_t)l * N;
+    const double *tt = T.td + row * N;
+    const double ti = tt[i];
+    double hi = fmax(p[i], ti), lo = fmin(p[i], ti);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int jn = nb[q];
+      if (jn >= 0) {
+        hi = fmax(hi, fmax(p[jn], tt[jn]));
+        lo = fmin(lo, fmin(p[jn], tt[jn]));
+      }
+    }
+    const double m1 = a.M1[(size_t)l * N + i];
+    const double qmax = (hi - ti) * m1, qmin = (ti - lo) * m1;
+    T.Rpf[row * N + i] = Pp > 0 ? (float)fmin(1.0, qmax / Pp) : 0.f;
+    T.Rmf[row * N + i] = Pm > 0 ? (float)fmin(1.0, qmin / Pm) : 0.f;
+  }
+}
+
 }  // namespace mixed
 }  // namespace isw

@@ -115,7 +115,8 @@ class Member:
         info = self.batch.info()
         n = sum(max(1, int(np.ceil(c * self.stacks[0].nfast))) for c in (1 / 3, 1 / 2, 1.0))
         nu4 = any(s.core.nu4 for s in self.stacks)
-        return 1 + (3 if nu4 else 0) + 3 * 5 + (3 if info['tiles'] else 2 * n) + 4
+        tr = any(s.T for s in self.stacks)
+        return 1 + (3 if nu4 else 0) + 3 * 5 + (3 * info['groups'] if info['tiles'] else 2 * n) + 1 + (6 if tr else 0)
 
 
 def planet_grid(g, omega=cases.OMEGA_EARTH):
