@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -47,6 +48,8 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
+  pdl_wait();
+  pdl_trigger();
   const int i = ch.begin + (int)threadIdx.x;
   if (i >= ch.end) return;
   const LayersDev &M = d.M;
@@ -274,6 +277,7 @@ struct isw_batch {
   int tile_cells = 0;                         // packed layout's owned cells per tile (0: by blocks per SM)
   int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
   int layout = 0;                             // 0: choose; 1 shared; 2 packed
+  bool pdl = true;                            // programmatic dependent launch between phase kernels
   std::map<std::tuple<const isw_grid *, int, int>, std::unique_ptr<TileCache>> tiles;
   std::map<std::pair<const isw_grid *, int>, std::vector<int32_t>> parts;
   cudaStream_t cap = nullptr;
@@ -621,21 +625,24 @@ void rebuild(isw_batch *b) {
   b->lmax = kernel_lmax(lmax);
 }
 
+// A phase kernel over every stack. pdl: launched as a programmatic dependent of the kernel before it in the stream
+// (never directly after a cooperative tile launch, which keeps plain stream order).
 template <int PH>
-void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j) {
+void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = true) {
   const Sched &sc = b->sc;
   const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
                  (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
   if (nb == 0) return;
+  pdl = pdl && b->pdl;
   if (b->mixed == 1) {
-    launch_phase_mixed(PH, b->lmax, nb, st, b->d_desc, sc, stage, j);
+    launch_phase_mixed(PH, b->lmax, nb, st, pdl, b->d_desc, sc, stage, j);
     return;
   }
   switch (b->lmax) {
-    case 2: k_phase<PH, 2><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
-    case 3: k_phase<PH, 3><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
-    case 5: k_phase<PH, 5><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
-    default: k_phase<PH, 8><<<nb, THREADS, 0, st>>>(b->d_desc, sc, stage, j); break;
+    case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
+    case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
+    case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
+    default: launch_phase_kernel(k_phase<PH, 8>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
   }
 }
 
@@ -666,9 +673,10 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
   }
 }
 
-// The launches of one step, in order.
+// The launches of one step, in order. The first kernel of the step and the first after a tile launch (or a memset)
+// take plain stream order; the others are programmatic dependents of the kernel before them.
 void enqueue(isw_batch *b, cudaStream_t st) {
-  launch_phase<PH_INIT>(b, st, 0, 0);
+  launch_phase<PH_INIT>(b, st, 0, 0, false);
   if (b->any_nu4) {
     launch_phase<PH_LAPE1>(b, st, 0, 0);
     launch_phase<PH_LAPCV>(b, st, 0, 0);
@@ -678,13 +686,14 @@ void enqueue(isw_batch *b, cudaStream_t st) {
     launch_phase<PH_A>(b, st, s, 0);
     launch_phase<PH_E>(b, st, s, 0);
     launch_phase<PH_S>(b, st, s, 0);
+    const bool tiled = !b->groups.empty();
     launch_fast(b, st, s, DEFAULT_TIMEOUT_NS, -1);
     if (b->any_untiled)
       for (int j = 0; j < b->nsub[s]; j++) {
-        launch_phase<PH_ETA>(b, st, s, j);
+        launch_phase<PH_ETA>(b, st, s, j, !(tiled && j == 0));
         launch_phase<PH_U>(b, st, s, j);
       }
-    launch_phase<PH_C>(b, st, s, 0);
+    launch_phase<PH_C>(b, st, s, 0, !tiled || b->any_untiled);
     launch_phase<PH_D>(b, st, s, 0);
   }
   if (b->any_vmix || b->any_tr) launch_phase<PH_POST>(b, st, 0, 0);
@@ -740,6 +749,7 @@ int isw_batch_create(int device, isw_batch **out) {
     ISW_CUDA(cudaSetDevice(device));
     isw_batch *b = new isw_batch();
     b->device = device;
+    if (const char *e = std::getenv("ISW_NO_PDL")) b->pdl = e[0] != '1';   // diagnostics: plain stream order
     try {
       ISW_CUDA(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device));
       ISW_CUDA(cudaMalloc(&b->bar, sizeof(GridBarrier)));

@@ -139,6 +139,26 @@ __device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s
 enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4,
              PH_P1, PH_P2E, PH_P3E };
 
+// Programmatic dependent launch between phase kernels: a phase kernel is launched while the previous one drains; it
+// stages only constant data (its stack descriptor) before waiting for the previous grid's completion and memory
+// (griddepcontrol.wait), and lets its own dependent launch at once (griddepcontrol.launch_dependents).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KA, class... A>
+void launch_phase_kernel(void (*kern)(KA...), int nb, cudaStream_t st, bool pdl, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)nb);
+  cfg.blockDim = dim3(THREADS);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  ISW_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
 // Domains of a phase, in block order: which chunk tables its blocks walk.
 template <int PH>
 struct Dom {
@@ -151,7 +171,8 @@ struct Dom {
 };
 
 
-void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j);
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage,
+                        int j);
 const void *fast_kernel_mixed(int bps);
 void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
                        GridBarrier *bar, int *status, long long timeout_ns, int fault_block);

@@ -41,6 +41,8 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
   if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
+  pdl_wait();
+  pdl_trigger();
   const int i = ch.begin + (int)threadIdx.x;
   if (i >= ch.end) return;
   const LayersDev &M = d.M;
@@ -230,37 +232,38 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
 }
 
 template <int PH>
-void launch_m(int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j) {
+void launch_m(int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage, int j) {
   switch (lmax) {
-    case 2: k_phase_m<PH, 2><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
-    case 3: k_phase_m<PH, 3><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
-    case 5: k_phase_m<PH, 5><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
-    default: k_phase_m<PH, 8><<<nb, THREADS, 0, st>>>(desc, sc, stage, j); break;
+    case 2: launch_phase_kernel(k_phase_m<PH, 2>, nb, st, pdl, desc, sc, stage, j); break;
+    case 3: launch_phase_kernel(k_phase_m<PH, 3>, nb, st, pdl, desc, sc, stage, j); break;
+    case 5: launch_phase_kernel(k_phase_m<PH, 5>, nb, st, pdl, desc, sc, stage, j); break;
+    default: launch_phase_kernel(k_phase_m<PH, 8>, nb, st, pdl, desc, sc, stage, j); break;
   }
 }
 
 }  // namespace
 
-void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, const StackDesc *desc, const Sched &sc, int stage, int j) {
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage,
+                        int j) {
   switch (ph) {
-    case PH_INIT: launch_m<PH_INIT>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_LAPE1: launch_m<PH_LAPE1>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_LAPCV: launch_m<PH_LAPCV>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_LAPE2: launch_m<PH_LAPE2>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_A: launch_m<PH_A>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_E: launch_m<PH_E>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_S: launch_m<PH_S>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_U: launch_m<PH_U>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_C: launch_m<PH_C>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_D: launch_m<PH_D>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_POST: launch_m<PH_POST>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P2: launch_m<PH_P2>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P3: launch_m<PH_P3>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P4: launch_m<PH_P4>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P1: launch_m<PH_P1>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, desc, sc, stage, j); break;
-    case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, desc, sc, stage, j); break;
+    case PH_INIT: launch_m<PH_INIT>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_LAPE1: launch_m<PH_LAPE1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_LAPCV: launch_m<PH_LAPCV>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_LAPE2: launch_m<PH_LAPE2>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_A: launch_m<PH_A>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_E: launch_m<PH_E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_S: launch_m<PH_S>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_U: launch_m<PH_U>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_C: launch_m<PH_C>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_D: launch_m<PH_D>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_POST: launch_m<PH_POST>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P2: launch_m<PH_P2>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P3: launch_m<PH_P3>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P4: launch_m<PH_P4>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P1: launch_m<PH_P1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     default: break;
   }
 }
