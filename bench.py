@@ -10,6 +10,7 @@ spherical-harmonic terrain, 1% perturbations, random tracers); the grid is built
     python bench.py --workload ensemble    # 64 members (40 at level 5, 16 at 6, 8 at 7), mixed form: member-days/s
     python bench.py --workload serving     # Poisson request stream with continuous batching: p50/p99, member-days/s
     python bench.py --workload accuracy    # mixed form against FP64: level-6 member 10 days, level-7 Galewsky 6 days
+    python bench.py --workload profile --form double|mixed --steps 5   # untimed steps, for ncu launch lists
 
 Under torchrun (N > 1) every rank advances its own member (replicas: the members are independent) and rank 0 prints
 one JSON line with the whole job's model days per second (the max step time over ranks). `--impl reference` times
@@ -281,6 +282,28 @@ def run_serving(args):
     print(json.dumps(out), flush=True)
 
 
+def run_profile(args):
+    """The workload without timing, for a profiler's launch list: the level-N member in one form (--form), stepped
+    --steps times through the batched graph."""
+    import torch
+    from isw import gpu
+    from isw.batch import Batch
+    from isw.workload import Member
+    g, _ = build_grid(args.level, 0)
+    gpu.set_precision(args.form)
+    try:
+        dg = gpu.DeviceGrid(g)
+    finally:
+        gpu.set_precision('double')
+    b = Batch(0)
+    m = Member(dg, seed=0, batch=b)
+    for _ in range(args.steps):
+        m.step()
+    torch.cuda.synchronize()
+    print(json.dumps(dict(workload='profile', form=args.form, level=args.level, steps=args.steps, layout=b.info(),
+                          launches_per_step=m.launches(), status=b.status())), flush=True)
+
+
 def run_accuracy(args):
     """The mixed form against the plain FP64 form: the level-6 member over 10 model days and the level-7 Galewsky jet
     over 6 model days (error norms and mass drifts; no timing)."""
@@ -300,7 +323,8 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
-    ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving', 'accuracy'))
+    ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving', 'accuracy', 'profile'))
+    ap.add_argument('--form', default='double', choices=('double', 'mixed'), help='profile: the precision form')
     ap.add_argument('--days-member', type=float, default=10.0, help='accuracy: model days of the level-6 member')
     ap.add_argument('--days-galewsky', type=float, default=6.0, help='accuracy: model days of the Galewsky jet')
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the stream')
@@ -309,7 +333,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.workload != 'member' and args.impl == 'isw':
-        {'ensemble': run_ensemble, 'serving': run_serving, 'accuracy': run_accuracy}[args.workload](args)
+        {'ensemble': run_ensemble, 'serving': run_serving, 'accuracy': run_accuracy, 'profile': run_profile}[args.workload](args)
         return
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
