@@ -283,25 +283,28 @@ def run_serving(args):
 
 
 def run_profile(args):
-    """The workload without timing, for a profiler's launch list: the level-N member in one form (--form), stepped
-    --steps times through the batched graph."""
+    """The workload without timing, for a profiler's launch list: --members members of the level-N workload in one form
+    (--form) in one batch, the fast loop as --tiles says (auto, off, shared or packed), stepped --steps times."""
     import torch
     from isw import gpu
-    from isw.batch import Batch
-    from isw.workload import Member
+    from isw.ensemble import Ensemble
     g, _ = build_grid(args.level, 0)
     gpu.set_precision(args.form)
     try:
-        dg = gpu.DeviceGrid(g)
+        grids = {args.level: gpu.DeviceGrid(g)}
     finally:
         gpu.set_precision('double')
-    b = Batch(0)
-    m = Member(dg, seed=0, batch=b)
+    ens = Ensemble.build([args.level] * args.members, seed=0, perturb=0.01, ntracers=3, precision=args.form, grids=grids)
+    if args.tiles == 'off':
+        ens.batch.config(tiles=False)
+    elif args.tiles != 'auto':
+        ens.batch.config(tiles=True, layout=args.tiles)
     for _ in range(args.steps):
-        m.step()
+        ens.step()
     torch.cuda.synchronize()
-    print(json.dumps(dict(workload='profile', form=args.form, level=args.level, steps=args.steps, layout=b.info(),
-                          launches_per_step=m.launches(), status=b.status())), flush=True)
+    print(json.dumps(dict(workload='profile', form=args.form, level=args.level, members=args.members, steps=args.steps,
+                          layout=ens.batch.info(), launches_per_step=ens.members[0].launches(), status=ens.batch.status())),
+          flush=True)
 
 
 def run_accuracy(args):
@@ -323,8 +326,11 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
+    ap.add_argument('--batched', type=int, default=8, help='members of the batched-core measurement (0: skip)')
     ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving', 'accuracy', 'profile'))
     ap.add_argument('--form', default='double', choices=('double', 'mixed'), help='profile: the precision form')
+    ap.add_argument('--members', type=int, default=1, help='profile: members in the batch')
+    ap.add_argument('--tiles', default='auto', choices=('auto', 'off', 'shared', 'packed'), help='profile: fast-loop layout')
     ap.add_argument('--days-member', type=float, default=10.0, help='accuracy: model days of the level-6 member')
     ap.add_argument('--days-galewsky', type=float, default=6.0, help='accuracy: model days of the Galewsky jet')
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the stream')
@@ -408,9 +414,32 @@ def main():
     with ClockSampler(local) as clk:
         ms = timed(member)
         ms_m = timed(mixed) if mixed is not None else None
+    batched = None
+    if mixed is not None and args.batched > 0 and not args.percall:
+        # the batched core: args.batched members of the same workload (seeds rank * 1000 + i) in one batch, per form
+        from isw.ensemble import Ensemble
+        batched = dict(members=args.batched, level=args.level)
+        for form in ('mixed', 'double'):
+            set_precision(form)
+            try:
+                grids = {args.level: DeviceGrid(g, device=local)}
+            finally:
+                set_precision('double')
+            ens = Ensemble.build([args.level] * args.batched, seed=rank * 1000, perturb=0.01, ntracers=3, precision=form,
+                                 device=local, grids=grids)
+            tuned, _ = ens.batch.autotune(steps=2)
+            t_b = timed(ens)
+            batched[form] = dict(value=world * ens.member_days_per_step() / (t_b / 1e3), unit='member-days/s',
+                                 ms_per_step=t_b, layout=ens.batch.info(), autotuned=tuned,
+                                 finite=all(bool(torch.isfinite(a).all()) for m_ in ens for a in m_.state()))
+            del ens
+
     finite = all(bool(torch.isfinite(a).all()) for a in member.state())
     dt = member.dt
     value = world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
+    if batched is not None:
+        batched['mixed_vs_fp64_member'] = batched['mixed']['value'] / value
+        batched['mixed_vs_fp64_batched'] = batched['mixed']['value'] / batched['double']['value']
 
     # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state, every step
     host = [torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for a in member.state()]
@@ -466,6 +495,8 @@ def main():
                             dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets',
                             tiles=layout_m, finite=all(bool(torch.isfinite(a).all()) for a in mixed.state()),
                             gpu_launches=mixed.launches() * args.steps)
+    if batched is not None:
+        out['batched'] = batched
 
     if rank == 0 and world == 1 and not args.no_cpu:
         ensure_oracle()

@@ -367,14 +367,19 @@ size_t smem_of(size_t nc, size_t ne, size_t nown, bool mixed) {
 }
 
 // The largest k' <= the probe's k whose largest tile fits `budget` bytes of shared memory (0 if none).
-int fitting_k(const TileSetHost &h, size_t budget, bool mixed) {
+// (mixed tiles also keep each thread's cells, edges and owned edges within the kernel's unrolled bounds)
+int fitting_k(const TileSetHost &h, size_t budget, bool mixed, int threads) {
   for (int kk = h.k; kk >= 1; kk--) {
     size_t worst = 0;
+    bool ok = true;
     for (int p = 0; p < h.P; p++) {
       const size_t nc = h.ncnt[(size_t)p * (h.k + 1) + kk], ne = h.ecnt[(size_t)p * (h.k + 1) + kk];
       worst = std::max(worst, smem_of(nc, ne, h.eown[p], mixed));
+      if (mixed && (nc > (size_t)FAST_CMAX * threads || ne > (size_t)FAST_EMAX * threads ||
+                    (size_t)h.eown[p] > (size_t)FAST_AMAX * threads))
+        ok = false;
     }
-    if (worst <= budget) return kk;
+    if (ok && worst <= budget) return kk;
   }
   return 0;
 }
@@ -421,7 +426,8 @@ Tiling plan_shared(isw_batch *b, int bps) {
     const int N = sl.layers->grid->d.N;
     const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
     if (Pq * 16 > N) return Tiling{};          // tiles of at least 16 owned cells, for every stack
-    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1);
+    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1,
+                             bps == 2 ? 512 : 1024);
     if (kf == 0) return Tiling{};
     t.P[q] = Pq;
     kmin = std::min(kmin, kf);
@@ -449,7 +455,8 @@ Tiling plan_packed(isw_batch *b, int bps) {
     const int N = sl.layers->grid->d.N;
     const int Pq = std::min(cap, std::max(1, (N + cells - 1) / cells));
     if (Pq * 16 > N) continue;
-    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1);
+    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1,
+                             bps == 2 ? 512 : 1024);
     if (kf == 0) continue;
     t.P[q] = Pq;
     t.K[q] = kf;                               // each stack its own interval: a group's rounds follow its slowest

@@ -11,6 +11,9 @@ namespace isw {
 namespace bt {
 
 constexpr int FAST_KMAX = 8;                  // the largest exchange interval of the tiled fast loop
+constexpr int FAST_CMAX = 4;                  // mixed tiles: cells per thread at most (nc <= FAST_CMAX x threads)
+constexpr int FAST_EMAX = 8;                  // mixed tiles: edges per thread at most
+constexpr int FAST_AMAX = 4;                  // mixed tiles: owned edges per thread at most (their sums in registers)
 
 struct TileSetDev {
   int P, k;

@@ -107,10 +107,13 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
   }
 }
 
-// The fast loop of stage `st` over every tiled stack in the mixed form (the tile scheme of batch.cu's k_fast): per cell
-// deta, Y = Gc (deta + gamma (deta - deta_prev)), 1/area, Gc and c0 = sum sign l_e H_e ubar0 (FP32) and its 8 edge slots
-// (16 bytes); per edge (l_e H_e, dub, G', 1/d_e) as one 16-byte record; per owned edge acc (FP64). Exchange buffers
-// xeta[r & 1] and xdub[r & 1]; the final dub and acc go to dub and acc, which no round reads.
+// The fast loop of stage `st` over every tiled stack in the mixed form (the tile scheme of batch.cu's k_fast). Shared
+// memory, FP32 arrays: per cell deta, Y = Gc (deta + gamma (deta - deta_prev)), 1/area, Gc, c0 = sum sign l_e H_e ubar0
+// and its 8 edge slots (16 bytes); per edge dub, fl = l_e H_e dub (what the cell pass sums: one float per gathered
+// edge), l_e H_e, G', 1/d_e and its two local cells. A thread's edges are always e = tid + j NT, so the FP64 sub-step
+// sum acc of its owned edges (j < FAST_AMAX) stays in registers. Exchange buffers xeta[r & 1] and xdub[r & 1]; the
+// final dub and acc go to dub and acc, which no round reads. The host keeps nc <= FAST_CMAX NT, ne <= FAST_EMAX NT and
+// eown <= FAST_AMAX NT.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
                                                       int rounds, GridBarrier *bar, int *status, long long timeout_ns,
@@ -127,39 +130,47 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
   const int eown = T.eown[p];
   const int *cells = T.cells + c0i;
   const int *edges = T.edges + e0;
-  float4 *EF = reinterpret_cast<float4 *>(smem);           // (l_e H_e, dub, G', 1/d_e)
-  const float2 *EF2 = reinterpret_cast<const float2 *>(EF);
-  uint4 *cedge = reinterpret_cast<uint4 *>(EF + ne);
-  double *acc = reinterpret_cast<double *>(cedge + nc);    // owned edges only
-  float *deta = reinterpret_cast<float *>(acc + eown);
+  uint4 *cedge = reinterpret_cast<uint4 *>(smem);
+  float *deta = reinterpret_cast<float *>(cedge + nc);
   float *Y = deta + nc;
   float *rA = Y + nc;
   float *gc = rA + nc;
   float *cz = gc + nc;
-  short2 *eij = reinterpret_cast<short2 *>(cz + nc);
+  float *dub = cz + nc;
+  float *fl = dub + ne;
+  float *lh = fl + ne;
+  float *G = lh + ne;
+  float *rde = G + ne;
+  short2 *eij = reinterpret_cast<short2 *>(rde + ne);
   const int skip = (int)blockIdx.x == fault_block;
   const int n = d.n[st];
   const float tau = (float)d.tau[st], gam = (float)M.div_damp;
-  if (threadIdx.x <= k) {
-    cnt[threadIdx.x] = T.ncnt[(size_t)p * (k + 1) + threadIdx.x];
-    cnt[FAST_KMAX + 1 + threadIdx.x] = T.ecnt[(size_t)p * (k + 1) + threadIdx.x];
+  const int t = threadIdx.x;
+  if (t <= k) {
+    cnt[t] = T.ncnt[(size_t)p * (k + 1) + t];
+    cnt[FAST_KMAX + 1 + t] = T.ecnt[(size_t)p * (k + 1) + t];
   }
+  double accr[FAST_AMAX];
+#pragma unroll
+  for (int j = 0; j < FAST_AMAX; j++) accr[j] = 0.0;
   const uint4 *gcedge = reinterpret_cast<const uint4 *>(T.cedge) + c0i;
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+  for (int c = t; c < nc; c += NT) {
     deta[c] = 0.f;
     rA[c] = T.arA32[c0i + c];
     gc[c] = M.Gc32[cells[c]];
     cedge[c] = gcedge[c];
   }
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+  for (int e = t; e < ne; e += NT) {
     const int ge = edges[e];
-    // dub holds ubar0 for the c0 pass below, then zero
-    EF[e] = make_float4(T.ale32[e0 + e] * M.He32[ge], (float)M.ub0[ge], M.G32[ge], T.arde32[e0 + e]);
-    if (e < eown) acc[e] = 0.0;
+    const float l = T.ale32[e0 + e] * M.He32[ge];
+    lh[e] = l;
+    fl[e] = l * (float)M.ub0[ge];          // ubar0's flux for the c0 pass below, then zero
+    G[e] = M.G32[ge];
+    rde[e] = T.arde32[e0 + e];
     eij[e] = make_short2(T.eIl[e0 + e], T.eJl[e0 + e]);
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+  for (int c = t; c < nc; c += NT) {
     const uint4 w = cedge[c];
     const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
                        (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
@@ -168,13 +179,16 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
     for (int q = 0; q < 6; q++) {
       const int v = vs[q];
       if (v == 0) continue;
-      const float2 pr = EF2[2 * ((v > 0 ? v : -v) - 1)];
-      s += (v > 0 ? pr.x : -pr.x) * pr.y;
+      const float f = fl[(v > 0 ? v : -v) - 1];
+      s += v > 0 ? f : -f;
     }
     cz[c] = s;
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) EF[e].y = 0.f;
+  for (int e = t; e < ne; e += NT) {
+    dub[e] = 0.f;
+    fl[e] = 0.f;
+  }
   const int nown = cnt[0];
   for (int r = 0; r < rounds; r++) {
     const int K = min(k, n - r * k);
@@ -183,51 +197,69 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
       if (K > 0) {
         const float *xe = M.xeta[(r - 1) & 1];
         const float *xu = M.xdub[(r - 1) & 1];
-        for (int c = nown + threadIdx.x; c < nc; c += blockDim.x) deta[c] = xe[cells[c]];
-        for (int e = eown + threadIdx.x; e < ne; e += blockDim.x) EF[e].y = xu[edges[e]];
+        for (int c = nown + t; c < nc; c += NT) deta[c] = xe[cells[c]];
+        for (int e = eown + t; e < ne; e += NT) {
+          const float v = xu[edges[e]];
+          dub[e] = v;
+          fl[e] = lh[e] * v;
+        }
       }
     }
     __syncthreads();
     for (int m = 1; m <= K; m++) {
       const int cn = cnt[K - m + 1];
-      for (int c = threadIdx.x; c < cn; c += blockDim.x) {
-        const float d0 = deta[c];
-        const uint4 w = cedge[c];
-        const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
-                           (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
-        float div = cz[c];
 #pragma unroll
-        for (int q = 0; q < 6; q++) {
-          const int v = vs[q];
-          if (v == 0) continue;
-          const float2 pr = EF2[2 * ((v > 0 ? v : -v) - 1)];
-          div += (v > 0 ? pr.x : -pr.x) * pr.y;
+      for (int j = 0; j < FAST_CMAX; j++) {
+        const int c = t + j * NT;
+        if (c < cn) {
+          const float d0 = deta[c];
+          const uint4 w = cedge[c];
+          const int vs[6] = {(int16_t)(w.x & 0xffff), (int16_t)(w.x >> 16), (int16_t)(w.y & 0xffff), (int16_t)(w.y >> 16),
+                             (int16_t)(w.z & 0xffff), (int16_t)(w.z >> 16)};
+          float div = cz[c];
+#pragma unroll
+          for (int q = 0; q < 6; q++) {
+            const int v = vs[q];
+            if (v == 0) continue;
+            const float f = fl[(v > 0 ? v : -v) - 1];
+            div += v > 0 ? f : -f;
+          }
+          const float dn = d0 - tau * div * rA[c];
+          deta[c] = dn;
+          Y[c] = gc[c] * (dn + gam * (dn - d0));
         }
-        const float dn = d0 - tau * div * rA[c];
-        deta[c] = dn;
-        Y[c] = gc[c] * (dn + gam * (dn - d0));
       }
       __syncthreads();
       const int en = cnt[FAST_KMAX + 1 + K - m];
-      for (int e = threadIdx.x; e < en; e += blockDim.x) {
-        const float4 f = EF[e];
-        const short2 ij = eij[e];
-        if (e < eown) acc[e] += (double)f.y;
-        EF[e].y = f.y + tau * (f.z - (Y[ij.y] - Y[ij.x]) * f.w);
+#pragma unroll
+      for (int j = 0; j < FAST_EMAX; j++) {
+        const int e = t + j * NT;
+        if (e < en) {
+          const float v = dub[e];
+          const short2 ij = eij[e];
+          if (j < FAST_AMAX && e < eown) accr[j < FAST_AMAX ? j : 0] += (double)v;
+          const float nv = v + tau * (G[e] - (Y[ij.y] - Y[ij.x]) * rde[e]);
+          dub[e] = nv;
+          fl[e] = lh[e] * nv;
+        }
       }
       __syncthreads();
     }
     if (r + 1 < rounds && K > 0) {
       float *xe = M.xeta[r & 1];
       float *xu = M.xdub[r & 1];
-      for (int c = threadIdx.x; c < nown; c += blockDim.x) xe[cells[c]] = deta[c];
-      for (int e = threadIdx.x; e < eown; e += blockDim.x) xu[edges[e]] = EF[e].y;
+      for (int c = t; c < nown; c += NT) xe[cells[c]] = deta[c];
+      for (int e = t; e < eown; e += NT) xu[edges[e]] = dub[e];
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < eown; e += blockDim.x) {
-    M.dub[edges[e]] = EF[e].y;
-    M.acc[edges[e]] = acc[e];
+#pragma unroll
+  for (int j = 0; j < FAST_AMAX; j++) {
+    const int e = t + j * NT;
+    if (e < eown) {
+      M.dub[edges[e]] = dub[e];
+      M.acc[edges[e]] = accr[j];
+    }
   }
 }
 

@@ -33,9 +33,9 @@ struct TileSetHost {
 // its 8 signed local edge ids (16 B); per edge (l_e H_e, ubar) and (G, d_e) (16 B each) and its two local cell ids
 // (4 B); per owned edge the sub-step sum acc (8 B); 64 B of alignment slack.
 inline size_t tile_smem_bytes(size_t nc, size_t ne, size_t nown) { return nc * (4 * 8 + 16) + ne * (2 * 16 + 4) + nown * 8 + 64; }
-// The mixed form's tile: per cell deta, Y, 1/area, Gc, c0 (4 B each) and the edge ids (16 B); per edge (l_e H_e, dub,
-// G', 1/d_e) (16 B) and the cell ids (4 B); per owned edge acc (8 B).
-inline size_t tile_smem_bytes_mixed(size_t nc, size_t ne, size_t nown) { return nc * (5 * 4 + 16) + ne * (16 + 4) + nown * 8 + 64; }
+// The mixed form's tile: per cell deta, Y, 1/area, Gc, c0 (4 B each) and the edge ids (16 B); per edge dub, its flux,
+// l_e H_e, G', 1/d_e (4 B each) and the cell ids (4 B); the owned edges' sums live in registers.
+inline size_t tile_smem_bytes_mixed(size_t nc, size_t ne, size_t) { return nc * (5 * 4 + 16) + ne * (5 * 4 + 4) + 64; }
 
 // Compact balanced partition of the N cells into P regions (owner per cell).
 std::vector<int32_t> partition_cells(int N, const int32_t *nbr, int P);
