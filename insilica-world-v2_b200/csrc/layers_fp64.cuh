@@ -285,6 +285,35 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, double tau, int e)
   M.ub[e] = v + tau * ((-(ej - ei)) / g.de[e] + M.G[e]);
 }
 
+
+// The batched step's grid-wide form of the two sub-step passes: the cell pass also stores Y = Gc (eta + gamma (eta -
+// eta_prev)) (in eta_prev's place), the expression bt_u_edge evaluates for each of an edge's two cells, so the edge
+// pass reads two values per edge. Same operations, same bits as bt_eta_cell / bt_u_edge.
+__device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, int i) {
+  const GridDev &g = M.g;
+  const double e0 = M.eta[i];
+  int es[6];
+#pragma unroll
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  double div = 0;
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = es[s];
+    if (e >= 0) div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
+  }
+  const double en = e0 - (tau * div) / g.areaCell[i];
+  M.eta[i] = en;
+  M.eta_prev[i] = M.Gc[i] * (en + M.div_damp * (en - e0));
+}
+
+__device__ __forceinline__ void bt_u_edge_y(const LayersDev &M, double tau, int e) {
+  const GridDev &g = M.g;
+  const double v = M.ub[e];
+  M.acc[e] += v;
+  const double *Y = M.eta_prev;
+  M.ub[e] = v + tau * ((-(Y[g.eJ[e]] - Y[g.eI[e]])) / g.de[e] + M.G[e]);
+}
+
 // ---- stage phase C: layer fluxes and the floor limiter's scale ----
 template <int L>
 __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &a, int i) {

@@ -249,7 +249,8 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
   M.ubs32[e] = U / H;
 }
 
-// ---- fast loop, grid-wide form (stacks without tiles): deviation variables ----
+// ---- fast loop, grid-wide form (stacks without tiles): deviation variables; the cell pass stores Y = Gc (deta +
+// gamma (deta - deta_prev)) in deprev for the edge pass ----
 __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int i) {
   const GridDev &g = M.g;
   int es[6];
@@ -271,23 +272,21 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
     c0 = M.c0[i];
   }
   const float d0 = M.deta[i];
-  M.deprev[i] = d0;
   float div = c0;
 #pragma unroll
   for (int s = 0; s < 6; s++)
     if (es[s] >= 0) div += c[s] * M.dub[es[s]];
-  M.deta[i] = d0 - tau * div * g.rA32[i];
+  const float dn = d0 - tau * div * g.rA32[i];
+  M.deta[i] = dn;
+  M.deprev[i] = M.Gc32[i] * (dn + (float)M.div_damp * (dn - d0));   // Y, what the edge pass reads
 }
 
 __device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) {
   const GridDev &g = M.g;
   const float v = M.dub[e];
   M.acc[e] += (double)v;
-  const int i = g.eI[e], j = g.eJ[e];
-  const float gam = (float)M.div_damp;
-  const float xj = M.deta[j] + gam * (M.deta[j] - M.deprev[j]);
-  const float xi = M.deta[i] + gam * (M.deta[i] - M.deprev[i]);
-  M.dub[e] = v + tau * (M.G32[e] - (M.Gc32[j] * xj - M.Gc32[i] * xi) * g.rde32[e]);
+  const float *Y = M.deprev;
+  M.dub[e] = v + tau * (M.G32[e] - (Y[g.eJ[e]] - Y[g.eI[e]]) * g.rde32[e]);
 }
 
 // ---- stage phase C: layer fluxes (FP64) and the floor limiter ----
