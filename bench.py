@@ -377,7 +377,10 @@ def main():
             m = Member(dg, seed=rank, batch=batch)
         finally:
             set_precision('double')
-        return m, (batch.info() if batch is not None else None)
+        if batch is None:
+            return m, None
+        tuned, _ = batch.autotune(steps=3)       # tile layout by timing (the member's state is restored)
+        return m, dict(batch.info(), autotuned=tuned)
 
     def timed(m):
         """Mean device ms per step over exactly args.steps steps (after the warm-up), max over ranks."""

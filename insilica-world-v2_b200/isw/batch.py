@@ -74,7 +74,7 @@ class Batch:
         saved = [a.clone() for a in arrays]
         if candidates is None:
             candidates = [dict(tiles=False)]
-            for layout, bps, k in itertools.product(('shared', 'packed'), (1, 2), (2, 4, 8)):
+            for layout, bps, k in itertools.product(('shared', 'packed'), (1, 2), (2, 3, 4, 6, 8)):
                 cells = (0,) if layout == 'shared' else ((256, 512) if bps == 2 else (512, 1024))
                 for c in cells:
                     candidates.append(dict(tiles=True, layout=layout, blocks_per_sm=bps, tile_k=k, tile_cells=c))
