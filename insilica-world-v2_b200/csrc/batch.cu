@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL>(M, a.us, a.cdt, i));
   } else if (PH == PH_ETA) {
-    if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], i);
+    if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], j, i);
   } else if (PH == PH_U) {
     if (!d.tiled && j < d.n[st]) fp64::bt_u_edge_y(M, d.tau[st], i);
   } else if (PH == PH_C) {

@@ -289,17 +289,30 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, double tau, int e)
 // The batched step's grid-wide form of the two sub-step passes: the cell pass also stores Y = Gc (eta + gamma (eta -
 // eta_prev)) (in eta_prev's place), the expression bt_u_edge evaluates for each of an edge's two cells, so the edge
 // pass reads two values per edge. Same operations, same bits as bt_eta_cell / bt_u_edge.
-__device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, int i) {
+__device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, int j, int i) {
   const GridDev &g = M.g;
   const double e0 = M.eta[i];
   int es[6];
 #pragma unroll
   for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  // the slot coefficients sign l_e H_e are constant over the stage's sub-steps: formed by sub-step 0, then read back
+  double c[6];
+  if (j == 0) {
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+      const int e = es[s];
+      c[s] = e >= 0 ? (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] : 0.0;
+      M.cw[(size_t)i * 6 + s] = c[s];
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < 6; s++) c[s] = M.cw[(size_t)i * 6 + s];
+  }
   double div = 0;
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
-    if (e >= 0) div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
+    if (e >= 0) div += c[s] * M.ub[e];
   }
   const double en = e0 - (tau * div) / g.areaCell[i];
   M.eta[i] = en;

@@ -256,19 +256,21 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
   int es[6];
   float c[6];
 #pragma unroll
-  for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    es[s] = e;
-    c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] * M.He32[e] : 0.f;
-  }
+  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
   float c0;
-  if (j == 0) {
+  if (j == 0) {                              // slot coefficients sign l_e H_e and c0, constant over the stage
     c0 = 0.f;
 #pragma unroll
-    for (int s = 0; s < 6; s++)
-      if (es[s] >= 0) c0 += c[s] * (float)M.ub0[es[s]];
+    for (int s = 0; s < 6; s++) {
+      const int e = es[s];
+      c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] * M.He32[e] : 0.f;
+      M.cw32[(size_t)i * 6 + s] = c[s];
+      if (e >= 0) c0 += c[s] * (float)M.ub0[e];
+    }
     M.c0[i] = c0;
   } else {
+#pragma unroll
+    for (int s = 0; s < 6; s++) c[s] = M.cw32[(size_t)i * 6 + s];
     c0 = M.c0[i];
   }
   const float d0 = M.deta[i];

@@ -131,10 +131,10 @@ def stack_bytes(g, L, T, mixed):
     N, E, NV = g.N, g.E, g.NV
     R = max(1, T) * L
     doubles = 3 * L * N + 2 * L * E + T * L * N
-    doubles += 5 * N + NV + 5 * L * N + 2 * L * NV + 10 * L * E + 8 * E
+    doubles += 11 * N + NV + 5 * L * N + 2 * L * NV + 10 * L * E + 8 * E
     doubles += 6 * R * N + R * E
     floats = 0
     if mixed:
-        floats += 10 * L * E + L * N + 2 * L * NV + 6 * E + 6 * N
+        floats += 10 * L * E + L * N + 2 * L * NV + 6 * E + 12 * N
         floats += 4 * R * N + R * E
     return 8 * doubles + 4 * floats
