@@ -53,6 +53,7 @@ struct LayersDev {
   // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)
   float *u32, *u1f, *u2f, *D1f, *Z1f, *L1f, *L2f, *q32, *Tp32, *G32, *He32, *ubs32, *Gc32;
   float *c0, *dub, *deta, *deprev, *xeta[2], *xdub[2], *cw32;
+  float *F32, *scale32;                      // mixed form: stored layer fluxes (L x E) and limiter factors (L x N)
   float4 *pk4;
 };
 

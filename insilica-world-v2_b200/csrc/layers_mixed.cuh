@@ -1,11 +1,12 @@
 // Phase functions of the time-split RK3 step, mixed form: the same phases as layers_fp64.cuh (reference layers.py:129-212),
 // with momentum, the TRiSK operators and the slow tendencies in FP32 and the quantities whose size dwarfs their change
 // in FP64, so that FP32 rounding only ever lands on small numbers:
-//   FP64  thicknesses h (stage and final), the layer fluxes F and the limiter, the Montgomery potential B, the free
-//         surface eta0, the barotropic wind at the step start ubar0 and the sub-step sum acc, the final wind u = u0 +
-//         dt T' + (ubar - ubar0), the interfacial stress (vmix);
+//   FP64  thicknesses h (stage and final) and every sum that updates them, the limiter's bound, the Montgomery
+//         potential B, the free surface eta0, the barotropic wind at the step start ubar0 and the sub-step sum acc, the
+//         final wind u = u0 + dt T' + (ubar - ubar0), the interfacial stress (vmix);
 //   FP32  the stage winds u1, u2 (and u's FP32 copy for stage 1), q, the packed neighbour record, the PV flux, KE, the
-//         Laplacians, T' and the column force, H_e, and the fast loop's state.
+//         Laplacians, T' and the column force, H_e, the fast loop's state, and the stored layer fluxes F and limiter
+//         factors (computed in FP64, each stored once per edge or cell).
 // The fast loop runs in deviation form: deta = eta - eta0 and dub = ubar - ubar0, both zero at each stage's start and
 // small, with eta0's gradient folded into the column force once per stage (G' = G - (Gc_J eta0_J - Gc_I eta0_I) / d_e)
 // and ubar0's divergence once per cell (c0 = sum sign l_e H_e ubar0); acc sums dub in FP64, so the mean barotropic wind
@@ -314,7 +315,7 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const MStageArgs 
     for (int k = 0; k < L; k++) {
       const double he = 0.5 * (a.hs[(size_t)k * N + ea] + a.hs[(size_t)k * N + eb]);
       const double F = he * ((double)(a.us[(size_t)k * E + e] - ubs) + ubm);
-      if (mine) M.F[(size_t)k * E + e] = F;
+      if (mine) M.F32[(size_t)k * E + e] = (float)F;
       const double f = F * le * a.cdt;
       if (mine) { if (f > 0) out[k] += f; }
       else if (!(f > 0)) out[k] -= f;
@@ -325,11 +326,20 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const MStageArgs 
   for (int k = 0; k < L; k++) {
     const double avail = a.h0[(size_t)k * N + i] - M.floor_;
     const double cap = (avail > 0 ? avail : 0.0) * A;
-    M.scale[(size_t)k * N + i] = out[k] > cap ? cap / out[k] : 1.0;
+    M.scale32[(size_t)k * N + i] = out[k] > cap ? __double2float_rz(cap / out[k]) : 1.f;   // rounded toward zero
   }
 }
 
 // ---- stage phase D: h (FP64) and the stage wind ----
+// The limited flux of layer k at edge e: the FP32 flux times its upwind cell's FP32 limiter factor, product in FP64.
+// One value per edge, used by both cells and by Fm, so volume and tracer mass move between cells exactly.
+__device__ __forceinline__ double limited(const LayersDev &M, int k, int e) {
+  const GridDev &g = M.g;
+  const float f = M.F32[(size_t)k * g.E + e];
+  const float sc = f > 0.f ? M.scale32[(size_t)k * g.N + g.eI[e]] : M.scale32[(size_t)k * g.N + g.eJ[e]];
+  return (double)f * (double)sc;
+}
+
 template <int L>
 __device__ __forceinline__ void h_cell(const LayersDev &M, const MStageArgs &a, int i) {
   const GridDev &g = M.g;
@@ -346,7 +356,7 @@ __device__ __forceinline__ void h_cell(const LayersDev &M, const MStageArgs &a, 
     if (e < 0) continue;
     const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
 #pragma unroll
-    for (int k = 0; k < L; k++) div[k] += c * fp64::limited(M, k, e);
+    for (int k = 0; k < L; k++) div[k] += c * limited(M, k, e);
   }
   const double rA = g.rA[i];
 #pragma unroll
@@ -367,7 +377,7 @@ __device__ __forceinline__ void u_edge(const LayersDev &M, const MStageArgs &a, 
     const size_t o = (size_t)k * E + e;
     const float tp = M.Tp32[o];
     if (a.un) {
-      if (a.Fm) a.Fm[o] = fp64::limited(M, k, e) * le * a.dt;
+      if (a.Fm) a.Fm[o] = limited(M, k, e) * le * a.dt;
       a.un[o] = a.u0[o] + (a.cdt * (double)tp + (double)dub);
     } else {
       a.unf[o] = a.u0f[o] + ((float)a.cdt * tp + dub);

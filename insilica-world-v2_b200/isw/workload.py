@@ -135,6 +135,6 @@ def stack_bytes(g, L, T, mixed):
     doubles += 6 * R * N + R * E
     floats = 0
     if mixed:
-        floats += 10 * L * E + L * N + 2 * L * NV + 6 * E + 12 * N
+        floats += 11 * L * E + 2 * L * N + 2 * L * NV + 6 * E + 12 * N
         floats += 4 * R * N + R * E
     return 8 * doubles + 4 * floats
