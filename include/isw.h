@@ -11,6 +11,8 @@
  *   isw_grid_create            src/insilica/gpu.py:55-83     DeviceGrid(grid)            (+ d2_stencil, gpu.py:86-108)
  *   isw_layers_create          src/insilica/layers.py:36-92  Layers(dg, layers, b, ...)
  *   isw_layers_step            src/insilica/layers.py:185-212 Layers.step(h, u, dt, nfast, Fm)
+ *   isw_layers_step_air        the same with theta: the air branch (layers.py:134-136, 152-166, 187-192, 203-206)
+ *   isw_layers_update_gfast    src/insilica/layers.py:104-109 Layers.update_gfast(h, theta)
  *   isw_layers_substeps        src/insilica/layers.py:99-102 Layers.substeps(h, dt)
  *   isw_layers_lap             src/insilica/layers.py:123-127 Layers._lap(u, out)   (used by lap_max, :111-121)
  *   isw_transport_create       src/insilica/transport.py:19-30 Transport(dg, layers, beta, tracers)
@@ -88,6 +90,10 @@ typedef struct isw_layers_params {
   double nu4, floor_, rotation, div_damp, thin, vmix, vmix_cd;
   const double *b;                        /* N topography (host) or NULL for none */
   int precision;                          /* ISW_FP64 or ISW_MIXED */
+  /* air layers (reference Layers(air=...)): h is mass per area (kg/m^2), each layer carries a potential temperature;
+   * cp, kappa, rd the air's constants, p0 the reference pressure of theta (Pa). air = 0: Boussinesq layers. */
+  int air;
+  double cp, kappa, rd, p0;
 } isw_layers_params;
 
 const char *isw_last_error(void);
@@ -100,7 +106,12 @@ int isw_layers_create(isw_grid *g, const isw_layers_params *p, isw_layers **out)
 int isw_layers_destroy(isw_layers *s);
 /* One time-split RK3 step in place on h (L x N), u (L x E); Fm (L x E, or NULL) receives l dt F of the final stage. */
 int isw_layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, void *stream);
-/* max(1, ceil(dt sqrt(max_i g sum_k h_k) / (0.5 d_min))): synchronises `stream`. */
+/* One step of air layers (reference Layers.step(h, u, dt, nfast, Fm, theta), layers.py:185-206 with the air branch of
+ * _stage, :134-136 and :152-166): theta (L x N) is read and, with the interfacial stress's heating, updated in place. */
+int isw_layers_step_air(isw_layers *s, double *h, double *u, double *Fm, double *theta, double dt, int nfast, void *stream);
+/* Air layers: the fast mode's coefficient per cell from the state (reference Layers.update_gfast, layers.py:104-109). */
+int isw_layers_update_gfast(isw_layers *s, const double *h, const double *theta, void *stream);
+/* max(1, ceil(dt sqrt(max_i Gc_i sum_k h_k) / (0.5 d_min))): synchronises `stream`. */
 int isw_layers_substeps(isw_layers *s, const double *h, double dt, int *out, void *stream);
 /* out (L x E) = the edge vector Laplacian of u (L x E). */
 int isw_layers_lap(isw_layers *s, const double *u, double *out, void *stream);

@@ -43,12 +43,17 @@ struct LayersDev {
   int L, precision;
   double grav, nu4, floor_, div_damp, thin, vmix, vmix_cd;
   double gp[LMAX], drag[LMAX], stress[LMAX];
-  const double *b, *fV, *Gc;
+  const double *b, *fV;
+  double *Gc;                                // the fast mode's coefficient per cell: g, or for air layers R T_s / mu
   double *B, *q, *Tp, *F, *scale, *G, *He, *ubs, *ub0, *ub, *acc, *eta0, *eta, *eta_prev;
   double *h1, *h2, *u1, *u2, *D1, *Z1, *L1, *L2, *hedge, *diss, *pk;
   double *ub2;                               // second exchange buffer of the tiled fast loop
   double *cw;                                // grid-wide fast loop: per cell and slot sign l_e H_e (N x 6)
   double *red;                               // reduction scratch (substeps)
+  // air layers (h = mass per area, theta per layer): their constants and scratch
+  int air;
+  double cpa, kap, rda, p0;
+  double *S, *pibar, *muf, *phi, *uf, *accL;
   // mixed-form scratch (allocated for ISW_MIXED only): FP32 stage winds and operators; the fast loop in deviation form
   // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)
   float *u32, *u1f, *u2f, *D1f, *Z1f, *L1f, *L2f, *q32, *Tp32, *G32, *He32, *ubs32, *Gc32;

@@ -7,7 +7,7 @@
 #include "transport_fp64.cuh"
 
 struct GraphEntry {
-  const double *h, *u, *Fm;
+  const double *h, *u, *Fm, *theta;
   double dt;
   int nfast;
   cudaGraphExec_t exec;

@@ -11,6 +11,7 @@
 
 #include "common.cuh"
 #include "handles.cuh"
+#include "layers_air.cuh"
 #include "layers_fp64.cuh"
 
 namespace isw {
@@ -50,9 +51,75 @@ __global__ void __launch_bounds__(THREADS) k_stage_e(const LayersDev M, const St
 }
 
 template <int L>
-__global__ void __launch_bounds__(THREADS) k_stage_s(const LayersDev M, const StageArgs a) {
+__global__ void __launch_bounds__(THREADS) k_stage_s(const LayersDev M, const StageArgs a, const double *__restrict__ theta) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < M.g.E) fp64::slow_edge<L>(M, a.us, a.cdt, t);
+  if (t < M.g.E) fp64::slow_edge<L>(M, a.us, a.cdt, t, theta);
+}
+
+// ---- air layers ----
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_stiff(const LayersDev M, const double *__restrict__ h, const double *__restrict__ theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::air_stiff_cell<L>(M, h, theta, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_gfast(const LayersDev M, const double *__restrict__ h, const double *__restrict__ theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::air_gfast_cell<L>(M, h, theta, t);
+}
+
+// stage A for air: B and pibar, the PV pass, and the fast state's masses
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_a(const LayersDev M, const StageArgs a, const double *__restrict__ theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) {
+    fp64::air_bern_cell<L>(M, a.hs, a.us, theta, t);
+    fp64::air_fast_init_cell<L>(M, a.h0, t);
+  } else if (t < M.g.N + M.g.NV) {
+    fp64::pv_vertex<L>(M, a.hs, a.us, t - M.g.N);
+  }
+}
+
+// stage E for air: the edge records and the fast state's winds
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_e(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) {
+    fp64::edge_hq<L>(M, a.hs, a.us, t);
+    fp64::air_fast_init_edge<L>(M, a.u0, t);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_af_muphi(const LayersDev M, double tau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::af_muphi_cell<L>(M, tau, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_af_u(const LayersDev M, double tau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::af_u_edge<L>(M, tau, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_c(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::air_scale_cell<L>(M, a, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_air_d(const LayersDev M, const StageArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::h_cell<L>(M, a, t);
+  else if (t < M.g.N + M.g.E) fp64::air_u_edge<L>(M, a, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_vmix_heat(const LayersDev M, const double *__restrict__ h, double *__restrict__ theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::vmix_heat_cell<L>(M, h, theta, t);
 }
 
 __global__ void __launch_bounds__(THREADS) k_bt_eta(const LayersDev M, double tau) {
@@ -189,7 +256,7 @@ void enqueue_step(isw_layers *s, double *h, double *u, double *Fm, double dt, in
     a.inv_n = 1.0 / a.n;
     ISW_DISPATCH_L(L, (k_stage_a<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, a)));
     ISW_DISPATCH_L(L, (k_stage_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a)));
-    ISW_DISPATCH_L(L, (k_stage_s<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_stage_s<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a, nullptr)));
     for (int j = 0; j < a.n; j++) {
       k_bt_eta<<<blocks_for(N), THREADS, 0, st>>>(M, a.tau);
       k_bt_u<<<blocks_for(E), THREADS, 0, st>>>(M, a.tau);
@@ -202,11 +269,62 @@ void enqueue_step(isw_layers *s, double *h, double *u, double *Fm, double dt, in
   ISW_CUDA(cudaGetLastError());
 }
 
+// One step of air layers in order on `st` (reference layers.py:185-206 with _stage's air branch, :134-136, 152-166):
+// air_stiff, the nabla^4 passes, per stage A (air_bern + PV + fast masses), E (+ fast winds), S (+ pibar grad theta),
+// n x (af_muphi, af_u), C (af_flux + lay_scale), D (lay_h, u = uf, Fm); then vmix and its heat.
+void enqueue_step_air(isw_layers *s, double *h, double *u, double *Fm, double *theta, double dt, int nfast, cudaStream_t st) {
+  const LayersDev &M = s->d;
+  const GridDev &g = M.g;
+  const int L = M.L;
+  const int N = g.N, E = g.E, NV = g.NV;
+  ISW_DISPATCH_L(L, (k_air_stiff<LL><<<blocks_for(N), THREADS, 0, st>>>(M, h, theta)));
+  if (M.nu4 != 0) {
+    ISW_DISPATCH_L(L, (k_lap_cv<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, u)));
+    ISW_DISPATCH_L(L, (k_lap_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, M.L1)));
+    ISW_DISPATCH_L(L, (k_lap_cv<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, M.L1)));
+    ISW_DISPATCH_L(L, (k_lap_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, M.L2)));
+  }
+  const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
+  for (int st_i = 0; st_i < 3; st_i++) {
+    const double c = cs[st_i];
+    StageArgs a;
+    a.h0 = h;
+    a.u0 = u;
+    a.hs = st_i == 0 ? h : st_i == 1 ? M.h1 : M.h2;
+    a.us = st_i == 0 ? u : st_i == 1 ? M.u1 : M.u2;
+    a.hn = st_i == 0 ? M.h1 : st_i == 1 ? M.h2 : h;
+    a.un = st_i == 0 ? M.u1 : st_i == 1 ? M.u2 : u;
+    a.Fm = st_i == 2 ? Fm : nullptr;
+    a.cdt = c * dt;
+    a.dt = dt;
+    const double cn = std::ceil(c * nfast);
+    a.n = cn > 1 ? (int)cn : 1;
+    a.tau = c * dt / a.n;
+    a.inv_n = 1.0 / a.n;
+    ISW_DISPATCH_L(L, (k_air_a<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, a, theta)));
+    ISW_DISPATCH_L(L, (k_air_e<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_stage_s<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a, theta)));
+    for (int j = 0; j < a.n; j++) {
+      ISW_DISPATCH_L(L, (k_af_muphi<LL><<<blocks_for(N), THREADS, 0, st>>>(M, a.tau)));
+      ISW_DISPATCH_L(L, (k_af_u<LL><<<blocks_for(E), THREADS, 0, st>>>(M, a.tau)));
+    }
+    ISW_DISPATCH_L(L, (k_air_c<LL><<<blocks_for(N), THREADS, 0, st>>>(M, a)));
+    ISW_DISPATCH_L(L, (k_air_d<LL><<<blocks_for(N + E), THREADS, 0, st>>>(M, a)));
+  }
+  if ((M.vmix != 0 || M.vmix_cd != 0) && L > 1) {
+    ISW_DISPATCH_L(L, (k_vmix<LL><<<blocks_for(E), THREADS, 0, st>>>(M, h, u, dt)));
+    ISW_DISPATCH_L(L, (k_vmix_heat<LL><<<blocks_for(N), THREADS, 0, st>>>(M, h, theta)));
+  }
+  ISW_CUDA(cudaGetLastError());
+}
+
 isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
   if (!g || !p) fail(ISW_EINVAL, "layers: null grid or parameters");
   if (p->L < 1 || p->L > LMAX) fail(ISW_EINVAL, "layers: L must be in 1..8");
   if (p->L > 1 && !p->gprime) fail(ISW_EINVAL, "layers: gprime needs L - 1 values");
   if (p->precision != ISW_FP64 && p->precision != ISW_MIXED) fail(ISW_EINVAL, "layers: precision must be ISW_FP64 or ISW_MIXED");
+  if (p->air && p->precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers: air layers run in the FP64 form only");
+  if (p->air && !(p->cp > 0 && p->kappa > 0 && p->rd > 0 && p->p0 > 0)) fail(ISW_EINVAL, "layers: air constants must be positive");
   ISW_CUDA(cudaSetDevice(g->device));
   isw_layers *s = new isw_layers();
   s->grid = g;
@@ -251,6 +369,12 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
     d.ub2 = dalloc(s, E);
     d.cw = dalloc(s, (size_t)N * 6);
+    if (p->air) {
+      d.air = 1;
+      d.cpa = p->cp; d.kap = p->kappa; d.rda = p->rd; d.p0 = p->p0;
+      d.S = dalloc(s, (size_t)L * N); d.pibar = dalloc(s, (size_t)L * N); d.muf = dalloc(s, (size_t)L * N);
+      d.phi = dalloc(s, (size_t)L * N); d.uf = dalloc(s, (size_t)L * E); d.accL = dalloc(s, (size_t)L * E);
+    }
     if (p->precision == ISW_MIXED) {
       auto f = [&](size_t n) { return talloc_t<float>(s, n); };
       d.u32 = f((size_t)L * E); d.u1f = f((size_t)L * E); d.u2f = f((size_t)L * E);
@@ -303,27 +427,33 @@ void layers_step_mixed(isw_layers *s, double *h, double *u, double *Fm, double d
     int slot = -1;
     ok(isw_batch_add(s->solo, s, nullptr, h, u, Fm, nullptr, nullptr, nullptr, 0, dt, nfast, &slot));
     s->solo_slot = slot;
-    k = GraphEntry{h, u, Fm, dt, nfast, nullptr};
+    k = GraphEntry{h, u, Fm, nullptr, dt, nfast, nullptr};
   }
   ok(isw_batch_step(s->solo, st));
 }
 
-void layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
+void layers_step(isw_layers *s, double *h, double *u, double *Fm, double *theta, double dt, int nfast, cudaStream_t st) {
   if (!h || !u) fail(ISW_EINVAL, "layers.step: null h or u");
   if (nfast < 1) fail(ISW_EINVAL, "layers.step: nfast must be >= 1");
   if (!(dt > 0) || !std::isfinite(dt)) fail(ISW_EINVAL, "layers.step: dt must be positive and finite");
+  if (s->d.air && !theta) fail(ISW_EINVAL, "layers.step: air layers step with theta (isw_layers_step_air)");
+  if (!s->d.air && theta) fail(ISW_EINVAL, "layers.step: theta is for air layers");
   if (s->d.precision == ISW_MIXED) {
     layers_step_mixed(s, h, u, Fm, dt, nfast, st);
     return;
   }
+  auto enqueue = [&](cudaStream_t q) {
+    if (s->d.air) enqueue_step_air(s, h, u, Fm, theta, dt, nfast, q);
+    else enqueue_step(s, h, u, Fm, dt, nfast, q);
+  };
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   ISW_CUDA(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) {   // the caller is capturing a graph of its own: just queue the kernels
-    enqueue_step(s, h, u, Fm, dt, nfast, st);
+    enqueue(st);
     return;
   }
   for (auto it = s->graphs.begin(); it != s->graphs.end(); ++it)
-    if (it->h == h && it->u == u && it->Fm == Fm && it->dt == dt && it->nfast == nfast) {
+    if (it->h == h && it->u == u && it->Fm == Fm && it->theta == theta && it->dt == dt && it->nfast == nfast) {
       s->graphs.splice(s->graphs.begin(), s->graphs, it);
       ISW_CUDA(cudaGraphLaunch(it->exec, st));
       return;
@@ -331,7 +461,7 @@ void layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int
   cudaGraph_t graph = nullptr;
   ISW_CUDA(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_step(s, h, u, Fm, dt, nfast, s->cap);
+    enqueue(s->cap);
   } catch (...) {
     cudaStreamEndCapture(s->cap, &graph);
     if (graph) cudaGraphDestroy(graph);
@@ -342,12 +472,19 @@ void layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, int
   const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   ISW_CUDA(ie);
-  s->graphs.push_front(GraphEntry{h, u, Fm, dt, nfast, exec});
+  s->graphs.push_front(GraphEntry{h, u, Fm, theta, dt, nfast, exec});
   if (s->graphs.size() > GRAPH_CACHE) {
     cudaGraphExecDestroy(s->graphs.back().exec);
     s->graphs.pop_back();
   }
   ISW_CUDA(cudaGraphLaunch(exec, st));
+}
+
+void layers_update_gfast(isw_layers *s, const double *h, const double *theta, cudaStream_t st) {
+  if (!s->d.air) fail(ISW_EINVAL, "layers.update_gfast: for air layers");
+  if (!h || !theta) fail(ISW_EINVAL, "layers.update_gfast: null h or theta");
+  ISW_DISPATCH_L(s->d.L, (k_air_gfast<LL><<<blocks_for(s->d.g.N), THREADS, 0, st>>>(s->d, h, theta)));
+  ISW_CUDA(cudaGetLastError());
 }
 
 int layers_substeps(isw_layers *s, const double *h, double dt, cudaStream_t st) {
@@ -408,7 +545,24 @@ int isw_layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, 
   return guarded([&] {
     if (!s) fail(ISW_EINVAL, "layers.step: null handle");
     ISW_CUDA(cudaSetDevice(s->grid->device));
-    layers_step(s, h, u, Fm, dt, nfast, (cudaStream_t)stream);
+    layers_step(s, h, u, Fm, nullptr, dt, nfast, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_step_air(isw_layers *s, double *h, double *u, double *Fm, double *theta, double dt, int nfast, void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.step: null handle");
+    if (!theta) fail(ISW_EINVAL, "layers.step: null theta");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    layers_step(s, h, u, Fm, theta, dt, nfast, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_update_gfast(isw_layers *s, const double *h, const double *theta, void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.update_gfast: null handle");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    layers_update_gfast(s, h, theta, (cudaStream_t)stream);
   });
 }
 

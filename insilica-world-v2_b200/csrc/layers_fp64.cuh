@@ -194,7 +194,8 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 
 // ---- stage phase S: slow tendencies ----
 template <int L>
-__device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__restrict__ u, double dts, int e) {
+__device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__restrict__ u, double dts, int e,
+                                          const double *__restrict__ theta = nullptr) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
   double he[L], cap[L], qf[L], Q[L];
@@ -241,6 +242,11 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
     if (ck != 0) {
       const double r = ck / (he[k] > M.floor_ ? he[k] : M.floor_);
       d = d - ((r * dts > 1e-8) ? (1 - exp(-r * dts)) / dts : r) * ue;
+    }
+    if (theta) {                   // air layers: + pibar grad(theta) (reference layers.cu:322-326)
+      const double *tl = theta + (size_t)k * N;
+      const double *pl = M.pibar + (size_t)k * N;
+      d = d + (0.5 * (pl[a] + pl[b]) * (tl[b] - tl[a])) / de;
     }
     if (M.nu4 != 0) d = d - M.nu4 * M.L2[(size_t)k * E + e];
     T[k] = d;

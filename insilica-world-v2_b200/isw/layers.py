@@ -2,9 +2,10 @@
 
 ``Layers`` keeps the reference's constructor and methods (``step``, ``substeps``, ``lap_max``, ``energy``) and argument
 meanings; the arrays are the caller's device arrays (h (L, N), u (L, E), Fm (L, E), FP64), updated in place on the
-current CUDA stream. Options of the reference that this core does not implement raise ``NotImplementedError`` at
-construction (air layers, walls, the shelf, the squeezed-layer bed, per-cell buoyancy, tides, the bottom drag law) or
-at the call (``exchange``).
+current CUDA stream. Air layers (``air=dict(cp=, kappa=, rd=)``: h is mass per area, ``step`` and ``update_gfast`` take
+the layers' potential temperature theta, updated in place by the interfacial stress's heating) run in the FP64 form.
+Options of the reference that this core does not implement raise ``NotImplementedError`` at construction (walls, the
+shelf, the squeezed-layer bed, per-cell buoyancy, tides, the bottom drag law) or at the call (``exchange``).
 """
 import ctypes
 import math
@@ -19,14 +20,15 @@ LMAX = 8
 FAST_COURANT = 0.5          # fast sub-step: tau sqrt(gH) / d_min <= this (reference layers.py:31)
 DIV_DAMP = 0.1              # divergence damping of the fast mode (reference layers.py:32)
 GRAV = 9.80616
+P0 = 1.0e5                  # reference pressure of potential temperature, Pa (reference constants.py:14)
+R_DRY, CP_DRY = 287.04, 1004.6   # the dry air's constants (reference constants.py:8-10)
+KAPPA = R_DRY / CP_DRY
 
 
 class Layers:
     def __init__(self, dg, layers=1, b=None, grav=GRAV, gprime=(), drag=0.0, stress=0.0, nu4=0.0, floor=1.0, rotation=1.0,
                  div_damp=DIV_DAMP, air=None, vmix=0.0, thin=2.0, wall=None, thin_wind=0.0, shelf=0.0, vmix_cd=0.0,
                  shelf_bed=False):
-        if air:
-            raise NotImplementedError('Layers: air layers (the theta branch) are not implemented by this core')
         if wall is not None:
             raise NotImplementedError('Layers: thin walls are not implemented by this core')
         if shelf:
@@ -41,7 +43,11 @@ class Layers:
         self.dg, self.L = dg, layers
         self.grav, self.nu4, self.floor, self.div_damp, self.thin = grav, nu4, floor, div_damp, thin
         self.vmix, self.vmix_cd = vmix, vmix_cd
-        self.air = None
+        self.air = air
+        # the air's constants (reference layers.py:64-65: cp 1004.6, kappa, R 287.04 unless the air dict gives them)
+        self.cpa, self.kap, self.rda = (air or {}).get('cp', CP_DRY), (air or {}).get('kappa', KAPPA), (air or {}).get('rd', R_DRY)
+        if air and dg.mixed:
+            raise NotImplementedError('Layers: air layers run in the FP64 form only')
         self.shelf = 0.0
         self.sig = self.zm = self.tide = None
         self.cd_bot, self.cbot = 0.0, None
@@ -56,7 +62,8 @@ class Layers:
         p = _lib.LayersParams(L=layers, grav=float(grav), gprime=_lib.host_ptr(gp), drag=_lib.host_ptr(self._drag),
                               stress=_lib.host_ptr(self._stress), nu4=float(nu4), floor_=float(floor), rotation=float(rotation),
                               div_damp=float(div_damp), thin=float(thin), vmix=float(vmix), vmix_cd=float(vmix_cd),
-                              b=_lib.host_ptr(self._b_host), precision=self.precision)
+                              b=_lib.host_ptr(self._b_host), precision=self.precision, air=1 if air else 0,
+                              cp=float(self.cpa), kappa=float(self.kap), rd=float(self.rda), p0=P0)
         h = ctypes.c_void_p()
         _lib.check(_lib.isw_layers_create(dg.handle, ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -75,14 +82,19 @@ class Layers:
 
     def step(self, h, u, dt, nfast, Fm=None, theta=None, stream=None):
         """One time-split RK3 step in place on h (L, N), u (L, E), with nfast fast sub-steps per full step (stage s takes
-        ceil(c_s nfast)). Fm, if given, receives each layer's final-stage volume flux l dt F (m^3)."""
-        if theta is not None:
-            raise NotImplementedError('Layers.step: theta (air layers) is not implemented by this core')
+        ceil(c_s nfast)). Fm, if given, receives each layer's final-stage volume flux l dt F (m^3; for air layers the
+        mass flux, kg). Air layers take theta (L, N), which the interfacial stress's heating updates in place."""
         sh, su = self._shapes()
         dev = self.dg.device
+        if bool(self.air) != (theta is not None):
+            raise ValueError('Layers.step: theta is required for air layers and only for them')
         ph = device_ptr(h, shape=sh, name='h', device=dev)
         pu = device_ptr(u, shape=su, name='u', device=dev)
         pf = device_ptr(Fm, shape=su, name='Fm', device=dev)
+        if self.air:
+            pt = device_ptr(theta, shape=sh, name='theta', device=dev)
+            _lib.check(_lib.isw_layers_step_air(self._h, ph, pu, pf, pt, float(dt), int(nfast), stream_of(dev, stream)))
+            return
         _lib.check(_lib.isw_layers_step(self._h, ph, pu, pf, float(dt), int(nfast), stream_of(dev, stream)))
 
     def substeps(self, h, dt, stream=None):
@@ -115,17 +127,21 @@ class Layers:
             out = torch.empty_like(v)
         return lam
 
-    def update_gfast(self, h, theta):
+    def update_gfast(self, h, theta, stream=None):
+        """Air layers: each cell's fast-mode coefficient R T_s / mu (+ its interfaces' terms) from the current state
+        (reference layers.py:104-109); substeps() then uses it. A no-op for Boussinesq layers."""
         if self.air:
-            raise NotImplementedError('Layers.update_gfast: air layers are not implemented by this core')
+            sh, _ = self._shapes()
+            dev = self.dg.device
+            _lib.check(_lib.isw_layers_update_gfast(self._h, device_ptr(h, shape=sh, name='h', device=dev),
+                                                    device_ptr(theta, shape=sh, name='theta', device=dev), stream_of(dev, stream)))
 
     def exchange(self, wx, h, u, M, psi, theta=None, seq=False):
         raise NotImplementedError('Layers.exchange: the between-layer exchange hook is not implemented by this core')
 
     def energy(self, h, u, theta=None):
-        """Total energy per unit density (J/rho0), Boussinesq form (reference layers.py:234-253), on the host."""
-        if theta is not None:
-            raise NotImplementedError('Layers.energy: air layers are not implemented by this core')
+        """Total energy per unit density (J/rho0; reference layers.py:234-253), on the host. Air layers: kinetic plus
+        enthalpy sum mu pibar theta plus the ground's potential g b mu."""
         gh = self.dg.host
         hh = h.detach().cpu().numpy() if isinstance(h, torch.Tensor) else np.asarray(h)
         uu = u.detach().cpu().numpy() if isinstance(u, torch.Tensor) else np.asarray(u)
@@ -133,6 +149,14 @@ class Layers:
         ce = np.where(gh.cellEdge >= 0, gh.cellEdge, 0)
         ok = gh.cellEdge >= 0
         kin = sum(np.sum(hh[k] * np.sum(np.where(ok, gh.le[ce] * gh.de[ce] * 0.25 * uu[k][ce] ** 2, 0.0), axis=1)) for k in range(self.L))
+        if self.air:
+            if theta is None:
+                raise ValueError('Layers.energy: air layers need theta')
+            th = theta.detach().cpu().numpy() if isinstance(theta, torch.Tensor) else np.asarray(theta)
+            p = np.cumsum(self.grav * hh, axis=0)
+            pt = np.vstack([np.zeros((1, hh.shape[1])), p[:-1]])
+            pib = self.cpa * (p ** (self.kap + 1) - pt ** (self.kap + 1)) / ((self.kap + 1) * (p - pt) * P0 ** self.kap)
+            return float(kin + np.sum(gh.areaCell * (np.sum(hh * pib * th, axis=0) + self.grav * b * hh.sum(0))))
         z = b + np.cumsum(hh[::-1], axis=0)[::-1]
         pot = np.sum(gh.areaCell * self.grav * (z[0] ** 2 - b ** 2) / 2)
         for k in range(1, self.L):

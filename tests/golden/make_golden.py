@@ -15,6 +15,10 @@ Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
 - outcrop_n4.npz the reference's own 'outcrop' case (floor, stress, nu4) with the cosine-bell tracer: 24 steps
 - bell_n4.npz    transport alone (solid-body flux): 20 steps of order 1 and of order 3
 - dsum.npz       deterministic tree sums of fixed inputs
+- airtheta_n4.npz the reference's air layers (h = mass per area, theta per layer; layers.py air branch) from its own
+                 aquaplanet start (cases.aqua), surface drag, nabla^4, interfacial stress with its heating: 12 steps
+
+`--only NAME` writes one fixture (e.g. `--only airtheta`).
 """
 import argparse
 import hashlib
@@ -53,6 +57,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference')
     ap.add_argument('--cache', default='/tmp/isw-grid-cache')
+    ap.add_argument('--only', default=None)
     a = ap.parse_args()
     os.environ['INSILICA_PRECISION'] = 'double'
     os.environ['INSILICA_CACHE'] = a.cache
@@ -70,11 +75,14 @@ def main():
     from isw import cases as mycases
 
     base = gridmod.get(4)
+    g = gridmod.for_planet(base, 6.371e6, 7.292e-5, 9.80616)
+    dg = DeviceGrid(g)
+    if a.only == 'airtheta':
+        save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
+        return
     save('grid_n4.npz', {k: getattr(base, k) for k in GRID_KEYS})
 
     # ---- config 1: Williamson 2, one layer ----
-    g = gridmod.for_planet(base, 6.371e6, 7.292e-5, 9.80616)
-    dg = DeviceGrid(g)
     h0, b, u0 = rcases.initial_state(g, 'w2')
     core = Layers(dg, 1, b=b)
     h, u = cp.asarray(h0[None]), cp.asarray(u0[None])
@@ -173,6 +181,36 @@ def main():
         d[f'x_{n}'] = dsum(cp.asarray(x))
         d[f'xy_{n}'] = dsum(cp.asarray(x), cp.asarray(y))
     save('dsum.npz', d)
+    save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
+
+
+def air_theta(cp, g, dg, Layers, rcases, mycases):
+    """The reference's air layers (Layers(air=...), step(..., theta=...)) from its aquaplanet start (cases.aqua: three
+    layers at rest, theta 415 / 342.5 / 290 - 30 sin^2 phi K) over flat ground, the aqua preset's surface drag and
+    nabla^4 (visc4_U 15), floor 10 kg/m^2, interfacial stress 5e-3 kg/m^2/s (so its heating, vmix_heat, runs too),
+    dt 1800 s (the preset's at n = 4), nfast from the world's rule ceil(1.2 substeps) after update_gfast."""
+    h0, b, u0, x = rcases.aqua(g)
+    theta0 = x['theta']
+    nu4 = mycases.visc4(g, 15.0)
+    stress = [0.0, 0.0, rcases.SURFACE_DRAG]
+    air = dict(t_ref=288.0)
+    core = Layers(dg, 3, b=b, gprime=[0.0, 0.0], stress=stress, nu4=nu4, floor=10.0, air=air, vmix=5e-3)
+    h, u, theta = cp.asarray(h0), cp.asarray(u0), cp.asarray(theta0)
+    dt = 1800.0
+    core.update_gfast(h, theta)
+    gc0 = core.Gc.get()
+    sub = core.substeps(h, dt)
+    nfast = int(math.ceil(1.2 * sub))
+    Fm = cp.zeros((3, g.E))
+    d = dict(dt=dt, nfast=nfast, substeps=sub, nu4=nu4, stress=np.array(stress), floor=10.0, vmix=5e-3, h0=h0, u0=u0,
+             theta0=theta0, b=b, Gc0=gc0, cp=core.cpa, kappa=core.kap, rd=core.rda)
+    for st in range(1, 13):
+        core.step(h, u, dt, nfast, Fm, theta=theta)
+        if st == 1:
+            d.update(h1=h.get(), u1=u.get(), theta1=theta.get(), Fm1=Fm.get())
+    core.update_gfast(h, theta)
+    d.update(h=h.get(), u=u.get(), theta=theta.get(), Fm=Fm.get(), Gc=core.Gc.get())
+    return d
 
 
 if __name__ == '__main__':

@@ -213,11 +213,20 @@ def test_repeat_runs_identical(dev, isw, grid4):
 
 
 def test_unsupported_options_refused(dev, isw, grid4):
+    """Options this core does not build are refused at construction: walls, the shelf, and air layers in the mixed
+    form (air layers run in the FP64 form)."""
     gpu, layers, _ = isw
     dg = gpu.DeviceGrid(grid4)
-    for kw in (dict(air={'cp': 1004.6}), dict(wall=np.ones(dg.E)), dict(shelf=50.0)):
+    for kw in (dict(wall=np.ones(dg.E)), dict(shelf=50.0)):
         with pytest.raises(NotImplementedError):
             layers.Layers(dg, 1, **kw)
+    gpu.set_precision('mixed')
+    try:
+        dgm = gpu.DeviceGrid(grid4)
+    finally:
+        gpu.set_precision('double')
+    with pytest.raises(NotImplementedError):
+        layers.Layers(dgm, 2, gprime=[0.0], air={'cp': 1004.6})
 
 
 def test_bad_arguments_rejected(dev, isw, grid4):
@@ -232,3 +241,34 @@ def test_bad_arguments_rejected(dev, isw, grid4):
         core.step(h.float(), u, 900.0, 2)
     with pytest.raises(ValueError):
         core.step(h, u, -1.0, 2)
+
+
+def test_air_layers_golden(dev, isw, grid4):
+    """Air layers (h = mass per area, theta per layer: the reference's air branch) from the reference's aquaplanet start,
+    with surface drag, nabla^4, interfacial stress and its heating: the fast-mode coefficient's sub-step count equals
+    the reference's, and h, u, theta and Fm after 1 and 12 steps equal the reference's to 1e-12 relative (the branch
+    calls pow, whose last bit may differ between the host's libm and CUDA's)."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('airtheta_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    core = layers.Layers(dg, 3, b=z['b'], gprime=[0.0, 0.0], stress=list(z['stress']), nu4=float(z['nu4']),
+                         floor=float(z['floor']), vmix=float(z['vmix']),
+                         air=dict(t_ref=288.0, cp=float(z['cp']), kappa=float(z['kappa']), rd=float(z['rd'])))
+    h, u, theta = T(z['h0'], dev), T(z['u0'], dev), T(z['theta0'], dev)
+    Fm = torch.zeros_like(u)
+    dt, nfast = float(z['dt']), int(z['nfast'])
+    core.update_gfast(h, theta)
+    assert core.substeps(h, dt) == int(z['substeps'])
+    worst = 0.0
+    for s in range(1, 13):
+        core.step(h, u, dt, nfast, Fm, theta=theta)
+        if s in (1, 12):
+            torch.cuda.synchronize()
+            sfx = '1' if s == 1 else ''
+            for name, x in (('h', h), ('u', u), ('theta', theta), ('Fm', Fm)):
+                e = rel(x.cpu().numpy(), z[name + sfx])
+                worst = max(worst, e)
+                assert e <= REL, (s, name, e)
+    with pytest.raises(ValueError):
+        core.step(h, u, dt, nfast, Fm)                      # air layers need theta
