@@ -13,6 +13,7 @@
  *   isw_layers_step            src/insilica/layers.py:185-212 Layers.step(h, u, dt, nfast, Fm)
  *   isw_layers_step_air        the same with theta: the air branch (layers.py:134-136, 152-166, 187-192, 203-206)
  *   isw_layers_update_gfast    src/insilica/layers.py:104-109 Layers.update_gfast(h, theta)
+ *   isw_layers_exchange        src/insilica/layers.py:214-232 Layers.exchange(wx, h, u, M, psi, theta, seq)
  *   isw_layers_substeps        src/insilica/layers.py:99-102 Layers.substeps(h, dt)
  *   isw_layers_lap             src/insilica/layers.py:123-127 Layers._lap(u, out)   (used by lap_max, :111-121)
  *   isw_transport_create       src/insilica/transport.py:19-30 Transport(dg, layers, beta, tracers)
@@ -94,6 +95,7 @@ typedef struct isw_layers_params {
    * cp, kappa, rd the air's constants, p0 the reference pressure of theta (Pa). air = 0: Boussinesq layers. */
   int air;
   double cp, kappa, rd, p0;
+  double thin_wind;                       /* air: below this thickness the exchange gives a layer its neighbours' wind */
 } isw_layers_params;
 
 const char *isw_last_error(void);
@@ -109,6 +111,12 @@ int isw_layers_step(isw_layers *s, double *h, double *u, double *Fm, double dt, 
 /* One step of air layers (reference Layers.step(h, u, dt, nfast, Fm, theta), layers.py:185-206 with the air branch of
  * _stage, :134-136 and :152-166): theta (L x N) is read and, with the interfacial stress's heating, updated in place. */
 int isw_layers_step_air(isw_layers *s, double *h, double *u, double *Fm, double *theta, double dt, int nfast, void *stream);
+/* Between-step exchange (reference Layers.exchange, layers.py:214-232): thickness wx (L - 1 x N, positive upward across
+ * the interface below layer k) moves between layers with the tracer psi and momentum, conservatively; M (L x N) the
+ * layers' mass; theta (air layers, or NULL) takes the heat of the momentum mixing and of the last step's nabla^4 loss;
+ * seq != 0 moves the tracer in the order water passes through the column. FP64 form. */
+int isw_layers_exchange(isw_layers *s, const double *wx, double *h, double *u, double *M, double *psi, double *theta, int seq,
+                        void *stream);
 /* Air layers: the fast mode's coefficient per cell from the state (reference Layers.update_gfast, layers.py:104-109). */
 int isw_layers_update_gfast(isw_layers *s, const double *h, const double *theta, void *stream);
 /* max(1, ceil(dt sqrt(max_i Gc_i sum_k h_k) / (0.5 d_min))): synchronises `stream`. */

@@ -52,7 +52,8 @@ struct LayersDev {
   double *red;                               // reduction scratch (substeps)
   // air layers (h = mass per area, theta per layer): their constants and scratch
   int air;
-  double cpa, kap, rda, p0;
+  double cpa, kap, rda, p0, thin_wind;
+  double *hold;                              // the exchange hook's h before it (L x N)
   double *S, *pibar, *muf, *phi, *uf, *accL;
   // mixed-form scratch (allocated for ISW_MIXED only): FP32 stage winds and operators; the fast loop in deviation form
   // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)

@@ -13,6 +13,7 @@
 #include "handles.cuh"
 #include "layers_air.cuh"
 #include "layers_fp64.cuh"
+#include "layers_xch.cuh"
 
 namespace isw {
 namespace {
@@ -114,6 +115,20 @@ __global__ void __launch_bounds__(THREADS) k_air_d(const LayersDev M, const Stag
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < M.g.N) fp64::h_cell<L>(M, a, t);
   else if (t < M.g.N + M.g.E) fp64::air_u_edge<L>(M, a, t - M.g.N);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_xch_cell(const LayersDev M, const double *__restrict__ wx, double *h, double *Mm,
+                                                      double *psi, int seq) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::xch_cell<L>(M, wx, h, Mm, psi, seq, t);
+}
+
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_xch_edge(const LayersDev M, const double *__restrict__ wx, double *u, double *diss,
+                                                      const double *lap4, double nu4dt, double hthin) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.E) fp64::xch_edge<L>(M, wx, M.hold, u, diss, lap4, nu4dt, hthin, t);
 }
 
 template <int L>
@@ -369,6 +384,8 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
     d.ub2 = dalloc(s, E);
     d.cw = dalloc(s, (size_t)N * 6);
+    d.hold = dalloc(s, (size_t)L * N);
+    d.thin_wind = p->thin_wind;
     if (p->air) {
       d.air = 1;
       d.cpa = p->cp; d.kap = p->kappa; d.rda = p->rd; d.p0 = p->p0;
@@ -438,6 +455,7 @@ void layers_step(isw_layers *s, double *h, double *u, double *Fm, double *theta,
   if (!(dt > 0) || !std::isfinite(dt)) fail(ISW_EINVAL, "layers.step: dt must be positive and finite");
   if (s->d.air && !theta) fail(ISW_EINVAL, "layers.step: air layers step with theta (isw_layers_step_air)");
   if (!s->d.air && theta) fail(ISW_EINVAL, "layers.step: theta is for air layers");
+  if (s->d.nu4 != 0) s->nu4dt = s->d.nu4 * dt;   // the step's nabla^4 loss, booked as heat by an air exchange
   if (s->d.precision == ISW_MIXED) {
     layers_step_mixed(s, h, u, Fm, dt, nfast, st);
     return;
@@ -478,6 +496,24 @@ void layers_step(isw_layers *s, double *h, double *u, double *Fm, double *theta,
     s->graphs.pop_back();
   }
   ISW_CUDA(cudaGraphLaunch(exec, st));
+}
+
+// The between-step exchange (reference layers.py:214-232): thickness, tracer and momentum between layers; for air
+// layers (theta given) the momentum mixing's kinetic-energy loss and the step's nabla^4 loss return as heat.
+void layers_exchange(isw_layers *s, const double *wx, double *h, double *u, double *Mm, double *psi, double *theta, int seq,
+                     cudaStream_t st) {
+  if (!wx || !h || !u || !Mm || !psi) fail(ISW_EINVAL, "layers.exchange: null array");
+  const LayersDev &M = s->d;
+  const int L = M.L, N = M.g.N, E = M.g.E;
+  if (L < 2) return;
+  const bool heat = M.air && theta;
+  const bool v4 = heat && M.nu4 != 0;
+  ISW_CUDA(cudaMemcpyAsync(M.hold, h, sizeof(double) * (size_t)L * N, cudaMemcpyDeviceToDevice, st));
+  ISW_DISPATCH_L(L, (k_xch_cell<LL><<<blocks_for(N), THREADS, 0, st>>>(M, wx, h, Mm, psi, seq ? 1 : 0)));
+  ISW_DISPATCH_L(L, (k_xch_edge<LL><<<blocks_for(E), THREADS, 0, st>>>(M, wx, u, heat ? M.diss : nullptr, v4 ? M.L2 : nullptr,
+                                                                       v4 ? s->nu4dt : 0.0, heat ? M.thin_wind : 0.0)));
+  if (heat) ISW_DISPATCH_L(L, (k_vmix_heat<LL><<<blocks_for(N), THREADS, 0, st>>>(M, h, theta)));
+  ISW_CUDA(cudaGetLastError());
 }
 
 void layers_update_gfast(isw_layers *s, const double *h, const double *theta, cudaStream_t st) {
@@ -555,6 +591,17 @@ int isw_layers_step_air(isw_layers *s, double *h, double *u, double *Fm, double 
     if (!theta) fail(ISW_EINVAL, "layers.step: null theta");
     ISW_CUDA(cudaSetDevice(s->grid->device));
     layers_step(s, h, u, Fm, theta, dt, nfast, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_exchange(isw_layers *s, const double *wx, double *h, double *u, double *M, double *psi, double *theta, int seq,
+                        void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.exchange: null handle");
+    if (s->d.precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers.exchange: the FP64 form only");
+    if (theta && !s->d.air) fail(ISW_EINVAL, "layers.exchange: theta is for air layers");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    layers_exchange(s, wx, h, u, M, psi, theta, seq, (cudaStream_t)stream);
   });
 }
 

@@ -30,7 +30,8 @@ class GridHost(ctypes.Structure):
 class LayersParams(ctypes.Structure):
     _fields_ = [('L', I), ('grav', D), ('gprime', P), ('drag', P), ('stress', P),
                 ('nu4', D), ('floor_', D), ('rotation', D), ('div_damp', D), ('thin', D), ('vmix', D), ('vmix_cd', D),
-                ('b', P), ('precision', I), ('air', I), ('cp', D), ('kappa', D), ('rd', D), ('p0', D)]
+                ('b', P), ('precision', I), ('air', I), ('cp', D), ('kappa', D), ('rd', D), ('p0', D),
+                ('thin_wind', D)]
 
 
 def _sig(name, res, args):
@@ -49,6 +50,7 @@ isw_layers_destroy = _sig('isw_layers_destroy', I, [P])
 isw_layers_step = _sig('isw_layers_step', I, [P, P, P, P, D, I, P])
 isw_layers_step_air = _sig('isw_layers_step_air', I, [P, P, P, P, P, D, I, P])
 isw_layers_update_gfast = _sig('isw_layers_update_gfast', I, [P, P, P, P])
+isw_layers_exchange = _sig('isw_layers_exchange', I, [P, P, P, P, P, P, P, I, P])
 isw_layers_substeps = _sig('isw_layers_substeps', I, [P, P, D, ctypes.POINTER(I), P])
 isw_layers_lap = _sig('isw_layers_lap', I, [P, P, P, P])
 isw_transport_create = _sig('isw_transport_create', I, [P, I, D, I, I, ctypes.POINTER(P)])

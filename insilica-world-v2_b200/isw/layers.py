@@ -35,14 +35,13 @@ class Layers:
             raise NotImplementedError('Layers: the shelf option is not implemented by this core')
         if shelf_bed:
             raise NotImplementedError('Layers: shelf_bed is not implemented by this core')
-        if thin_wind:
-            raise NotImplementedError('Layers: thin_wind (air exchange) is not implemented by this core')
         assert 1 <= layers <= LMAX and len(gprime) == layers - 1
         if not isinstance(dg, DeviceGrid):
             raise TypeError('Layers: dg must be an isw DeviceGrid')
         self.dg, self.L = dg, layers
         self.grav, self.nu4, self.floor, self.div_damp, self.thin = grav, nu4, floor, div_damp, thin
         self.vmix, self.vmix_cd = vmix, vmix_cd
+        self.thin_wind = thin_wind
         self.air = air
         # the air's constants (reference layers.py:64-65: cp 1004.6, kappa, R 287.04 unless the air dict gives them)
         self.cpa, self.kap, self.rda = (air or {}).get('cp', CP_DRY), (air or {}).get('kappa', KAPPA), (air or {}).get('rd', R_DRY)
@@ -63,7 +62,8 @@ class Layers:
                               stress=_lib.host_ptr(self._stress), nu4=float(nu4), floor_=float(floor), rotation=float(rotation),
                               div_damp=float(div_damp), thin=float(thin), vmix=float(vmix), vmix_cd=float(vmix_cd),
                               b=_lib.host_ptr(self._b_host), precision=self.precision, air=1 if air else 0,
-                              cp=float(self.cpa), kappa=float(self.kap), rd=float(self.rda), p0=P0)
+                              cp=float(self.cpa), kappa=float(self.kap), rd=float(self.rda), p0=P0,
+                              thin_wind=float(thin_wind))
         h = ctypes.c_void_p()
         _lib.check(_lib.isw_layers_create(dg.handle, ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -136,8 +136,21 @@ class Layers:
             _lib.check(_lib.isw_layers_update_gfast(self._h, device_ptr(h, shape=sh, name='h', device=dev),
                                                     device_ptr(theta, shape=sh, name='theta', device=dev), stream_of(dev, stream)))
 
-    def exchange(self, wx, h, u, M, psi, theta=None, seq=False):
-        raise NotImplementedError('Layers.exchange: the between-layer exchange hook is not implemented by this core')
+    def exchange(self, wx, h, u, M, psi, theta=None, seq=False, stream=None):
+        """Move thickness wx (L-1, N; positive upward across the interface below layer k) between layers with its tracer
+        psi and momentum, conservatively (reference layers.py:214-232); M (L, N) the layers' mass. For air layers with
+        theta given, the kinetic energy the momentum mixing removed (and the last step's nabla^4 loss) warms the column
+        and a nearly empty layer takes its neighbours' wind (thin_wind). seq: the tracer moves in the order water passes
+        through the column. The caller keeps donors above the floor."""
+        sh, su = self._shapes()
+        dev = self.dg.device
+        if self.L < 2:
+            return
+        pt = device_ptr(theta, shape=sh, name='theta', device=dev) if theta is not None else None
+        _lib.check(_lib.isw_layers_exchange(self._h, device_ptr(wx, shape=(self.L - 1, self.dg.N), name='wx', device=dev),
+                                            device_ptr(h, shape=sh, name='h', device=dev), device_ptr(u, shape=su, name='u', device=dev),
+                                            device_ptr(M, shape=sh, name='M', device=dev), device_ptr(psi, shape=sh, name='psi', device=dev),
+                                            pt, 1 if seq else 0, stream_of(dev, stream)))
 
     def energy(self, h, u, theta=None):
         """Total energy per unit density (J/rho0; reference layers.py:234-253), on the host. Air layers: kinetic plus

@@ -17,6 +17,8 @@ Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
 - dsum.npz       deterministic tree sums of fixed inputs
 - airtheta_n4.npz the reference's air layers (h = mass per area, theta per layer; layers.py air branch) from its own
                  aquaplanet start (cases.aqua), surface drag, nabla^4, interfacial stress with its heating: 12 steps
+- exchange_n4.npz the between-step exchange hook (Layers.exchange): Boussinesq layers after one step, seeded thickness
+                 moves, plain and sequential; air layers after one step, with heating and the thin layers' wind
 
 `--only NAME` writes one fixture (e.g. `--only airtheta`).
 """
@@ -79,6 +81,9 @@ def main():
     dg = DeviceGrid(g)
     if a.only == 'airtheta':
         save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
+        return
+    if a.only == 'exchange':
+        save('exchange_n4.npz', exchange(cp, g, dg, Layers, rcases, mycases))
         return
     save('grid_n4.npz', {k: getattr(base, k) for k in GRID_KEYS})
 
@@ -182,6 +187,52 @@ def main():
         d[f'xy_{n}'] = dsum(cp.asarray(x), cp.asarray(y))
     save('dsum.npz', d)
     save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
+    save('exchange_n4.npz', exchange(cp, g, dg, Layers, rcases, mycases))
+
+
+def exchange(cp, g, dg, Layers, rcases, mycases):
+    """Layers.exchange after one step: (1) the three-layer Boussinesq stack with seeded moves wx ~ U(-20, 20) m, plain
+    and sequential, the demo tracer and masses; (2) the reference's air layers (aqua start, nabla^4, thin_wind 100 kg/m^2,
+    one layer pressed near its floor in a band of cells) with wx ~ U(-300, 300) kg/m^2, heating theta."""
+    rng = np.random.default_rng(11)
+    out = {}
+    s = mycases.stack_state(g, 'air', 7)
+    core = Layers(dg, 3, b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'], vmix=s['vmix'])
+    h, u = cp.asarray(s['h']), cp.asarray(s['u'])
+    core.step(h, u, mycases.stack_dt(4), 20)
+    wx = rng.uniform(-20.0, 20.0, (2, g.N))
+    psi0 = rng.uniform(0.0, 1.0, (3, g.N))
+    out.update(b_h0=s['h'], b_u0=s['u'], b_b=s['b'], b_gprime=np.array(s['gprime']), b_stress=np.array(s['stress']),
+               b_nu4=s['nu4'], b_floor=s['floor'], b_vmix=s['vmix'], b_dt=mycases.stack_dt(4), b_wx=wx, b_psi0=psi0)
+    for seq in (False, True):
+        hh, uu = h.copy(), u.copy()
+        M = hh * cp.asarray(g.areaCell)[None]
+        psi = cp.asarray(psi0)
+        core.exchange(cp.asarray(wx), hh, uu, M, psi, seq=seq)
+        tag = 'seq' if seq else 'plain'
+        out.update({f'b_{tag}_h': hh.get(), f'b_{tag}_u': uu.get(), f'b_{tag}_M': M.get(), f'b_{tag}_psi': psi.get()})
+    h0, b, u0, x = rcases.aqua(g)
+    h0 = h0.copy()
+    band = np.abs(g.lat - 0.3) < 0.1
+    h0[2, band] = 60.0                                         # a nearly empty bottom layer in a band (thin_wind acts)
+    theta0 = x['theta']
+    nu4 = mycases.visc4(g, 15.0)
+    core = Layers(dg, 3, b=b, gprime=[0.0, 0.0], stress=[0.0, 0.0, rcases.SURFACE_DRAG], nu4=nu4, floor=10.0,
+                  air=dict(t_ref=288.0), thin_wind=100.0)
+    h, u, theta = cp.asarray(h0), cp.asarray(u0), cp.asarray(theta0)
+    core.update_gfast(h, theta)
+    nfast = int(math.ceil(1.2 * core.substeps(h, 1800.0)))
+    core.step(h, u, 1800.0, nfast, theta=theta)
+    wx = rng.uniform(-300.0, 300.0, (2, g.N))
+    wx[1, band] = np.minimum(wx[1, band], 0.0)                # nothing taken from the emptied layer
+    psi0 = rng.uniform(0.0, 1.0, (3, g.N))
+    out.update(a_h0=h0, a_u0=u0, a_theta0=theta0, a_nu4=nu4, a_nfast=nfast, a_wx=wx, a_psi0=psi0,
+               a_cp=core.cpa, a_kappa=core.kap, a_rd=core.rda, a_drag=rcases.SURFACE_DRAG)
+    M = h * cp.asarray(g.areaCell)[None]
+    psi = cp.asarray(psi0)
+    core.exchange(cp.asarray(wx), h, u, M, psi, theta=theta)
+    out.update(a_h=h.get(), a_u=u.get(), a_M=M.get(), a_psi=psi.get(), a_theta=theta.get())
+    return out
 
 
 def air_theta(cp, g, dg, Layers, rcases, mycases):

@@ -272,3 +272,41 @@ def test_air_layers_golden(dev, isw, grid4):
                 assert e <= REL, (s, name, e)
     with pytest.raises(ValueError):
         core.step(h, u, dt, nfast, Fm)                      # air layers need theta
+
+
+def test_exchange_golden(dev, isw, grid4):
+    """The between-step exchange hook (Layers.exchange) after one step, against the reference's own: Boussinesq layers
+    with seeded thickness moves, plain and sequential (h, u, M and the tracer); air layers with the momentum mixing's
+    heat, the step's nabla^4 loss and a nearly empty layer taking its neighbours' wind (h, u, M, tracer, theta). To
+    1e-12 relative (the steps before call exp and pow)."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('exchange_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    A = T(dg.host.areaCell, dev)
+    core = layers.Layers(dg, 3, b=z['b_b'], gprime=list(z['b_gprime']), stress=list(z['b_stress']), nu4=float(z['b_nu4']),
+                         floor=float(z['b_floor']), vmix=float(z['b_vmix']))
+    h0, u0 = T(z['b_h0'], dev), T(z['b_u0'], dev)
+    core.step(h0, u0, float(z['b_dt']), 20)
+    for tag, seq in (('plain', False), ('seq', True)):
+        h, u = h0.clone(), u0.clone()
+        M = (h * A[None]).contiguous()
+        psi = T(z['b_psi0'], dev)
+        core.exchange(T(z['b_wx'], dev), h, u, M, psi, seq=seq)
+        torch.cuda.synchronize()
+        for name, x in (('h', h), ('u', u), ('M', M), ('psi', psi)):
+            e = rel(x.cpu().numpy(), z[f'b_{tag}_{name}'])
+            assert e <= REL, (tag, name, e)
+    core = layers.Layers(dg, 3, b=np.zeros(dg.N), gprime=[0.0, 0.0], stress=[0.0, 0.0, float(z['a_drag'])],
+                         nu4=float(z['a_nu4']), floor=10.0, thin_wind=100.0,
+                         air=dict(t_ref=288.0, cp=float(z['a_cp']), kappa=float(z['a_kappa']), rd=float(z['a_rd'])))
+    h, u, theta = T(z['a_h0'], dev), T(z['a_u0'], dev), T(z['a_theta0'], dev)
+    core.update_gfast(h, theta)
+    core.step(h, u, 1800.0, int(z['a_nfast']), theta=theta)
+    M = (h * A[None]).contiguous()
+    psi = T(z['a_psi0'], dev)
+    core.exchange(T(z['a_wx'], dev), h, u, M, psi, theta=theta)
+    torch.cuda.synchronize()
+    for name, x in (('h', h), ('u', u), ('M', M), ('psi', psi), ('theta', theta)):
+        e = rel(x.cpu().numpy(), z[f'a_{name}'])
+        assert e <= REL, ('air', name, e)
