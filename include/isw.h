@@ -96,7 +96,22 @@ typedef struct isw_layers_params {
   int air;
   double cp, kappa, rd, p0;
   double thin_wind;                       /* air: below this thickness the exchange gives a layer its neighbours' wind */
+  /* option branches of Boussinesq layers (reference layers.py:36-40): wall (E host values, 0 = a closed edge, or NULL),
+   * shelf (a layer squeezed below it takes the thinner cell's thickness at an edge and fades its pressure force; 0 off),
+   * shelf_bed != 0: only layers resting on the sea floor count as squeezed. FP64 form. */
+  const double *wall;
+  double shelf;
+  int shelf_bed;
 } isw_layers_params;
+
+/* Per-step fields of the option branches (reference attributes Layers.sig / .zm, .tide, .cbot, .cd_bot set by the ocean
+ * and the tides): array is a device array the caller keeps filled (borrowed until replaced or cleared with NULL).
+ *   ISW_OPT_SIG     L x N buoyancy sigma_k = g (rho_k - rho_0) / rho_0 per cell (the layers' mid-heights zm are kept
+ *                   by the core); replaces the fixed g'
+ *   ISW_OPT_TIDE    N tide-generating potential (m^2/s^2)
+ *   ISW_OPT_CBOT    E internal-tide drag of the bottom layer (m/s per edge)
+ *   ISW_OPT_CD_BOT  value: the bottom layer's quadratic drag coefficient (array unused) */
+enum { ISW_OPT_SIG = 1, ISW_OPT_TIDE = 2, ISW_OPT_CBOT = 3, ISW_OPT_CD_BOT = 4 };
 
 const char *isw_last_error(void);
 int isw_version(void);
@@ -117,6 +132,9 @@ int isw_layers_step_air(isw_layers *s, double *h, double *u, double *Fm, double 
  * seq != 0 moves the tracer in the order water passes through the column. FP64 form. */
 int isw_layers_exchange(isw_layers *s, const double *wx, double *h, double *u, double *M, double *psi, double *theta, int seq,
                         void *stream);
+/* Set one per-step field of the option branches (ISW_OPT_*); cached step graphs are dropped. Set options before adding
+ * the Layers to a batch (a batch reads them when its stacks change). FP64 form. */
+int isw_layers_set_option(isw_layers *s, int option, const double *array, double value);
 /* Air layers: the fast mode's coefficient per cell from the state (reference Layers.update_gfast, layers.py:104-109). */
 int isw_layers_update_gfast(isw_layers *s, const double *h, const double *theta, void *stream);
 /* max(1, ceil(dt sqrt(max_i Gc_i sum_k h_k) / (0.5 d_min))): synchronises `stream`. */

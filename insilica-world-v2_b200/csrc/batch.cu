@@ -796,6 +796,7 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     if (!b || !layers || !h || !u || !Fm || !slot) fail(ISW_EINVAL, "batch.add: null argument");
     if (layers->grid->device != b->device) fail(ISW_EINVAL, "batch.add: the stack is on another device");
     if (layers->d.air) fail(ISW_EUNSUPPORTED, "batch.add: air layers step call by call (isw_layers_step_air)");
+    if (layers->d.wall || layers->d.ob) fail(ISW_EUNSUPPORTED, "batch.add: walls and the shelf bed step call by call");
     if (!(dt > 0) || !std::isfinite(dt) || nfast < 1) fail(ISW_EINVAL, "batch.add: dt must be positive and nfast >= 1");
     if (tr) {
       if (!M || !M1 || !tracers) fail(ISW_EINVAL, "batch.add: transport needs M, M1 and the tracers");

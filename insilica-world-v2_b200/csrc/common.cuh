@@ -54,6 +54,12 @@ struct LayersDev {
   int air;
   double cpa, kap, rda, p0, thin_wind;
   double *hold;                              // the exchange hook's h before it (L x N)
+  // option branches (reference layers.py:36-90; null / 0 when off): thin walls (E mask, 0 = closed), the squeezed-layer
+  // shelf and its bed flags ob (L x N), per-cell buoyancy sig with the layers' mid-heights zm (L x N), the tide potential
+  // (N), the bottom layer's quadratic drag cd_bot and the internal tide's drag cbot (E)
+  double shelf, cd_bot;
+  const double *wall, *sig, *tide, *cbot;
+  double *zm, *ob;
   double *S, *pibar, *muf, *phi, *uf, *accL;
   // mixed-form scratch (allocated for ISW_MIXED only): FP32 stage winds and operators; the fast loop in deviation form
   // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)

@@ -118,6 +118,12 @@ __global__ void __launch_bounds__(THREADS) k_air_d(const LayersDev M, const Stag
 }
 
 template <int L>
+__global__ void __launch_bounds__(THREADS) k_onbed(const LayersDev M, const double *__restrict__ h) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < M.g.N) fp64::onbed_cell<L>(M, h, t);
+}
+
+template <int L>
 __global__ void __launch_bounds__(THREADS) k_xch_cell(const LayersDev M, const double *__restrict__ wx, double *h, double *Mm,
                                                       double *psi, int seq) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -245,6 +251,7 @@ void enqueue_step(isw_layers *s, double *h, double *u, double *Fm, double dt, in
   const GridDev &g = M.g;
   const int L = M.L;
   const int N = g.N, E = g.E, NV = g.NV;
+  if (M.ob) ISW_DISPATCH_L(L, (k_onbed<LL><<<blocks_for(N), THREADS, 0, st>>>(M, h)));
   ISW_DISPATCH_L(L, (k_init<LL><<<blocks_for(N + E), THREADS, 0, st>>>(M, h, u)));
   if (M.nu4 != 0) {
     ISW_DISPATCH_L(L, (k_lap_cv<LL><<<blocks_for(N + NV), THREADS, 0, st>>>(M, u)));
@@ -340,6 +347,10 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
   if (p->precision != ISW_FP64 && p->precision != ISW_MIXED) fail(ISW_EINVAL, "layers: precision must be ISW_FP64 or ISW_MIXED");
   if (p->air && p->precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers: air layers run in the FP64 form only");
   if (p->air && !(p->cp > 0 && p->kappa > 0 && p->rd > 0 && p->p0 > 0)) fail(ISW_EINVAL, "layers: air constants must be positive");
+  if ((p->wall || p->shelf != 0 || p->shelf_bed) && p->precision != ISW_FP64)
+    fail(ISW_EUNSUPPORTED, "layers: walls and the shelf run in the FP64 form only");
+  if (p->wall && p->air) fail(ISW_EINVAL, "layers: walls are for Boussinesq layers");
+  if (!(p->shelf >= 0)) fail(ISW_EINVAL, "layers: shelf must be >= 0");
   ISW_CUDA(cudaSetDevice(g->device));
   isw_layers *s = new isw_layers();
   s->grid = g;
@@ -386,6 +397,13 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.cw = dalloc(s, (size_t)N * 6);
     d.hold = dalloc(s, (size_t)L * N);
     d.thin_wind = p->thin_wind;
+    if (p->wall) {
+      double *w = dalloc(s, E);
+      ISW_CUDA(cudaMemcpy(w, p->wall, sizeof(double) * E, cudaMemcpyHostToDevice));
+      d.wall = w;
+    }
+    d.shelf = p->shelf;
+    if (p->shelf_bed && p->shelf > 0) d.ob = dalloc(s, (size_t)L * N);
     if (p->air) {
       d.air = 1;
       d.cpa = p->cp; d.kap = p->kappa; d.rda = p->rd; d.p0 = p->p0;
@@ -602,6 +620,31 @@ int isw_layers_exchange(isw_layers *s, const double *wx, double *h, double *u, d
     if (theta && !s->d.air) fail(ISW_EINVAL, "layers.exchange: theta is for air layers");
     ISW_CUDA(cudaSetDevice(s->grid->device));
     layers_exchange(s, wx, h, u, M, psi, theta, seq, (cudaStream_t)stream);
+  });
+}
+
+int isw_layers_set_option(isw_layers *s, int option, const double *array, double value) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.set_option: null handle");
+    if (s->d.precision != ISW_FP64) fail(ISW_EUNSUPPORTED, "layers.set_option: the FP64 form only");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    LayersDev &d = s->d;
+    switch (option) {
+      case ISW_OPT_SIG:
+        if (array && d.air) fail(ISW_EINVAL, "layers.set_option: per-cell buoyancy is for Boussinesq layers");
+        if (array && !d.zm) d.zm = dalloc(s, (size_t)d.L * d.g.N);
+        d.sig = array;
+        break;
+      case ISW_OPT_TIDE: d.tide = array; break;
+      case ISW_OPT_CBOT: d.cbot = array; break;
+      case ISW_OPT_CD_BOT:
+        if (!(value >= 0)) fail(ISW_EINVAL, "layers.set_option: cd_bot must be >= 0");
+        d.cd_bot = value;
+        break;
+      default: fail(ISW_EINVAL, "layers.set_option: unknown option");
+    }
+    for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);   // the step graphs hold the old descriptor
+    s->graphs.clear();
   });
 }
 

@@ -24,6 +24,37 @@ namespace fp64 {
 
 __device__ __forceinline__ double edge_h(double a, double b) { return 0.5 * (a + b); }
 
+// A layer's thickness at an edge with the shelf option (reference layers.cu:41-45, 59-61): the mean of its two cells,
+// or the thinner where the shelf has squeezed one side below `shelf` (only layers flagged on the bed when ob is kept).
+__device__ __forceinline__ double shelf_at(const LayersDev &M, int k, int i, int j) {
+  const int N = M.g.N;
+  return !M.ob || M.ob[(size_t)k * N + i] > 0 || M.ob[(size_t)k * N + j] > 0 ? M.shelf : 0.0;
+}
+
+__device__ __forceinline__ double edge_hk(const LayersDev &M, int k, int i, int j, double a, double b) {
+  if (M.shelf > 0) {
+    const double sh = shelf_at(M, k, i, j);
+    const double m = a < b ? a : b;
+    if (sh > 0 && m < sh) return m;
+  }
+  return 0.5 * (a + b);
+}
+
+__device__ __forceinline__ bool walled(const LayersDev &M, int e) { return M.wall && M.wall[e] == 0; }
+
+// the squeezed-layer flags ob (reference lay_onbed, layers.cu:51-58)
+template <int L>
+__device__ __forceinline__ void onbed_cell(const LayersDev &M, const double *__restrict__ h, int i) {
+  const int N = M.g.N;
+  double below = 0;
+#pragma unroll
+  for (int k = L - 1; k >= 0; k--) {
+    const bool stack = k + 1 < L && h[(size_t)k * N + i] < 2 * M.floor_ && h[(size_t)(k + 1) * N + i] < 2 * M.floor_;
+    M.ob[(size_t)k * N + i] = below <= (L - 1 - k) * 2 * M.floor_ || stack ? 1.0 : 0.0;
+    below += h[(size_t)k * N + i];
+  }
+}
+
 // ---- init ----
 template <int L>
 __device__ __forceinline__ void eta0_cell(const LayersDev &M, const double *__restrict__ h, int i) {
@@ -41,11 +72,11 @@ __device__ __forceinline__ void ubar0_edge(const LayersDev &M, const double *__r
   double H = 0, U = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    const double he = edge_h(h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    const double he = edge_hk(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
     H += he;
     U += he * u[(size_t)k * E + e];
   }
-  M.ub0[e] = U / H;
+  M.ub0[e] = walled(M, e) ? 0.0 : U / H;
 }
 
 // ---- vector Laplacian ----
@@ -125,10 +156,17 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
     c[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
   }
   const double A = g.areaCell[i];
-  double Mp = 0;
+  double Mp = 0, P = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    if (k > 0) Mp += M.gp[k - 1] * z[k];
+    if (M.sig) {                   // per-cell buoyancy (reference layers.cu:90-95): M_k = P_k + sigma_k z_k
+      const double sk = M.sig[(size_t)k * N + i], hk = h[(size_t)k * N + i];
+      Mp = P + sk * z[k];
+      P += sk * hk;
+      M.zm[(size_t)k * N + i] = z[k] - 0.5 * hk;
+    } else if (k > 0) {
+      Mp += M.gp[k - 1] * z[k];
+    }
     const double *ul = u + (size_t)k * E;
     double ke = 0;
 #pragma unroll
@@ -137,7 +175,9 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
         const double ue = ul[es[t]];
         ke += c[t] * ue * ue;
       }
-    M.B[(size_t)k * N + i] = Mp + ke / A;
+    double Bk = Mp + ke / A;
+    if (M.tide) Bk -= M.tide[i];   // the tide-generating potential (reference layers.cu:106)
+    M.B[(size_t)k * N + i] = Bk;
   }
   M.eta[i] = M.eta0[i];
 }
@@ -181,7 +221,7 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const size_t o = (size_t)k * E + e;
-    const double hv = edge_h(h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    const double hv = edge_hk(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
     const double qv = 0.5 * (M.q[(size_t)k * NV + v1] + M.q[(size_t)k * NV + v2]);
     M.hedge[o] = hv;
     pp[k * 3 + 0] = hv;
@@ -229,16 +269,30 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
   }
   const int a = g.eI[e], b = g.eJ[e];
   const double de = g.de[e];
-  double T[L];
+  double T[L], sqk[L];
   double H = 0, U = 0, GT = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const double ue = u[(size_t)k * E + e];
     const double *Bl = M.B + (size_t)k * N;
-    // shelf off: sq = 1, so the force is -(B_J - B_I) / d and the squeezed-layer drag term is (1 - 1) / 21600 = 0
-    const double sq = 1.0;
+    // a layer squeezed by the shelf fades its pressure force and takes a day's drag (reference layers.cu:293-297);
+    // shelf off: sq = 1, the force is -(B_J - B_I) / d and the drag term (1 - 1) / 21600 = 0
+    const double shk = M.shelf > 0 ? shelf_at(M, k, a, b) : 0.0;
+    const double sq0 = shk > 0 && he[k] < shk ? (he[k] - 2 * M.floor_ > 0 ? (he[k] - 2 * M.floor_) / (shk - 2 * M.floor_) : 0.0) : 1.0;
+    const double sq = theta ? 1.0 : sq0;
+    sqk[k] = sq0;
     double d = Q[k] - (sq * (Bl[b] - Bl[a])) / de - (M.drag[k] + (1 - sq) / 21600.0) * ue;
-    const double ck = M.stress[k];
+    double ck = M.stress[k];
+    if (k == L - 1 && (M.cd_bot > 0 || M.cbot)) {
+      // the bottom layer's quadratic stress cd |u| (|u| from the normal and the TRiSK tangential wind) and the internal
+      // tide's drag (reference layers.cu:303-311)
+      if (M.cd_bot > 0) {
+        double vt = 0;
+        for (int t = 0; t < cnt; t++) vt += g.w[m0 + t] * M.pk[((size_t)ix[t] * L + k) * 3 + 1];
+        ck += M.cd_bot * sqrt(ue * ue + vt * vt);
+      }
+      if (M.cbot) ck += M.cbot[e];
+    }
     if (ck != 0) {
       const double r = ck / (he[k] > M.floor_ ? he[k] : M.floor_);
       d = d - ((r * dts > 1e-8) ? (1 - exp(-r * dts)) / dts : r) * ue;
@@ -248,10 +302,31 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
       const double *pl = M.pibar + (size_t)k * N;
       d = d + (0.5 * (pl[a] + pl[b]) * (tl[b] - tl[a])) / de;
     }
+    if (M.sig) {                   // per-cell buoyancy: + zm grad(sigma) (reference layers.cu:327-331)
+      const double *sl = M.sig + (size_t)k * N;
+      const double *zl = M.zm + (size_t)k * N;
+      d = d + sq * ((0.5 * (zl[a] + zl[b]) * (sl[b] - sl[a])) / de);
+    }
     if (M.nu4 != 0) d = d - M.nu4 * M.L2[(size_t)k * E + e];
     T[k] = d;
     H += he[k];
     U += he[k] * ue;
+  }
+  if (theta && M.shelf > 0) {      // air squeezed against the ground takes its neighbours' tendency (layers.cu:341-355)
+    double Tn[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      Tn[k] = T[k];
+      if (sqk[k] >= 1) continue;
+      double w = 0, s = 0;
+      for (int j = k - 1; j >= 0; j--)
+        if (sqk[j] >= 1) { w += he[j]; s += he[j] * T[j]; break; }
+      for (int j = k + 1; j < L; j++)
+        if (sqk[j] >= 1) { w += he[j]; s += he[j] * T[j]; break; }
+      if (w > 0) Tn[k] = sqk[k] * T[k] + (1 - sqk[k]) * s / w;
+    }
+#pragma unroll
+    for (int k = 0; k < L; k++) T[k] = Tn[k];
   }
 #pragma unroll
   for (int k = 0; k < L; k++) GT += he[k] * T[k];
@@ -289,6 +364,10 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, double tau, int e)
   const double ej = M.Gc[j] * (M.eta[j] + gam * (M.eta[j] - M.eta_prev[j]));
   const double ei = M.Gc[i] * (M.eta[i] + gam * (M.eta[i] - M.eta_prev[i]));
   M.ub[e] = v + tau * ((-(ej - ei)) / g.de[e] + M.G[e]);
+  if (walled(M, e)) {              // walls (reference layers.py:173-174)
+    M.ub[e] = 0.0;
+    M.acc[e] = 0.0;
+  }
 }
 
 
@@ -353,8 +432,8 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &
     const double ubs = M.ubs[e], acc = M.acc[e], le = g.le[e];
 #pragma unroll
     for (int k = 0; k < L; k++) {
-      const double he = edge_h(a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
-      const double F = he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
+      const double he = edge_hk(M, k, ea, eb, a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
+      const double F = walled(M, e) ? 0.0 : he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
       if (mine) M.F[(size_t)k * E + e] = F;
       const double f = F * le * a.cdt;
       if (mine) { if (f > 0) out[k] += f; }
@@ -414,7 +493,7 @@ __device__ __forceinline__ void u_edge(const LayersDev &M, const StageArgs &a, i
   for (int k = 0; k < L; k++) {
     const size_t o = (size_t)k * E + e;
     if (a.Fm) a.Fm[o] = limited(M, k, e) * le * a.dt;
-    a.un[o] = a.u0[o] + a.cdt * M.Tp[o] + dub;
+    a.un[o] = walled(M, e) ? 0.0 : a.u0[o] + a.cdt * M.Tp[o] + dub;
   }
 }
 
@@ -441,6 +520,8 @@ __device__ __forceinline__ void vmix_edge(const LayersDev &M, const double *__re
     d += 0.5 * ha * hb / (ha + hb) * (du0 * du0 - du1 * du1);
   }
   M.diss[e] = d;
+  if (walled(M, e))
+    for (int k = 0; k < L; k++) u[(size_t)k * E + e] = 0.0;
 }
 
 }  // namespace fp64

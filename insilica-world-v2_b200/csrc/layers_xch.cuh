@@ -129,6 +129,8 @@ __device__ __forceinline__ void xch_edge(const LayersDev &M, const double *__res
     k1 += hn[k] * un[k] * un[k];
   }
   if (diss) diss[e] = 0.5 * (k0 - k1) + nu4dt * v4;
+  if (M.wall && M.wall[e] == 0)    // walls: the exchange's wind masked after it (reference layers.py:226)
+    for (int k = 0; k < L; k++) u[(size_t)k * E + e] = 0.0;
 }
 
 }  // namespace fp64

@@ -31,7 +31,7 @@ class LayersParams(ctypes.Structure):
     _fields_ = [('L', I), ('grav', D), ('gprime', P), ('drag', P), ('stress', P),
                 ('nu4', D), ('floor_', D), ('rotation', D), ('div_damp', D), ('thin', D), ('vmix', D), ('vmix_cd', D),
                 ('b', P), ('precision', I), ('air', I), ('cp', D), ('kappa', D), ('rd', D), ('p0', D),
-                ('thin_wind', D)]
+                ('thin_wind', D), ('wall', P), ('shelf', D), ('shelf_bed', I)]
 
 
 def _sig(name, res, args):
@@ -51,6 +51,8 @@ isw_layers_step = _sig('isw_layers_step', I, [P, P, P, P, D, I, P])
 isw_layers_step_air = _sig('isw_layers_step_air', I, [P, P, P, P, P, D, I, P])
 isw_layers_update_gfast = _sig('isw_layers_update_gfast', I, [P, P, P, P])
 isw_layers_exchange = _sig('isw_layers_exchange', I, [P, P, P, P, P, P, P, I, P])
+isw_layers_set_option = _sig('isw_layers_set_option', I, [P, I, P, D])
+ISW_OPT_SIG, ISW_OPT_TIDE, ISW_OPT_CBOT, ISW_OPT_CD_BOT = 1, 2, 3, 4
 isw_layers_substeps = _sig('isw_layers_substeps', I, [P, P, D, ctypes.POINTER(I), P])
 isw_layers_lap = _sig('isw_layers_lap', I, [P, P, P, P])
 isw_transport_create = _sig('isw_transport_create', I, [P, I, D, I, I, ctypes.POINTER(P)])

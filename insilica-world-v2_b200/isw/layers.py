@@ -4,8 +4,9 @@
 meanings; the arrays are the caller's device arrays (h (L, N), u (L, E), Fm (L, E), FP64), updated in place on the
 current CUDA stream. Air layers (``air=dict(cp=, kappa=, rd=)``: h is mass per area, ``step`` and ``update_gfast`` take
 the layers' potential temperature theta, updated in place by the interfacial stress's heating) run in the FP64 form.
-Options of the reference that this core does not implement raise ``NotImplementedError`` at construction (walls, the
-shelf, the squeezed-layer bed, per-cell buoyancy, tides, the bottom drag law) or at the call (``exchange``).
+The option branches of Boussinesq layers are built in the FP64 form: thin walls (``wall``), the shelf and its bed flags
+(``shelf``, ``shelf_bed``), and the per-step fields the ocean and the tides set as attributes (``sig`` with ``zm``,
+``tide``, ``cd_bot``, ``cbot``). Air layers or options in the mixed form raise ``NotImplementedError``.
 """
 import ctypes
 import math
@@ -29,12 +30,9 @@ class Layers:
     def __init__(self, dg, layers=1, b=None, grav=GRAV, gprime=(), drag=0.0, stress=0.0, nu4=0.0, floor=1.0, rotation=1.0,
                  div_damp=DIV_DAMP, air=None, vmix=0.0, thin=2.0, wall=None, thin_wind=0.0, shelf=0.0, vmix_cd=0.0,
                  shelf_bed=False):
-        if wall is not None:
-            raise NotImplementedError('Layers: thin walls are not implemented by this core')
-        if shelf:
-            raise NotImplementedError('Layers: the shelf option is not implemented by this core')
-        if shelf_bed:
-            raise NotImplementedError('Layers: shelf_bed is not implemented by this core')
+        if (wall is not None or shelf or shelf_bed) and dg.mixed:
+            raise NotImplementedError('Layers: walls and the shelf run in the FP64 form only')
+        assert wall is None or not air, 'walls are for Boussinesq layers'
         assert 1 <= layers <= LMAX and len(gprime) == layers - 1
         if not isinstance(dg, DeviceGrid):
             raise TypeError('Layers: dg must be an isw DeviceGrid')
@@ -47,9 +45,12 @@ class Layers:
         self.cpa, self.kap, self.rda = (air or {}).get('cp', CP_DRY), (air or {}).get('kappa', KAPPA), (air or {}).get('rd', R_DRY)
         if air and dg.mixed:
             raise NotImplementedError('Layers: air layers run in the FP64 form only')
-        self.shelf = 0.0
-        self.sig = self.zm = self.tide = None
-        self.cd_bot, self.cbot = 0.0, None
+        self.shelf = float(shelf)
+        self._wall = None if wall is None else np.ascontiguousarray(np.asarray(
+            wall.detach().cpu().numpy() if isinstance(wall, torch.Tensor) else wall, dtype=np.float64).reshape(-1))
+        self.wall = None if wall is None else torch.as_tensor(self._wall, device=f'cuda:{dg.device}')
+        self._opts = dict(sig=None, tide=None, cbot=None, cd_bot=0.0)
+        self._zm = None
         self.precision = _lib.ISW_MIXED if dg.mixed else _lib.ISW_FP64
         self._b_host = np.zeros(dg.N) if b is None else np.ascontiguousarray(np.asarray(
             b.detach().cpu().numpy() if isinstance(b, torch.Tensor) else b, dtype=np.float64))
@@ -63,7 +64,8 @@ class Layers:
                               div_damp=float(div_damp), thin=float(thin), vmix=float(vmix), vmix_cd=float(vmix_cd),
                               b=_lib.host_ptr(self._b_host), precision=self.precision, air=1 if air else 0,
                               cp=float(self.cpa), kappa=float(self.kap), rd=float(self.rda), p0=P0,
-                              thin_wind=float(thin_wind))
+                              thin_wind=float(thin_wind), wall=_lib.host_ptr(self._wall) if self._wall is not None else None,
+                              shelf=float(shelf), shelf_bed=1 if shelf_bed else 0)
         h = ctypes.c_void_p()
         _lib.check(_lib.isw_layers_create(dg.handle, ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -76,6 +78,55 @@ class Layers:
         if h is not None and h.value and destroy is not None:      # (module globals are gone at interpreter exit)
             destroy(h)
             self._h = None
+
+    # the per-step fields of the option branches, set as attributes as the reference's callers do (ocean.py:159,
+    # tides.py:64-69); the arrays are borrowed by the core until replaced or set to None
+    def _set(self, name, code, a, shape, value=0.0):
+        ptr = None if a is None else device_ptr(a, shape=shape, name=name, device=self.dg.device)
+        _lib.check(_lib.isw_layers_set_option(self._h, code, ptr, float(value)))
+        self._opts[name] = a
+
+    @property
+    def sig(self):
+        return self._opts['sig']
+
+    @sig.setter
+    def sig(self, a):
+        self._set('sig', _lib.ISW_OPT_SIG, a, (self.L, self.dg.N))
+
+    @property
+    def zm(self):
+        """The layers' mid-heights of the per-cell buoyancy form; the core keeps its own (an assigned array is unused)."""
+        return self._zm
+
+    @zm.setter
+    def zm(self, a):
+        self._zm = a
+
+    @property
+    def tide(self):
+        return self._opts['tide']
+
+    @tide.setter
+    def tide(self, a):
+        self._set('tide', _lib.ISW_OPT_TIDE, a, (self.dg.N,))
+
+    @property
+    def cbot(self):
+        return self._opts['cbot']
+
+    @cbot.setter
+    def cbot(self, a):
+        self._set('cbot', _lib.ISW_OPT_CBOT, a, (self.dg.E,))
+
+    @property
+    def cd_bot(self):
+        return self._opts['cd_bot']
+
+    @cd_bot.setter
+    def cd_bot(self, v):
+        _lib.check(_lib.isw_layers_set_option(self._h, _lib.ISW_OPT_CD_BOT, None, float(v)))
+        self._opts['cd_bot'] = float(v)
 
     def _shapes(self):
         return (self.L, self.dg.N), (self.L, self.dg.E)

@@ -19,6 +19,8 @@ Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
                  aquaplanet start (cases.aqua), surface drag, nabla^4, interfacial stress with its heating: 12 steps
 - exchange_n4.npz the between-step exchange hook (Layers.exchange): Boussinesq layers after one step, seeded thickness
                  moves, plain and sequential; air layers after one step, with heating and the thin layers' wind
+- options_n4.npz the option branches on the reference's outcrop case: thin walls, the shelf with its bed flags,
+                 per-cell buoyancy (sig, zm), a tide potential, the bottom's quadratic and internal-tide drag: 12 steps
 
 `--only NAME` writes one fixture (e.g. `--only airtheta`).
 """
@@ -81,6 +83,9 @@ def main():
     dg = DeviceGrid(g)
     if a.only == 'airtheta':
         save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
+        return
+    if a.only == 'options':
+        save('options_n4.npz', options(cp, base, Layers, DeviceGrid, rcases, mycases))
         return
     if a.only == 'exchange':
         save('exchange_n4.npz', exchange(cp, g, dg, Layers, rcases, mycases))
@@ -188,6 +193,39 @@ def main():
     save('dsum.npz', d)
     save('airtheta_n4.npz', air_theta(cp, g, dg, Layers, rcases, mycases))
     save('exchange_n4.npz', exchange(cp, g, dg, Layers, rcases, mycases))
+    save('options_n4.npz', options(cp, base, Layers, DeviceGrid, rcases, mycases))
+
+
+def options(cp, g0, Layers, DeviceGrid, rcases, mycases):
+    """The reference's outcrop case (two layers over a ridge that pierces the lower one) with every option branch on:
+    5% of the edges walled (seeded), shelf 50 m with the bed flags, per-cell buoyancy sigma = (0, 0.02 (1 + 0.05 r)) for
+    the fixed g', a tide potential 0.5 sin(2 lon) cos^2(lat) m^2/s^2, bottom quadratic drag 2.5e-3 and an internal-tide
+    drag U(0, 1e-4) m/s per edge; 12 steps of 3600 s."""
+    rng = np.random.default_rng(5)
+    dg0 = DeviceGrid(g0)
+    ho, bo, uo = rcases.outcrop(g0)
+    nu4 = mycases.visc4(g0, 0.5)
+    wall = np.where(rng.uniform(0, 1, g0.E) < 0.05, 0.0, 1.0)
+    core = Layers(dg0, 2, b=bo, gprime=[0.02], stress=[0.0, 2.5e-4], nu4=nu4, floor=1.0, wall=wall, shelf=50.0,
+                  shelf_bed=True)
+    sig = np.stack([np.zeros(g0.N), 0.02 * (1 + 0.05 * rng.uniform(-1, 1, g0.N))])
+    tide = 0.5 * np.sin(2 * g0.lon) * np.cos(g0.lat) ** 2
+    cbot = rng.uniform(0.0, 1e-4, g0.E)
+    core.sig, core.zm = cp.asarray(sig), cp.zeros((2, g0.N))
+    core.tide = cp.asarray(tide)
+    core.cd_bot = 2.5e-3
+    core.cbot = cp.asarray(cbot)
+    h, u = cp.asarray(ho), cp.asarray(uo)
+    dt = 3600.0
+    nfast = int(math.ceil(1.2 * core.substeps(h, dt)))
+    Fm = cp.zeros((2, g0.E))
+    d = dict(dt=dt, nfast=nfast, nu4=nu4, h0=ho, u0=uo, b=bo, wall=wall, sig=sig, tide=tide, cbot=cbot)
+    for st in range(1, 13):
+        core.step(h, u, dt, nfast, Fm)
+        if st == 1:
+            d.update(h1=h.get(), u1=u.get(), Fm1=Fm.get())
+    d.update(h=h.get(), u=u.get(), Fm=Fm.get(), zm=core.zm.get())
+    return d
 
 
 def exchange(cp, g, dg, Layers, rcases, mycases):

@@ -213,20 +213,16 @@ def test_repeat_runs_identical(dev, isw, grid4):
 
 
 def test_unsupported_options_refused(dev, isw, grid4):
-    """Options this core does not build are refused at construction: walls, the shelf, and air layers in the mixed
-    form (air layers run in the FP64 form)."""
+    """The option branches and air layers run in the FP64 form; in the mixed form they are refused at construction."""
     gpu, layers, _ = isw
-    dg = gpu.DeviceGrid(grid4)
-    for kw in (dict(wall=np.ones(dg.E)), dict(shelf=50.0)):
-        with pytest.raises(NotImplementedError):
-            layers.Layers(dg, 1, **kw)
     gpu.set_precision('mixed')
     try:
         dgm = gpu.DeviceGrid(grid4)
     finally:
         gpu.set_precision('double')
-    with pytest.raises(NotImplementedError):
-        layers.Layers(dgm, 2, gprime=[0.0], air={'cp': 1004.6})
+    for kw in (dict(wall=np.ones(dgm.E)), dict(shelf=50.0), dict(air={'cp': 1004.6})):
+        with pytest.raises(NotImplementedError):
+            layers.Layers(dgm, 2, gprime=[0.0], **kw)
 
 
 def test_bad_arguments_rejected(dev, isw, grid4):
@@ -310,3 +306,35 @@ def test_exchange_golden(dev, isw, grid4):
     for name, x in (('h', h), ('u', u), ('M', M), ('psi', psi), ('theta', theta)):
         e = rel(x.cpu().numpy(), z[f'a_{name}'])
         assert e <= REL, ('air', name, e)
+
+
+def test_option_branches_golden(dev, isw, grid4):
+    """Every option branch of Boussinesq layers at once on the reference's outcrop case (walls, the shelf with its bed
+    flags, per-cell buoyancy, a tide potential, the bottom's quadratic and internal-tide drag), set as the reference's
+    callers set them: h, u, Fm after 1 and 12 steps to 1e-12 of the reference's (its stress term calls exp), and the
+    step with walls refused by a batch."""
+    gpu, layers, _ = isw
+    z = golden('options_n4')
+    dg = gpu.DeviceGrid(grid4)
+    core = layers.Layers(dg, 2, b=z['b'], gprime=[0.02], stress=[0.0, 2.5e-4], nu4=float(z['nu4']), floor=1.0,
+                         wall=z['wall'], shelf=50.0, shelf_bed=True)
+    sig, tide, cbot = T(z['sig'], dev), T(z['tide'], dev), T(z['cbot'], dev)
+    core.sig, core.zm = sig, torch.zeros_like(sig)
+    core.tide = tide
+    core.cd_bot = 2.5e-3
+    core.cbot = cbot
+    h, u = T(z['h0'], dev), T(z['u0'], dev)
+    Fm = torch.zeros_like(u)
+    dt, nfast = float(z['dt']), int(z['nfast'])
+    assert core.substeps(h, dt) * 1.2 <= nfast
+    for s in range(1, 13):
+        core.step(h, u, dt, nfast, Fm)
+        if s in (1, 12):
+            torch.cuda.synchronize()
+            sfx = '1' if s == 1 else ''
+            for name, x in (('h', h), ('u', u), ('Fm', Fm)):
+                e = rel(x.cpu().numpy(), z[name + sfx])
+                assert e <= REL, (s, name, e)
+    from isw.batch import Batch
+    with pytest.raises(NotImplementedError):
+        Batch(0).add(core, h, u, Fm, dt=dt, nfast=nfast)
