@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
       ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
       if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, fp64::div_cell<LL>(M, d.u, i));
     } else if (kind == 1) {
-      ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL>(M, d.h, d.u, i));
+      ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
     } else if (M.nu4 != 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::curl_vertex<LL>(M, d.u, i));
     }
@@ -71,28 +71,28 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     }
   } else if (PH == PH_A) {
     const StageArgs a = stage_args(d, st);
-    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL>(M, a.hs, a.us, i));
+    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL, false>(M, a.hs, a.us, i));
     else ISW_BATCH_L(d.L, LMAXK, fp64::pv_vertex<LL>(M, a.hs, a.us, i));
   } else if (PH == PH_E) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL>(M, a.hs, a.us, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL, false>(M, a.hs, a.us, i));
   } else if (PH == PH_S) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL>(M, a.us, a.cdt, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i));
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], j, i);
   } else if (PH == PH_U) {
     if (!d.tiled && j < d.n[st]) fp64::bt_u_edge_y(M, d.tau[st], i);
   } else if (PH == PH_C) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::scale_cell<LL>(M, a, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::scale_cell<LL, false>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
-    else ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL>(M, a, i));
+    else ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
   } else if (PH == PH_POST) {
     if (kind == 1) {
-      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
+      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
     } else {
       ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
     }
@@ -796,7 +796,9 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     if (!b || !layers || !h || !u || !Fm || !slot) fail(ISW_EINVAL, "batch.add: null argument");
     if (layers->grid->device != b->device) fail(ISW_EINVAL, "batch.add: the stack is on another device");
     if (layers->d.air) fail(ISW_EUNSUPPORTED, "batch.add: air layers step call by call (isw_layers_step_air)");
-    if (layers->d.wall || layers->d.ob) fail(ISW_EUNSUPPORTED, "batch.add: walls and the shelf bed step call by call");
+    if (layers->d.wall || layers->d.ob || layers->d.shelf > 0 || layers->d.sig || layers->d.tide || layers->d.cbot ||
+        layers->d.cd_bot > 0)
+      fail(ISW_EUNSUPPORTED, "batch.add: the option branches (walls, shelf, sig, tide, bottom drag) step call by call");
     if (!(dt > 0) || !std::isfinite(dt) || nfast < 1) fail(ISW_EINVAL, "batch.add: dt must be positive and nfast >= 1");
     if (tr) {
       if (!M || !M1 || !tracers) fail(ISW_EINVAL, "batch.add: transport needs M, M1 and the tracers");

@@ -95,17 +95,17 @@ __device__ inline bool grid_sync(GridBarrier *b, int *status, long long timeout_
   return ok != 0;
 }
 
-#define ISW_BATCH_L(LV, LMAXK, CALL)                                                            \
+#define ISW_BATCH_L(LV, LMAXK, ...)                                                             \
   do {                                                                                          \
     switch (LV) {                                                                               \
-      case 1: { constexpr int LL = 1; CALL; } break;                                            \
-      case 2: if (LMAXK >= 2) { constexpr int LL = 2 <= LMAXK ? 2 : 1; CALL; } break;           \
-      case 3: if (LMAXK >= 3) { constexpr int LL = 3 <= LMAXK ? 3 : 1; CALL; } break;           \
-      case 4: if (LMAXK >= 4) { constexpr int LL = 4 <= LMAXK ? 4 : 1; CALL; } break;           \
-      case 5: if (LMAXK >= 5) { constexpr int LL = 5 <= LMAXK ? 5 : 1; CALL; } break;           \
-      case 6: if (LMAXK >= 6) { constexpr int LL = 6 <= LMAXK ? 6 : 1; CALL; } break;           \
-      case 7: if (LMAXK >= 7) { constexpr int LL = 7 <= LMAXK ? 7 : 1; CALL; } break;           \
-      case 8: if (LMAXK >= 8) { constexpr int LL = 8 <= LMAXK ? 8 : 1; CALL; } break;           \
+      case 1: { constexpr int LL = 1; __VA_ARGS__; } break;                                     \
+      case 2: if (LMAXK >= 2) { constexpr int LL = 2 <= LMAXK ? 2 : 1; __VA_ARGS__; } break;    \
+      case 3: if (LMAXK >= 3) { constexpr int LL = 3 <= LMAXK ? 3 : 1; __VA_ARGS__; } break;    \
+      case 4: if (LMAXK >= 4) { constexpr int LL = 4 <= LMAXK ? 4 : 1; __VA_ARGS__; } break;    \
+      case 5: if (LMAXK >= 5) { constexpr int LL = 5 <= LMAXK ? 5 : 1; __VA_ARGS__; } break;    \
+      case 6: if (LMAXK >= 6) { constexpr int LL = 6 <= LMAXK ? 6 : 1; __VA_ARGS__; } break;    \
+      case 7: if (LMAXK >= 7) { constexpr int LL = 7 <= LMAXK ? 7 : 1; __VA_ARGS__; } break;    \
+      case 8: if (LMAXK >= 8) { constexpr int LL = 8 <= LMAXK ? 8 : 1; __VA_ARGS__; } break;    \
       default: break;                                                                           \
     }                                                                                           \
   } while (0)

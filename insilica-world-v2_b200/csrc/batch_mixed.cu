@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
     else ISW_BATCH_L(d.L, LMAXK, mixed::u_edge<LL>(M, a, i));
   } else if (PH == PH_POST) {
     if (kind == 1) {
-      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL>(M, d.h, d.u, d.dt, i));
+      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
     } else {
       ISW_BATCH_L(d.L, LMAXK, mixed::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
     }

@@ -31,8 +31,9 @@ __device__ __forceinline__ double shelf_at(const LayersDev &M, int k, int i, int
   return !M.ob || M.ob[(size_t)k * N + i] > 0 || M.ob[(size_t)k * N + j] > 0 ? M.shelf : 0.0;
 }
 
+template <bool OPT>
 __device__ __forceinline__ double edge_hk(const LayersDev &M, int k, int i, int j, double a, double b) {
-  if (M.shelf > 0) {
+  if (OPT && M.shelf > 0) {
     const double sh = shelf_at(M, k, i, j);
     const double m = a < b ? a : b;
     if (sh > 0 && m < sh) return m;
@@ -40,7 +41,8 @@ __device__ __forceinline__ double edge_hk(const LayersDev &M, int k, int i, int 
   return 0.5 * (a + b);
 }
 
-__device__ __forceinline__ bool walled(const LayersDev &M, int e) { return M.wall && M.wall[e] == 0; }
+template <bool OPT>
+__device__ __forceinline__ bool walled(const LayersDev &M, int e) { return OPT && M.wall && M.wall[e] == 0; }
 
 // the squeezed-layer flags ob (reference lay_onbed, layers.cu:51-58)
 template <int L>
@@ -65,18 +67,18 @@ __device__ __forceinline__ void eta0_cell(const LayersDev &M, const double *__re
   M.eta0[i] = z;
 }
 
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void ubar0_edge(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int e) {
   const int N = M.g.N, E = M.g.E;
   const int a = M.g.eI[e], b = M.g.eJ[e];
   double H = 0, U = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    const double he = edge_hk(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    const double he = edge_hk<OPT>(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
     H += he;
     U += he * u[(size_t)k * E + e];
   }
-  M.ub0[e] = walled(M, e) ? 0.0 : U / H;
+  M.ub0[e] = walled<OPT>(M, e) ? 0.0 : U / H;
 }
 
 // ---- vector Laplacian ----
@@ -139,7 +141,7 @@ __device__ __forceinline__ void lap_edge(const LayersDev &M, double *__restrict_
 }
 
 // ---- stage phase A ----
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int i) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
@@ -159,7 +161,7 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
   double Mp = 0, P = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    if (M.sig) {                   // per-cell buoyancy (reference layers.cu:90-95): M_k = P_k + sigma_k z_k
+    if (OPT && M.sig) {            // per-cell buoyancy (reference layers.cu:90-95): M_k = P_k + sigma_k z_k
       const double sk = M.sig[(size_t)k * N + i], hk = h[(size_t)k * N + i];
       Mp = P + sk * z[k];
       P += sk * hk;
@@ -176,7 +178,7 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
         ke += c[t] * ue * ue;
       }
     double Bk = Mp + ke / A;
-    if (M.tide) Bk -= M.tide[i];   // the tide-generating potential (reference layers.cu:106)
+    if (OPT && M.tide) Bk -= M.tide[i];   // the tide-generating potential (reference layers.cu:106)
     M.B[(size_t)k * N + i] = Bk;
   }
   M.eta[i] = M.eta0[i];
@@ -212,7 +214,7 @@ __device__ __forceinline__ void pv_vertex(const LayersDev &M, const double *__re
 }
 
 // ---- stage phase E ----
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u, int e) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E, NV = g.NV;
@@ -221,7 +223,7 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const size_t o = (size_t)k * E + e;
-    const double hv = edge_hk(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
+    const double hv = edge_hk<OPT>(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
     const double qv = 0.5 * (M.q[(size_t)k * NV + v1] + M.q[(size_t)k * NV + v2]);
     M.hedge[o] = hv;
     pp[k * 3 + 0] = hv;
@@ -233,7 +235,7 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 }
 
 // ---- stage phase S: slow tendencies ----
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__restrict__ u, double dts, int e,
                                           const double *__restrict__ theta = nullptr) {
   const GridDev &g = M.g;
@@ -277,13 +279,13 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
     const double *Bl = M.B + (size_t)k * N;
     // a layer squeezed by the shelf fades its pressure force and takes a day's drag (reference layers.cu:293-297);
     // shelf off: sq = 1, the force is -(B_J - B_I) / d and the drag term (1 - 1) / 21600 = 0
-    const double shk = M.shelf > 0 ? shelf_at(M, k, a, b) : 0.0;
+    const double shk = OPT && M.shelf > 0 ? shelf_at(M, k, a, b) : 0.0;
     const double sq0 = shk > 0 && he[k] < shk ? (he[k] - 2 * M.floor_ > 0 ? (he[k] - 2 * M.floor_) / (shk - 2 * M.floor_) : 0.0) : 1.0;
     const double sq = theta ? 1.0 : sq0;
     sqk[k] = sq0;
     double d = Q[k] - (sq * (Bl[b] - Bl[a])) / de - (M.drag[k] + (1 - sq) / 21600.0) * ue;
     double ck = M.stress[k];
-    if (k == L - 1 && (M.cd_bot > 0 || M.cbot)) {
+    if (OPT && k == L - 1 && (M.cd_bot > 0 || M.cbot)) {
       // the bottom layer's quadratic stress cd |u| (|u| from the normal and the TRiSK tangential wind) and the internal
       // tide's drag (reference layers.cu:303-311)
       if (M.cd_bot > 0) {
@@ -302,7 +304,7 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
       const double *pl = M.pibar + (size_t)k * N;
       d = d + (0.5 * (pl[a] + pl[b]) * (tl[b] - tl[a])) / de;
     }
-    if (M.sig) {                   // per-cell buoyancy: + zm grad(sigma) (reference layers.cu:327-331)
+    if (OPT && M.sig) {            // per-cell buoyancy: + zm grad(sigma) (reference layers.cu:327-331)
       const double *sl = M.sig + (size_t)k * N;
       const double *zl = M.zm + (size_t)k * N;
       d = d + sq * ((0.5 * (zl[a] + zl[b]) * (sl[b] - sl[a])) / de);
@@ -312,7 +314,7 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
     H += he[k];
     U += he[k] * ue;
   }
-  if (theta && M.shelf > 0) {      // air squeezed against the ground takes its neighbours' tendency (layers.cu:341-355)
+  if (OPT && theta && M.shelf > 0) {   // air squeezed against the ground takes its neighbours' tendency (layers.cu:341-355)
     double Tn[L];
 #pragma unroll
     for (int k = 0; k < L; k++) {
@@ -364,7 +366,7 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, double tau, int e)
   const double ej = M.Gc[j] * (M.eta[j] + gam * (M.eta[j] - M.eta_prev[j]));
   const double ei = M.Gc[i] * (M.eta[i] + gam * (M.eta[i] - M.eta_prev[i]));
   M.ub[e] = v + tau * ((-(ej - ei)) / g.de[e] + M.G[e]);
-  if (walled(M, e)) {              // walls (reference layers.py:173-174)
+  if (walled<true>(M, e)) {        // walls (reference layers.py:173-174)
     M.ub[e] = 0.0;
     M.acc[e] = 0.0;
   }
@@ -413,7 +415,7 @@ __device__ __forceinline__ void bt_u_edge_y(const LayersDev &M, double tau, int 
 }
 
 // ---- stage phase C: layer fluxes and the floor limiter's scale ----
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &a, int i) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
@@ -432,8 +434,8 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &
     const double ubs = M.ubs[e], acc = M.acc[e], le = g.le[e];
 #pragma unroll
     for (int k = 0; k < L; k++) {
-      const double he = edge_hk(M, k, ea, eb, a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
-      const double F = walled(M, e) ? 0.0 : he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
+      const double he = edge_hk<OPT>(M, k, ea, eb, a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
+      const double F = walled<OPT>(M, e) ? 0.0 : he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
       if (mine) M.F[(size_t)k * E + e] = F;
       const double f = F * le * a.cdt;
       if (mine) { if (f > 0) out[k] += f; }
@@ -483,7 +485,7 @@ __device__ __forceinline__ void h_cell(const LayersDev &M, const StageArgs &a, i
   }
 }
 
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void u_edge(const LayersDev &M, const StageArgs &a, int e) {
   const GridDev &g = M.g;
   const int E = g.E;
@@ -493,12 +495,12 @@ __device__ __forceinline__ void u_edge(const LayersDev &M, const StageArgs &a, i
   for (int k = 0; k < L; k++) {
     const size_t o = (size_t)k * E + e;
     if (a.Fm) a.Fm[o] = limited(M, k, e) * le * a.dt;
-    a.un[o] = walled(M, e) ? 0.0 : a.u0[o] + a.cdt * M.Tp[o] + dub;
+    a.un[o] = walled<OPT>(M, e) ? 0.0 : a.u0[o] + a.cdt * M.Tp[o] + dub;
   }
 }
 
 // ---- after the stages: interfacial stress ----
-template <int L>
+template <int L, bool OPT = true>
 __device__ __forceinline__ void vmix_edge(const LayersDev &M, const double *__restrict__ h, double *__restrict__ u, double dt, int e) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
@@ -520,7 +522,7 @@ __device__ __forceinline__ void vmix_edge(const LayersDev &M, const double *__re
     d += 0.5 * ha * hb / (ha + hb) * (du0 * du0 - du1 * du1);
   }
   M.diss[e] = d;
-  if (walled(M, e))
+  if (walled<OPT>(M, e))
     for (int k = 0; k < L; k++) u[(size_t)k * E + e] = 0.0;
 }
 
