@@ -37,6 +37,7 @@ class Request:
     layers: int             # 3: the air stack; 5: air and ocean
     seed: int = 0
     state: list = field(default=None, repr=False)   # the initial stack states (host), as a client sends them
+    resume: dict = field(default=None, repr=False)  # a checkpoint to continue from: arrays and steps left
 
 
 @dataclass
@@ -120,11 +121,57 @@ class Server:
         finally:
             gpu.set_precision(prev)
         steps = max(1, int(math.ceil(req.days * SECONDS_PER_DAY / m.dt - 1e-9)))
-        return dict(req=req, member=m, left=steps, steps=steps, admitted=now, bytes=self.footprint(req))
+        left = steps
+        if req.resume is not None:                  # continue a checkpointed run from its saved state
+            for k, st in enumerate(m.stacks):
+                st.load(req.resume['arrays'], f's{k}_')
+            left = int(req.resume['left'])
+        return dict(req=req, member=m, left=left, steps=steps, admitted=now, bytes=self.footprint(req))
 
-    def run(self, requests, stream=None, clock=time.perf_counter):
+    def checkpoint(self, directory, active, waiting):
+        """Write every resident request's state (reference save-file format: isw.savefile) and the waiting requests'
+        descriptions to `directory`; Server.resume reads them back."""
+        import json
+        from pathlib import Path
+        from . import savefile
+        d = Path(directory)
+        d.mkdir(parents=True, exist_ok=True)
+        files = []
+        for a in active:
+            r, m = a['req'], a['member']
+            arrays = {}
+            for k, st in enumerate(m.stacks):
+                arrays.update(st.arrays(f's{k}_'))
+            meta = dict(rid=r.rid, arrival=r.arrival, level=r.level, days=r.days, layers=r.layers, seed=r.seed,
+                        steps=a['steps'], left=a['left'], precision=self.precision, ntracers=self.ntracers)
+            name = f'request_{r.rid}.zip'
+            savefile.write(d / name, meta, arrays)
+            files.append(name)
+        pending = [dict(rid=r.rid, arrival=r.arrival, level=r.level, days=r.days, layers=r.layers, seed=r.seed) for r in waiting]
+        (d / 'manifest.json').write_text(json.dumps(dict(resident=files, waiting=pending), indent=1, sort_keys=True))
+
+    @staticmethod
+    def resume(directory):
+        """The requests of a checkpoint (Server.checkpoint): resident ones carry their saved state and steps left,
+        waiting ones start from their seeds; all arrive at time 0 of the next run."""
+        import json
+        from pathlib import Path
+        from . import savefile
+        d = Path(directory)
+        man = json.loads((d / 'manifest.json').read_text())
+        out = []
+        for name in man['resident']:
+            meta, arrays = savefile.read(d / name)
+            out.append(Request(meta['rid'], 0.0, meta['level'], meta['days'], meta['layers'], seed=meta['seed'],
+                               resume=dict(arrays=arrays, left=meta['left'])))
+        for w in man['waiting']:
+            out.append(Request(w['rid'], 0.0, w['level'], w['days'], w['layers'], seed=w['seed']))
+        return out
+
+    def run(self, requests, stream=None, clock=time.perf_counter, stop_after=None, checkpoint_dir=None):
         """Serve the requests (arrival times relative to the start of the call); returns (results in completion order,
-        stats). A request is done when its final state is on the host."""
+        stats). A request is done when its final state is on the host. stop_after: after that many batched steps,
+        checkpoint the resident and waiting requests to checkpoint_dir and return (Server.resume continues them)."""
         st = torch.cuda.current_stream(self.dev) if stream is None else stream
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         waiting, active, results = deque(), [], []
@@ -149,6 +196,12 @@ class Server:
                 if pending:                                 # idle until the next arrival
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
                 continue
+            if stop_after is not None and steps >= stop_after:
+                self.checkpoint(checkpoint_dir, active, list(waiting) + list(pending))
+                for a in active:
+                    a['member'].unregister()
+                active = []
+                break
             self.batch.step(st)
             st.synchronize()
             steps += 1

@@ -42,6 +42,17 @@ class Stack:
     def state(self):
         return [self.h, self.u, self.M] + self.tracers
 
+    def arrays(self, prefix):
+        """The stack's resident state as host arrays named prefix + h, u, M, tr0.. (for a save file)."""
+        out = {prefix + 'h': self.h.cpu().numpy(), prefix + 'u': self.u.cpu().numpy(), prefix + 'M': self.M.cpu().numpy()}
+        out.update({f'{prefix}tr{j}': t.cpu().numpy() for j, t in enumerate(self.tracers)})
+        return out
+
+    def load(self, arrays, prefix):
+        """Overwrite the resident state from arrays (as written by arrays())."""
+        for name, t in [('h', self.h), ('u', self.u), ('M', self.M)] + [(f'tr{j}', x) for j, x in enumerate(self.tracers)]:
+            t.copy_(torch.as_tensor(arrays[prefix + name], device=t.device))
+
     def register(self, batch):
         """Add this stack to a Batch: the batch's step then does this stack's step(), with M <- M1 copied (not swapped)."""
         return batch.add(self.core, self.h, self.u, self.Fm, tr=self.tr if self.T else None, M=self.M, M1=self.M1,

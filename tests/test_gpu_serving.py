@@ -70,3 +70,25 @@ def test_admission_respects_budget(dev, grids):
     assert [r.rid for r in results] == [0, 1, 2]
     for a, b in zip(results, results[1:]):
         assert b.admitted >= a.done - 1e-3
+
+
+def test_checkpoint_resume_equals_uninterrupted(dev, grids, tmp_path):
+    """A served request stopped after 5 batched steps, checkpointed (reference save-file format) and resumed in a new
+    server ends bit for bit where the uninterrupted run ends; a request still waiting at the checkpoint runs too."""
+    from isw.serving import Request, Server
+    def reqs():
+        return [Request(0, 0.0, 4, 0.25, 5, seed=61), Request(1, 0.0, 5, 0.1, 3, seed=62)]
+    whole = Server(0, precision='mixed', ntracers=2, grids=grids, keep_state=True)
+    first = Server(0, precision='mixed', ntracers=2, grids=grids, budget_bytes=1.0)   # one resident at a time
+    again = Server(0, precision='mixed', ntracers=2, grids=grids, keep_state=True)
+    for srv in (whole, first, again):
+        srv.batch.config(layout='packed')          # every stack in tiles, whatever shares the batch
+    ref = {r.rid: r for r in whole.run(reqs())[0]}
+    done, _ = first.run(reqs(), stop_after=5, checkpoint_dir=tmp_path)
+    assert not done and (tmp_path / 'manifest.json').exists()
+    res = {r.rid: r for r in again.run(Server.resume(tmp_path))[0]}
+    assert sorted(res) == [0, 1]
+    for rid in (0, 1):
+        assert res[rid].steps == ref[rid].steps
+        for x, y in zip(res[rid].state, ref[rid].state):
+            assert torch.equal(x, y)
