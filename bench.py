@@ -174,6 +174,23 @@ def run_reference(args, rank):
     print(json.dumps(out), flush=True)
 
 
+def max_over_ranks(x, dist, device):
+    """The largest of every rank's x (a time: the job runs at its slowest rank's pace); x itself without a process
+    group. Every rank takes this collective at the same point."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, dt, ms):
+    """Model days per second of the whole job: `world` replicas, each advancing dt seconds of model time per step of
+    ms milliseconds (the max over ranks)."""
+    return world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
+
+
 def fp64_step_seconds(keys, warmup=3, steps=10):
     """Seconds per step of ONE member of each (level, layers) key alone on the plain FP64 core (its own batched graph):
     the sequential baseline of the ensemble and serving workloads."""
@@ -406,11 +423,7 @@ def main():
         if dist:
             dist.barrier()
         t = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
-        if dist:
-            x = torch.tensor([t], device=dev)
-            dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            t = float(x.item())
-        return t
+        return max_over_ranks(t, dist, dev)
 
     member, layout = make('double')
     mixed, layout_m = (None, None) if args.no_mixed else make('mixed')
@@ -439,7 +452,7 @@ def main():
 
     finite = all(bool(torch.isfinite(a).all()) for a in member.state())
     dt = member.dt
-    value = world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
+    value = job_value(world, dt, ms)
     if batched is not None:
         batched['mixed_vs_fp64_member'] = batched['mixed']['value'] / value
         batched['mixed_vs_fp64_batched'] = batched['mixed']['value'] / batched['double']['value']
@@ -460,11 +473,7 @@ def main():
             hbuf.copy_(a, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
     io_bytes = sum(a.numel() * a.element_size() for a in member.state())
 
     bytes_step = 0
@@ -489,11 +498,11 @@ def main():
                            parallelism=f'replicas x{world}', l2='flushed between timed steps (252 MB write)'),
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=traffic,
                              peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step'),
-               e2e=dict(value=world * (dt / SECONDS_PER_DAY) / (e2e_ms / 1e3), unit='model days/s',
+               e2e=dict(value=job_value(world, dt, e2e_ms), unit='model days/s',
                         h2d_bytes_per_step=io_bytes, d2h_bytes_per_step=io_bytes),
                gpu_launches=member.launches() * args.steps, clocks=clk.summary(), finite=finite, grid_build_s=t_grid)
     if mixed is not None:
-        vm = world * (dt / SECONDS_PER_DAY) / (ms_m / 1e3)
+        vm = job_value(world, dt, ms_m)
         out['mixed'] = dict(value=vm, unit='model days/s', ms_per_step=ms_m, speedup_vs_fp64=vm / value, steps=args.steps,
                             dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets',
                             tiles=layout_m, finite=all(bool(torch.isfinite(a).all()) for a in mixed.state()),
