@@ -1,6 +1,7 @@
-// Phase functions of the FCT transport step, mixed form: the passes of transport_fp64.cuh (reference fused.cu:122-241)
-// with the 3rd-order flux's curvature correction in FP32 (stencil weights, the stencil sums and f (a + b) - |f| (b - a)
-// beta) and the stage fields p1, p2, the antidiffusive fluxes A and the ratios R+- stored in FP32, as the reference's
+// Phase functions of the FCT transport step, mixed form, for the batched step's edge and cell passes (the passes of
+// transport_fp64.cuh, reference fused.cu:122-241) with the 3rd-order flux's curvature correction in FP32 (stencil
+// weights, the stencil sums and f (a + b) - |f| (b - a) beta) and the stage fields p1, p2, the antidiffusive fluxes A
+// and the ratios R+- stored in FP32, as the reference's
 // mixed form keeps its stencil weights and field copy 32-bit (gpu.py:77, transport.py:28). Tracer masses stay FP64:
 // the upwind fluxes, the mean-value part of the 3rd-order flux f (p_I + p_J) / 2, every cell sum, td, the bounds and the
 // limited update. Each edge's flux enters both of its cells with the same value (the passes compute it from the same
@@ -41,150 +42,6 @@ __device__ __forceinline__ double hoflux(double f, const T *__restrict__ ps, con
   const float ff = (float)f;
   const float corr = fabsf(ff) * ((y - x) * beta) - ff * (x + y);
   return f * (0.5 * ((double)pa + (double)pb)) + (double)corr;
-}
-
-// P1 for (tracer j, cell i), every layer: M1 (tracer 0 stores it), td and p1 (FP32)
-template <int L>
-__device__ __forceinline__ void tr_p1(const TransportDev &T, const TrArgs &a, int j, int i) {
-  const GridDev &g = T.g;
-  const int N = g.N, E = g.E;
-  fp64::CellEdges c;
-  fp64::load_edges(g, i, c);
-  const float beta = (float)a.beta;
-  double m1[L], td[L], s[L], mx[L];
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t om = (size_t)l * N + i;
-    const double m0 = a.M0[om], pi = a.tr[j][om];
-    T.psi0[(size_t)(j * L + l) * N + i] = pi;
-    m1[l] = m0;
-    td[l] = m0 * pi;
-    s[l] = m0 * pi;
-    mx[l] = m0;
-  }
-  const double frac = 1.0 / 3.0;
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const int e = c.e[q];
-    if (e >= 0) {
-      const bool out = c.a[q] == i;
-      Stencil32 stn;
-      load_stencil(g, e, stn);
-#pragma unroll
-      for (int l = 0; l < L; l++) {
-        const double *p = a.tr[j] + (size_t)l * N;
-        const double f = a.Fm[(size_t)l * E + e];
-        const double pa = p[c.a[q]], pb = p[c.b[q]];
-        const double fu = fp64::upwind_v(f, pa, pb);
-        const double hf = frac * hoflux(f, p, stn, pa, pb, beta);
-        const double m = frac * f;
-        if (out) { m1[l] -= f; td[l] -= fu; s[l] -= hf; mx[l] -= m; }
-        else { m1[l] += f; td[l] += fu; s[l] += hf; mx[l] += m; }
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
-    if (j == 0) a.M1[om] = m1[l];
-    T.td[o] = td[l] / m1[l];
-    T.p1f[o] = (float)(s[l] / mx[l]);
-  }
-}
-
-template <int L>
-__device__ __forceinline__ void tr_p2(const TransportDev &T, const TrArgs &a, int j, int i) {
-  const GridDev &g = T.g;
-  const int N = g.N, E = g.E;
-  fp64::CellEdges c;
-  fp64::load_edges(g, i, c);
-  const float beta = (float)a.beta;
-  double s[L], mx[L];
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
-    s[l] = a.M0[om] * T.psi0[o];
-    mx[l] = a.M0[om];
-  }
-  const double frac = 1.0 / 2.0;
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const int e = c.e[q];
-    if (e >= 0) {
-      const bool out = c.a[q] == i;
-      Stencil32 stn;
-      load_stencil(g, e, stn);
-#pragma unroll
-      for (int l = 0; l < L; l++) {
-        const float *p1 = T.p1f + (size_t)(j * L + l) * N;
-        const double f = a.Fm[(size_t)l * E + e];
-        const double hf = frac * hoflux(f, p1, stn, p1[c.a[q]], p1[c.b[q]], beta);
-        const double m = frac * f;
-        if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < L; l++) T.p2f[(size_t)(j * L + l) * N + i] = (float)(s[l] / mx[l]);
-}
-
-template <int L>
-__device__ __forceinline__ void tr_p3(const TransportDev &T, const TrArgs &a, int j, int i) {
-  const GridDev &g = T.g;
-  const int N = g.N, E = g.E;
-  fp64::CellEdges c;
-  fp64::load_edges(g, i, c);
-  const float beta = (float)a.beta;
-  int nb[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) nb[q] = g.nbr[i * 6 + q];
-  double Pp[L], Pm[L];
-#pragma unroll
-  for (int l = 0; l < L; l++) { Pp[l] = 0; Pm[l] = 0; }
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const int e = c.e[q];
-    if (e >= 0) {
-      const bool out = c.a[q] == i;
-      Stencil32 stn;
-      load_stencil(g, e, stn);
-#pragma unroll
-      for (int l = 0; l < L; l++) {
-        const size_t row = (size_t)(j * L + l);
-        const double *p = T.psi0 + row * N;
-        const float *p2 = T.p2f + row * N;
-        const double f = a.Fm[(size_t)l * E + e];
-        const float Af = (float)(hoflux(f, p2, stn, p2[c.a[q]], p2[c.b[q]], beta) - fp64::upwind_v(f, p[c.a[q]], p[c.b[q]]));
-        const double A = (double)Af;
-        if (out) {
-          T.Af[row * E + e] = Af;
-          if (A > 0) Pm[l] += A; else Pp[l] -= A;
-        } else {
-          if (A > 0) Pp[l] += A; else Pm[l] -= A;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t row = (size_t)(j * L + l);
-    const double *p = T.psi0 + row * N;
-    const double *tt = T.td + row * N;
-    const double ti = tt[i];
-    double hi = fmax(p[i], ti), lo = fmin(p[i], ti);
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-      const int jn = nb[q];
-      if (jn >= 0) {
-        hi = fmax(hi, fmax(p[jn], tt[jn]));
-        lo = fmin(lo, fmin(p[jn], tt[jn]));
-      }
-    }
-    const double m1 = a.M1[(size_t)l * N + i];
-    const double qmax = (hi - ti) * m1, qmin = (ti - lo) * m1;
-    T.Rpf[row * N + i] = Pp[l] > 0 ? (float)fmin(1.0, qmax / Pp[l]) : 0.f;
-    T.Rmf[row * N + i] = Pm[l] > 0 ? (float)fmin(1.0, qmin / Pm[l]) : 0.f;
-  }
 }
 
 template <int L>
