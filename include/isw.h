@@ -178,6 +178,13 @@ int isw_batch_step(isw_batch *b, void *stream);
  * 64..4096, 0 = by blocks per SM; stacks packed into cooperative launches of at most SMs x blocks-per-SM tiles).
  * blocks_per_sm: 0 choose, 1 (1024-thread tiles) or 2 (512-thread tiles). */
 int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, int tile_cells, int blocks_per_sm);
+/* Pipelined steps (on != 0): each isw_batch_step queues a step's dynamics beside the previous step's transport (two
+ * branches of one graph, the step's layer fluxes Fm double-buffered), so the registered masses M and tracers lag the
+ * dynamics by one step until isw_batch_flush, which completes the last step's transport and puts its Fm in the
+ * registered arrays; the state is then bit-identical to stepping in the plain order. Adding or removing stacks,
+ * configuring or switching the mode flushes first. Off by default. */
+int isw_batch_pipeline(isw_batch *b, int on);
+int isw_batch_flush(isw_batch *b, void *stream);
 /* The batch's layout: registered stacks, fast-loop tiles, the exchange interval in use, the largest tile's shared memory
  * (bytes), the cooperative launches per stage, tile blocks per SM (0 when untiled). */
 int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes, int *groups, int *blocks_per_sm);

@@ -90,6 +90,10 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     const StageArgs a = stage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
     else ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
+  } else if (PH == PH_VMIX) {
+    if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
+  } else if (PH == PH_HF1) {
+    ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
   } else if (PH == PH_POST) {
     if (kind == 1) {
       if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
@@ -278,6 +282,17 @@ struct isw_batch {
   int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
   int layout = 0;                             // 0: choose; 1 shared; 2 packed
   bool pdl = true;                            // programmatic dependent launch between phase kernels
+  // pipelined steps: step n's dynamics beside step n-1's transport (two branches of one graph), Fm double-buffered.
+  // desc[q] describes a step whose dynamics write Fm_q and whose transport reads it: Fm_0 the registered Fm, Fm_1 fm_alt
+  bool pipeline = false, primed = false;
+  int parity = 0;
+  StackDesc *d_desc1 = nullptr;
+  std::vector<void *> fm_alt;
+  std::vector<std::pair<double *, size_t>> fm_pairs;  // (registered Fm, bytes) per stack, for the flush's copy-back
+  cudaGraphExec_t pexec[6] = {};              // dynamics D_0, D_1; both branches DT_0, DT_1; transport T_0, T_1
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  const StackDesc *cur = nullptr;             // the descriptors the launches being queued use
   std::map<std::tuple<const isw_grid *, int, int>, std::unique_ptr<TileCache>> tiles;
   std::map<std::pair<const isw_grid *, int>, std::vector<int32_t>> parts;
   cudaStream_t cap = nullptr;
@@ -559,12 +574,25 @@ void rebuild(isw_batch *b) {
   b->d_desc = nullptr;
   b->d_chunks = nullptr;
   b->d_refs = nullptr;
+  b->cur = nullptr;
   b->groups.clear();
   b->ntiles = 0;
   if (b->exec) {
     cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
   }
+  for (auto &x : b->pexec)
+    if (x) {
+      cudaGraphExecDestroy(x);
+      x = nullptr;
+    }
+  cudaFree(b->d_desc1);
+  b->d_desc1 = nullptr;
+  for (void *q : b->fm_alt) cudaFree(q);
+  b->fm_alt.clear();
+  b->fm_pairs.clear();
+  b->primed = false;
+  b->parity = 0;
   b->dirty = false;
   if (desc.empty()) return;
   std::vector<Chunk> all;
@@ -604,6 +632,21 @@ void rebuild(isw_batch *b) {
     }
   }
   ISW_CUDA(cudaMemcpy(b->d_desc, desc.data(), sizeof(StackDesc) * desc.size(), cudaMemcpyHostToDevice));
+  if (b->pipeline) {                         // the other parity's descriptors: the same stacks with a second Fm
+    std::vector<StackDesc> desc1 = desc;
+    for (auto &d : desc1) {
+      const size_t bytes = sizeof(double) * (size_t)d.L * d.M.g.E;
+      void *alt = nullptr;
+      ISW_CUDA(cudaMalloc(&alt, bytes));
+      ISW_CUDA(cudaMemset(alt, 0, bytes));
+      b->fm_alt.push_back(alt);
+      b->fm_pairs.emplace_back(d.Fm, bytes);
+      d.Fm = (double *)alt;
+      d.tr.Fm = (double *)alt;
+    }
+    ISW_CUDA(cudaMalloc(&b->d_desc1, sizeof(StackDesc) * desc1.size()));
+    ISW_CUDA(cudaMemcpy(b->d_desc1, desc1.data(), sizeof(StackDesc) * desc1.size(), cudaMemcpyHostToDevice));
+  }
   if (!refs.empty()) {
     ISW_CUDA(cudaMalloc(&b->d_refs, sizeof(TileRef) * refs.size()));
     ISW_CUDA(cudaMemcpy(b->d_refs, refs.data(), sizeof(TileRef) * refs.size(), cudaMemcpyHostToDevice));
@@ -640,20 +683,22 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = tr
   const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
                  (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
   if (nb == 0) return;
+  if (!b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
   pdl = pdl && b->pdl;
   if (b->mixed == 1) {
-    launch_phase_mixed(PH, b->lmax, nb, st, pdl, b->d_desc, sc, stage, j);
+    launch_phase_mixed(PH, b->lmax, nb, st, pdl, b->cur, sc, stage, j);
     return;
   }
   switch (b->lmax) {
-    case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
-    case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
-    case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
-    default: launch_phase_kernel(k_phase<PH, 8>, nb, st, pdl, (const StackDesc *)b->d_desc, sc, stage, j); break;
+    case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, pdl, b->cur, sc, stage, j); break;
+    case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, pdl, b->cur, sc, stage, j); break;
+    case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, pdl, b->cur, sc, stage, j); break;
+    default: launch_phase_kernel(k_phase<PH, 8>, nb, st, pdl, b->cur, sc, stage, j); break;
   }
 }
 
 void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns, int fault_block) {
+  if (!b->groups.empty() && !b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
   for (const FastGroup &fg : b->groups) {
     if (fg.count == 0) continue;
     ISW_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), st));
@@ -668,7 +713,7 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const TileRef *refs = b->d_refs + fg.begin;
-    const StackDesc *desc = b->d_desc;
+    const StackDesc *desc = b->cur;
     const int rounds = fg.rounds[stage];
     if (b->mixed == 1)
       launch_fast_mixed(b->fast_bps, cfg, desc, refs, stage, rounds, b->bar, b->status, timeout_ns, fault_block);
@@ -680,9 +725,9 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
   }
 }
 
-// The launches of one step, in order. The first kernel of the step and the first after a tile launch (or a memset)
-// take plain stream order; the others are programmatic dependents of the kernel before them.
-void enqueue(isw_batch *b, cudaStream_t st) {
+// The dynamics of one step (through the last stage's D). The first kernel and the first after a tile launch (or a
+// memset) take plain stream order; the others are programmatic dependents of the kernel before them.
+void enqueue_dyn(isw_batch *b, cudaStream_t st) {
   launch_phase<PH_INIT>(b, st, 0, 0, false);
   if (b->any_nu4) {
     launch_phase<PH_LAPE1>(b, st, 0, 0);
@@ -703,14 +748,50 @@ void enqueue(isw_batch *b, cudaStream_t st) {
     launch_phase<PH_C>(b, st, s, 0, !tiled || b->any_untiled);
     launch_phase<PH_D>(b, st, s, 0);
   }
+}
+
+// The transport passes after the stage-1 edge fluxes (P1 .. P4, M <- M1).
+void enqueue_tr_tail(isw_batch *b, cudaStream_t st) {
+  launch_phase<PH_P1>(b, st, 0, 0);
+  launch_phase<PH_P2E>(b, st, 0, 0);
+  launch_phase<PH_P2>(b, st, 0, 0);
+  launch_phase<PH_P3E>(b, st, 0, 0);
+  launch_phase<PH_P3>(b, st, 0, 0);
+  launch_phase<PH_P4>(b, st, 0, 0);
+}
+
+// One step in the plain order: dynamics, then the interfacial stress with the transport's stage-1 edge fluxes, then
+// the transport.
+void enqueue(isw_batch *b, cudaStream_t st) {
+  b->cur = b->d_desc;
+  enqueue_dyn(b, st);
   if (b->any_vmix || b->any_tr) launch_phase<PH_POST>(b, st, 0, 0);
-  if (b->any_tr) {
-    launch_phase<PH_P1>(b, st, 0, 0);
-    launch_phase<PH_P2E>(b, st, 0, 0);
-    launch_phase<PH_P2>(b, st, 0, 0);
-    launch_phase<PH_P3E>(b, st, 0, 0);
-    launch_phase<PH_P3>(b, st, 0, 0);
-    launch_phase<PH_P4>(b, st, 0, 0);
+  if (b->any_tr) enqueue_tr_tail(b, st);
+  ISW_CUDA(cudaGetLastError());
+}
+
+// Pipelined: the dynamics of the step described by `dyn` (with its interfacial stress) on `st`, and beside it on the
+// side stream the transport of the step described by `tr` (the previous one); either may be null.
+void enqueue_pipelined(isw_batch *b, cudaStream_t st, const StackDesc *dyn, const StackDesc *tr) {
+  const bool trans = tr && b->any_tr;
+  if (trans && dyn) {
+    ISW_CUDA(cudaEventRecord(b->ev_fork, st));
+    ISW_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+  }
+  cudaStream_t ts = trans && dyn ? b->side : st;
+  if (trans) {
+    b->cur = tr;
+    launch_phase<PH_HF1>(b, ts, 0, 0, false);
+    enqueue_tr_tail(b, ts);
+  }
+  if (dyn) {
+    b->cur = dyn;
+    enqueue_dyn(b, st);
+    if (b->any_vmix) launch_phase<PH_VMIX>(b, st, 0, 0);
+  }
+  if (trans && dyn) {
+    ISW_CUDA(cudaEventRecord(b->ev_join, b->side));
+    ISW_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
   }
   ISW_CUDA(cudaGetLastError());
 }
@@ -719,31 +800,68 @@ void prepare(isw_batch *b) {
   if (b->dirty) rebuild(b);
 }
 
-void step(isw_batch *b, cudaStream_t st) {
-  prepare(b);
-  if (b->nstacks == 0) return;
+// Queue `body` on st: directly when st is capturing a graph of the caller's, else as a graph of our own (captured on
+// the private stream the first time, cached in *exec).
+template <class F>
+void run_graph(isw_batch *b, cudaStream_t st, cudaGraphExec_t *exec, F body) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   ISW_CUDA(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) {    // inside the caller's capture: queue the launches themselves
-    enqueue(b, st);
+    body(st);
     return;
   }
-  if (!b->exec) {
+  if (!*exec) {
     cudaGraph_t graph = nullptr;
     ISW_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
     try {
-      enqueue(b, b->cap);
+      body(b->cap);
     } catch (...) {
       cudaStreamEndCapture(b->cap, &graph);
       if (graph) cudaGraphDestroy(graph);
       throw;
     }
     ISW_CUDA(cudaStreamEndCapture(b->cap, &graph));
-    const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+    const cudaError_t ie = cudaGraphInstantiate(exec, graph, 0);
     cudaGraphDestroy(graph);
     ISW_CUDA(ie);
   }
-  ISW_CUDA(cudaGraphLaunch(b->exec, st));
+  ISW_CUDA(cudaGraphLaunch(*exec, st));
+}
+
+const StackDesc *desc_of(isw_batch *b, int q) { return q == 0 ? b->d_desc : b->d_desc1; }
+
+// Complete a pipelined batch: the last step's transport, and its Fm back into the registered arrays.
+void flush(isw_batch *b, cudaStream_t st) {
+  if (!b->pipeline || !b->primed) return;
+  const int q = b->parity ^ 1;                // the last step's buffers
+  if (b->any_tr) run_graph(b, st, &b->pexec[4 + q], [&](cudaStream_t s2) { enqueue_pipelined(b, s2, nullptr, desc_of(b, q)); });
+  if (q == 1)
+    for (size_t i = 0; i < b->fm_alt.size(); i++)
+      ISW_CUDA(cudaMemcpyAsync(b->fm_pairs[i].first, b->fm_alt[i], b->fm_pairs[i].second, cudaMemcpyDeviceToDevice, st));
+  b->primed = false;
+}
+
+// Flush a primed pipelined batch before its stacks or settings change (synchronising its private stream).
+void settle(isw_batch *b) {
+  if (b->pipeline && b->primed) {
+    flush(b, b->cap);
+    ISW_CUDA(cudaStreamSynchronize(b->cap));
+  }
+}
+
+void step(isw_batch *b, cudaStream_t st) {
+  prepare(b);
+  if (b->nstacks == 0) return;
+  if (b->pipeline) {
+    const int p = b->parity;
+    const bool both = b->primed;
+    run_graph(b, st, &b->pexec[both ? 2 + p : p],
+              [&](cudaStream_t s2) { enqueue_pipelined(b, s2, desc_of(b, p), both ? desc_of(b, p ^ 1) : nullptr); });
+    b->parity ^= 1;
+    b->primed = true;
+    return;
+  }
+  run_graph(b, st, &b->exec, [&](cudaStream_t s2) { enqueue(b, s2); });
 }
 
 }  // namespace
@@ -764,6 +882,9 @@ int isw_batch_create(int device, isw_batch **out) {
       ISW_CUDA(cudaMalloc(&b->status, sizeof(int)));
       ISW_CUDA(cudaMemset(b->status, 0, sizeof(int)));
       ISW_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+      ISW_CUDA(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+      ISW_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+      ISW_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     } catch (...) {
       cudaFree(b->bar);
       cudaFree(b->status);
@@ -778,7 +899,14 @@ int isw_batch_destroy(isw_batch *b) {
   if (!b) return ISW_OK;
   cudaSetDevice(b->device);
   if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (auto x : b->pexec)
+    if (x) cudaGraphExecDestroy(x);
   if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
+  cudaFree(b->d_desc1);
+  for (void *q : b->fm_alt) cudaFree(q);
   cudaFree(b->d_desc);
   cudaFree(b->d_chunks);
   cudaFree(b->d_refs);
@@ -810,6 +938,8 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     bool any = false;
     for (auto &q : b->slots) any = any || q.used;
     if (any && b->mixed != mixed) fail(ISW_EINVAL, "batch.add: a batch holds stacks of one precision form");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
     BatchSlot sl;
     sl.used = true;
     sl.layers = layers;
@@ -835,6 +965,8 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
 int isw_batch_remove(isw_batch *b, int slot) {
   return guarded([&] {
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used) fail(ISW_EINVAL, "batch.remove: no such slot");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
     b->slots[slot] = BatchSlot();
     b->dirty = true;
   });
@@ -847,6 +979,8 @@ int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, in
     if (layout < 0 || layout > 2) fail(ISW_EINVAL, "batch.config: layout must be 0 (choose), 1 (shared) or 2 (packed)");
     if (tile_cells != 0 && (tile_cells < 64 || tile_cells > 4096)) fail(ISW_EINVAL, "batch.config: tile_cells outside 64..4096");
     if (blocks_per_sm < 0 || blocks_per_sm > 2) fail(ISW_EINVAL, "batch.config: blocks_per_sm must be 0 (choose), 1 or 2");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
     b->tiles_enabled = tiles_enabled ? 1 : 0;
     b->tile_k = tile_k;
     b->layout = layout;
@@ -878,6 +1012,24 @@ int isw_batch_step(isw_batch *b, void *stream) {
   });
 }
 
+int isw_batch_pipeline(isw_batch *b, int on) {
+  return guarded([&] {
+    if (!b) fail(ISW_EINVAL, "batch.pipeline: null handle");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
+    b->pipeline = on != 0;
+    b->dirty = true;
+  });
+}
+
+int isw_batch_flush(isw_batch *b, void *stream) {
+  return guarded([&] {
+    if (!b) fail(ISW_EINVAL, "batch.flush: null handle");
+    ISW_CUDA(cudaSetDevice(b->device));
+    flush(b, (cudaStream_t)stream);
+  });
+}
+
 int isw_batch_status(isw_batch *b, void *stream, int reset) {
   int out = ISW_OK;
   const int rc = guarded([&] {
@@ -900,6 +1052,7 @@ int isw_batch_fault_test(isw_batch *b, long long timeout_ns, void *stream) {
     prepare(b);
     if (b->ntiles == 0) fail(ISW_EUNSUPPORTED, "batch.fault_test: no tiled stack in the batch");
     if (b->groups.empty() || b->groups[0].rounds[2] < 2) fail(ISW_EUNSUPPORTED, "batch.fault_test: the last stage has no grid barrier");
+    b->cur = b->d_desc;
     launch_fast(b, (cudaStream_t)stream, 2, timeout_ns, 0);
   });
 }

@@ -139,8 +139,9 @@ __device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s
 
 // The FCT step's passes: POST (edges: interfacial stress; (tracer, edge): stage-1 fluxes), P1 (cells: M1, td, p1),
 // P2E (stage-2 fluxes), P2 (cells: p2), P3E (antidiffusive fluxes), P3 (cells: ratios), P4 (cells: limited update).
+// A pipelined batch splits POST into VMIX (edges, the dynamics' last pass) and HF1 ((tracer, edge), the transport's first).
 enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4,
-             PH_P1, PH_P2E, PH_P3E };
+             PH_P1, PH_P2E, PH_P3E, PH_VMIX, PH_HF1 };
 
 // Programmatic dependent launch between phase kernels: a phase kernel is launched while the previous one drains; it
 // stages only constant data (its stack descriptor) before waiting for the previous grid's completion and memory
@@ -167,10 +168,10 @@ template <int PH>
 struct Dom {
   static constexpr bool cell = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A || PH == PH_ETA || PH == PH_C || PH == PH_D;
   static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
-                               PH == PH_D || PH == PH_POST;
+                               PH == PH_D || PH == PH_POST || PH == PH_VMIX;
   static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
   static constexpr bool rows = PH == PH_P1 || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
-  static constexpr bool erows = PH == PH_POST || PH == PH_P2E || PH == PH_P3E;
+  static constexpr bool erows = PH == PH_POST || PH == PH_P2E || PH == PH_P3E || PH == PH_HF1;
 };
 
 

@@ -83,6 +83,10 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
     const mixed::MStageArgs a = mstage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, mixed::h_cell<LL>(M, a, i));
     else ISW_BATCH_L(d.L, LMAXK, mixed::u_edge<LL>(M, a, i));
+  } else if (PH == PH_VMIX) {
+    if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
+  } else if (PH == PH_HF1) {
+    ISW_BATCH_L(d.L, LMAXK, mixed::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
   } else if (PH == PH_POST) {
     if (kind == 1) {
       if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
@@ -296,6 +300,8 @@ void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, con
     case PH_P1: launch_m<PH_P1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_VMIX: launch_m<PH_VMIX>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_HF1: launch_m<PH_HF1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     default: break;
   }
 }

@@ -106,6 +106,16 @@ class Batch:
     def step(self, stream=None):
         _lib.check(_lib.isw_batch_step(self._h, stream_of(self.device, stream)))
 
+    def pipeline(self, on=True):
+        """Pipelined steps: each step runs its dynamics beside the previous step's transport (two branches of one
+        graph); the registered masses and tracers lag by one step until flush(), after which the state is bit-identical
+        to the plain order. add/remove/config flush first."""
+        _lib.check(_lib.isw_batch_pipeline(self._h, 1 if on else 0))
+
+    def flush(self, stream=None):
+        """Complete a pipelined batch's last transport (a no-op otherwise)."""
+        _lib.check(_lib.isw_batch_flush(self._h, stream_of(self.device, stream)))
+
     def status(self, reset=False, stream=None):
         """The device status word: 0, or ISW_ETIMEOUT (5) after a grid barrier's bounded wait ran out."""
         st = _lib.isw_batch_status(self._h, stream_of(self.device, stream), 1 if reset else 0)

@@ -220,3 +220,41 @@ def test_autotune_keeps_state(dev, grid4):
     torch.cuda.synchronize()
     for x, y in zip(a.state(), b.state()):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize('precision', ['double', 'mixed'])
+def test_pipelined_equals_plain(dev, grid4, precision):
+    """A pipelined batch (each step's dynamics beside the previous step's transport) gives, after flush(), the plain
+    order's h, u, M, Fm and tracers bit for bit, for an odd and an even number of steps; a stack added midway is
+    flushed in first and the result still matches."""
+    from isw import gpu
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    gpu.set_precision(precision)
+    try:
+        dg = DeviceGrid(planet_grid(grid4))
+        for steps in (5, 6):
+            plain, piped = Batch(0), Batch(0)
+            piped.pipeline(True)
+            a, b = Member(dg, 31, batch=plain), Member(dg, 31, batch=piped)
+            for _ in range(steps):
+                plain.step()
+                piped.step()
+            piped.flush()
+            torch.cuda.synchronize()
+            for sa, sb in zip(a.stacks, b.stacks):
+                for x, y in zip(sa.state() + [sa.Fm], sb.state() + [sb.Fm]):
+                    assert torch.equal(x, y), steps
+        plain.step()
+        piped.step()                                                      # a transport pending ...
+        c, d = Member(dg, 32, batch=plain), Member(dg, 32, batch=piped)   # ... which adding a stack flushes first
+        for _ in range(3):
+            plain.step()
+            piped.step()
+        piped.flush()
+        torch.cuda.synchronize()
+        for x, y in zip(a.state() + c.state(), b.state() + d.state()):
+            assert torch.equal(x, y)
+    finally:
+        gpu.set_precision('double')
