@@ -6,7 +6,9 @@ vorticity) and mass drifts by the deterministic sum.
   state; per stack the relative L2 (area-weighted) and Linf errors of h and u after `days`, and the relative drift of
   every layer's volume and every tracer's mass over the run, in both forms.
 - galewsky(level, days): the Galewsky jet (one layer, the reference's initial state) in both forms; L2/Linf of vertex
-  vorticity and of h, and the mass drift."""
+  vorticity and of h, and the mass drift.
+- w2(level, days): Williamson 2 (one layer, steady solid-body flow, dt 900 s at level 4) in both forms: h and u
+  errors and the mass drift."""
 import numpy as np
 import torch
 
@@ -110,3 +112,32 @@ def galewsky(level=7, days=6.0, nfast=2, device=0):
                 h_l2=l2rel(g.areaCell, hm, hd), h_linf=linf(hm, hd),
                 mass_drift_mixed=float(dm), mass_drift_double=float(dd),
                 status=[res['double'][3], res['mixed'][3]])
+
+
+def w2(level=4, days=5.0, device=0):
+    g = G.for_planet(G.build(level, device=device), 6.371e6, 7.292e-5, 9.80616)
+    h0, bt, u0 = cases.initial_state(g, 'w2')
+    dt, nfast = 900.0 * 2.0 ** (4 - level), 2
+    A = torch.as_tensor(g.areaCell, device=f'cuda:{device}')
+    res = {}
+    for prec in ('double', 'mixed'):
+        gpu.set_precision(prec)
+        try:
+            core = Layers(gpu.DeviceGrid(g, device=device), 1, b=bt)
+        finally:
+            gpu.set_precision('double')
+        h = torch.as_tensor(np.ascontiguousarray(h0[None]), device=f'cuda:{device}')
+        u = torch.as_tensor(np.ascontiguousarray(u0[None]), device=f'cuda:{device}')
+        b = Batch(device)
+        b.add(core, h, u, torch.zeros_like(u), dt=dt, nfast=nfast)
+        m0 = gpu.dsum(h[0], A)
+        steps = int(round(days * SECONDS_PER_DAY / dt))
+        for _ in range(steps):
+            b.step()
+        torch.cuda.synchronize()
+        res[prec] = (h.cpu().numpy()[0], u.cpu().numpy()[0], (gpu.dsum(h[0], A) - m0) / m0, steps)
+    hd, ud, dd, steps = res['double']
+    hm, um, dm, _ = res['mixed']
+    le_de = g.le * g.de
+    return dict(level=level, days=days, steps=steps, h_l2=l2rel(g.areaCell, hm, hd), u_l2=l2rel(le_de, um, ud),
+                h_linf=linf(hm, hd), u_linf=linf(um, ud), mass_drift_mixed=float(dm), mass_drift_double=float(dd))
