@@ -102,6 +102,9 @@ typedef struct isw_layers_params {
   const double *wall;
   double shelf;
   int shelf_bed;
+  /* FP64 Boussinesq layers without options step through a private one-stack batch (tiled fast loop, one graph per
+   * step; bit-identical results); percall != 0 keeps the per-call kernels (two grid-wide passes per fast sub-step). */
+  int percall;
 } isw_layers_params;
 
 /* Per-step fields of the option branches (reference attributes Layers.sig / .zm, .tide, .cbot, .cd_bot set by the ocean

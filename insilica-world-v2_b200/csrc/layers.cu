@@ -397,6 +397,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.cw = dalloc(s, (size_t)N * 6);
     d.hold = dalloc(s, (size_t)L * N);
     d.thin_wind = p->thin_wind;
+    s->percall = p->percall != 0;
     if (p->wall) {
       double *w = dalloc(s, E);
       ISW_CUDA(cudaMemcpy(w, p->wall, sizeof(double) * E, cudaMemcpyHostToDevice));
@@ -447,8 +448,10 @@ void layers_destroy(isw_layers *s) {
   delete s;
 }
 
-// The mixed form call by call: a private batch holding this one stack (rebuilt when the arrays, dt or nfast change).
-void layers_step_mixed(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
+// A step call by call through a private batch holding this one stack (rebuilt when the arrays, dt or nfast change): the
+// tiled fast loop and one graph per step. The mixed form always steps this way; the FP64 form does when the stack has
+// no air and no option branches, with bit-identical results.
+void layers_step_solo(isw_layers *s, double *h, double *u, double *Fm, double dt, int nfast, cudaStream_t st) {
   auto ok = [](int rc) { if (rc != ISW_OK) fail(rc, isw_last_error()); };
   if (!s->solo) ok(isw_batch_create(s->grid->device, &s->solo));
   if (!Fm) {
@@ -475,8 +478,21 @@ void layers_step(isw_layers *s, double *h, double *u, double *Fm, double *theta,
   if (!s->d.air && theta) fail(ISW_EINVAL, "layers.step: theta is for air layers");
   if (s->d.nu4 != 0) s->nu4dt = s->d.nu4 * dt;   // the step's nabla^4 loss, booked as heat by an air exchange
   if (s->d.precision == ISW_MIXED) {
-    layers_step_mixed(s, h, u, Fm, dt, nfast, st);
+    layers_step_solo(s, h, u, Fm, dt, nfast, st);
     return;
+  }
+  const LayersDev &D = s->d;
+  if (!s->percall && !D.air && !D.wall && !D.ob && !(D.shelf > 0) && !D.sig && !D.tide && !D.cbot && !(D.cd_bot > 0)) {
+    cudaStreamCaptureStatus cs0 = cudaStreamCaptureStatusNone;
+    ISW_CUDA(cudaStreamIsCapturing(st, &cs0));
+    const GraphEntry &k = s->solo_key;
+    const bool ready = s->solo && s->solo_slot >= 0 && k.h == h && k.u == u && k.dt == dt && k.nfast == nfast &&
+                       (Fm ? k.Fm == Fm : k.Fm == s->solo_Fm);
+    // (inside a capture of the caller's the batch cannot be built: the per-call kernels below give the same bits)
+    if (cs0 == cudaStreamCaptureStatusNone || ready) {
+      layers_step_solo(s, h, u, Fm, dt, nfast, st);
+      return;
+    }
   }
   auto enqueue = [&](cudaStream_t q) {
     if (s->d.air) enqueue_step_air(s, h, u, Fm, theta, dt, nfast, q);

@@ -31,7 +31,8 @@ class LayersParams(ctypes.Structure):
     _fields_ = [('L', I), ('grav', D), ('gprime', P), ('drag', P), ('stress', P),
                 ('nu4', D), ('floor_', D), ('rotation', D), ('div_damp', D), ('thin', D), ('vmix', D), ('vmix_cd', D),
                 ('b', P), ('precision', I), ('air', I), ('cp', D), ('kappa', D), ('rd', D), ('p0', D),
-                ('thin_wind', D), ('wall', P), ('shelf', D), ('shelf_bed', I)]
+                ('thin_wind', D), ('wall', P), ('shelf', D), ('shelf_bed', I),
+                ('percall', I)]
 
 
 def _sig(name, res, args):

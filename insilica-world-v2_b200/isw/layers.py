@@ -29,7 +29,10 @@ KAPPA = R_DRY / CP_DRY
 class Layers:
     def __init__(self, dg, layers=1, b=None, grav=GRAV, gprime=(), drag=0.0, stress=0.0, nu4=0.0, floor=1.0, rotation=1.0,
                  div_damp=DIV_DAMP, air=None, vmix=0.0, thin=2.0, wall=None, thin_wind=0.0, shelf=0.0, vmix_cd=0.0,
-                 shelf_bed=False):
+                 shelf_bed=False, batched=True):
+        """The reference's constructor (layers.py:36-37). batched (this core's): FP64 Boussinesq layers without option
+        branches step through a private one-stack batch (tiled fast loop, one graph; bit-identical results); False keeps
+        the per-call kernels."""
         if (wall is not None or shelf or shelf_bed) and dg.mixed:
             raise NotImplementedError('Layers: walls and the shelf run in the FP64 form only')
         assert wall is None or not air, 'walls are for Boussinesq layers'
@@ -65,7 +68,7 @@ class Layers:
                               b=_lib.host_ptr(self._b_host), precision=self.precision, air=1 if air else 0,
                               cp=float(self.cpa), kappa=float(self.kap), rd=float(self.rda), p0=P0,
                               thin_wind=float(thin_wind), wall=_lib.host_ptr(self._wall) if self._wall is not None else None,
-                              shelf=float(shelf), shelf_bed=1 if shelf_bed else 0)
+                              shelf=float(shelf), shelf_bed=1 if shelf_bed else 0, percall=0 if batched else 1)
         h = ctypes.c_void_p()
         _lib.check(_lib.isw_layers_create(dg.handle, ctypes.byref(p), ctypes.byref(h)))
         self._h = h

@@ -28,7 +28,7 @@ def make_stack(dg, z, dev):
     from isw.transport import Transport
     L = int(z['L'])
     core = Layers(dg, L, b=z['b'], gprime=list(z['gprime']), stress=list(z['stress']), nu4=float(z['nu4']),
-                  floor=float(z['floor']), vmix=float(z['vmix']))
+                  floor=float(z['floor']), vmix=float(z['vmix']), batched=False)   # call by call: the per-call kernels
     tr = Transport(dg, layers=L, tracers=3)
     st = dict(core=core, tr=tr, h=T(z['h0'], dev), u=T(z['u0'], dev))
     st['M'] = T(z['h0'] * dg.host.areaCell[None], dev)

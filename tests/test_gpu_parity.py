@@ -169,6 +169,18 @@ def test_graph_capture_equals_direct(dev, isw, grid4):
         a.step(ha, ua, 900.0, 2)
     torch.cuda.synchronize()
     assert torch.equal(ha, hb) and torch.equal(ua, ub)
+    # a first step inside the capture (the private batch cannot be built there: the per-call kernels are captured)
+    c = layers.Layers(dg, 1, b=z['b'])
+    hc, uc = T(z['h0'], dev), T(z['u0'], dev)
+    with torch.cuda.stream(s):
+        g2 = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g2, stream=s):
+            c.step(hc, uc, 900.0, 2)
+    torch.cuda.synchronize()
+    for _ in range(11):
+        g2.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(ha, hc) and torch.equal(ua, uc)
 
 
 def test_two_equal_layers_equal_one(dev, isw, grid4):
