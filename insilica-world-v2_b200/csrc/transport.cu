@@ -2,15 +2,14 @@
 // kernels/trisk.cu:48-59), plain FP64 form, and the Transport part of the C ABI.
 //
 // Rows y = tracer j * L + layer l, as the reference stacks them; row y's tracer values live in the caller's own array
-// tracers[j] + l * N (no packed copy). The reference's 8 launches per call (td, 2 x (hflux, stage), aflux, ratios,
-// apply) become 4 cell passes: every 3rd-order edge flux is recomputed by the cell pass that sums it, with the
-// reference's arithmetic, so results are bit-identical:
-// Threads are (tracer, cell) pairs, each over every layer of its tracer (transport_fp64.cuh).
-//   P1  td (fused.cu:146-160) and the first RK stage p1 (fused.cu:163-186, frac 1/3, fluxes of psi)
-//   P2  the second RK stage p2 (frac 1/2, fluxes of p1)
-//   P3  antidiffusive fluxes A (fused.cu:189-194; stored by each edge's eI cell) and the Zalesak ratios (fused.cu:197-222)
-//   P4  the limited update (fused.cu:225-241), written into the caller's tracer arrays
-// Order 1 stops after td, which is copied out (the reference returns td).
+// tracers[j] + l * N (no packed copy). Order 3 runs each RK stage as an edge pass (every 3rd-order edge flux computed
+// once, for all layers of a (tracer, edge)) and a cell pass summing them in the reference's edge order, then the
+// limited update: 7 launches against the reference's 8, bit-identical (transport_fp64.cuh).
+//   HF1 / C1  stage-1 fluxes of psi; td (fused.cu:146-160) and p1 (fused.cu:163-186, frac 1/3) with the caller's M1
+//   HF2 / C2  stage-2 fluxes of p1; p2 (frac 1/2)
+//   A / C3    antidiffusive fluxes (fused.cu:189-194) and the Zalesak ratios (fused.cu:197-222)
+//   P4        the limited update (fused.cu:225-241), written into the caller's tracer arrays
+// Order 1 is td alone, copied out (the reference returns td): one cell pass (tr_p1).
 #include <cstring>
 
 #include "common.cuh"
@@ -50,16 +49,34 @@ __global__ void __launch_bounds__(THREADS) k_p1(const TransportDev T, const TrAr
   ISW_TR_L(a.L, fp64::tr_p1<LL>(T, a, order, false, t / T.g.N, t % T.g.N));
 }
 
-__global__ void __launch_bounds__(THREADS) k_p2(const TransportDev T, const TrArgs a, int ntr) {
+__global__ void __launch_bounds__(THREADS) k_hf(const TransportDev T, const TrArgs a, int ntr, int stage) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= T.g.N * ntr) return;
-  ISW_TR_L(a.L, fp64::tr_p2<LL>(T, a, t / T.g.N, t % T.g.N));
+  if (t >= T.g.E * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_hf_edge<LL>(T, a, stage, t / T.g.E, t % T.g.E));
 }
 
-__global__ void __launch_bounds__(THREADS) k_p3(const TransportDev T, const TrArgs a, int ntr) {
+__global__ void __launch_bounds__(THREADS) k_aflux(const TransportDev T, const TrArgs a, int ntr) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T.g.E * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_a_edge<LL>(T, a, t / T.g.E, t % T.g.E));
+}
+
+__global__ void __launch_bounds__(THREADS) k_c1(const TransportDev T, const TrArgs a, int ntr) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T.g.N * ntr) return;
-  ISW_TR_L(a.L, fp64::tr_p3<LL>(T, a, t / T.g.N, t % T.g.N));
+  ISW_TR_L(a.L, fp64::tr_c1<LL>(T, a, t / T.g.N, t % T.g.N, false));
+}
+
+__global__ void __launch_bounds__(THREADS) k_c2(const TransportDev T, const TrArgs a, int ntr) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_c2<LL>(T, a, t / T.g.N, t % T.g.N));
+}
+
+__global__ void __launch_bounds__(THREADS) k_c3(const TransportDev T, const TrArgs a, int ntr) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T.g.N * ntr) return;
+  ISW_TR_L(a.L, fp64::tr_c3<LL>(T, a, t / T.g.N, t % T.g.N));
 }
 
 __global__ void __launch_bounds__(THREADS) k_p4(const TransportDev T, const TrArgs a, int ntr) {
@@ -173,13 +190,17 @@ int isw_transport_step_many(isw_transport *t, const double *M0, const double *M1
       a.tr[j] = tracers[j];
     }
     cudaStream_t st = (cudaStream_t)stream;
-    const int nb = blocks_for((long long)t->d.g.N * ntr);
-    k_p1<<<nb, THREADS, 0, st>>>(t->d, a, ntr, order);
+    const int nb = blocks_for((long long)t->d.g.N * ntr), ne = blocks_for((long long)t->d.g.E * ntr);
     if (order == 1) {
+      k_p1<<<nb, THREADS, 0, st>>>(t->d, a, ntr, order);
       k_td_out<<<blocks_for((long long)t->d.g.N * a.rows), THREADS, 0, st>>>(t->d, a);
     } else {
-      k_p2<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
-      k_p3<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
+      k_hf<<<ne, THREADS, 0, st>>>(t->d, a, ntr, 1);
+      k_c1<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
+      k_hf<<<ne, THREADS, 0, st>>>(t->d, a, ntr, 2);
+      k_c2<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
+      k_aflux<<<ne, THREADS, 0, st>>>(t->d, a, ntr);
+      k_c3<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
       k_p4<<<nb, THREADS, 0, st>>>(t->d, a, ntr);
     }
     ISW_CUDA(cudaGetLastError());

@@ -145,98 +145,6 @@ __device__ __forceinline__ void tr_p1(const TransportDev &T, const TrArgs &a, in
 }
 
 template <int L>
-__device__ __forceinline__ void tr_p2(const TransportDev &T, const TrArgs &a, int j, int i) {
-  const GridDev &g = T.g;
-  const int N = g.N, E = g.E;
-  CellEdges c;
-  load_edges(g, i, c);
-  double s[L], mx[L];
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
-    s[l] = a.M0[om] * T.psi0[o];
-    mx[l] = a.M0[om];
-  }
-  const double frac = 1.0 / 2.0;
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const int e = c.e[q];
-    if (e >= 0) {
-      const bool out = c.a[q] == i;
-      Stencil stn;
-      load_stencil(g, e, stn);
-#pragma unroll
-      for (int l = 0; l < L; l++) {
-        const double *p1 = T.p1 + (size_t)(j * L + l) * N;
-        const double f = a.Fm[(size_t)l * E + e];
-        const double hf = frac * hoflux_s(f, p1, stn, p1[c.a[q]], p1[c.b[q]], a.beta);
-        const double m = frac * f;
-        if (out) { s[l] -= hf; mx[l] -= m; } else { s[l] += hf; mx[l] += m; }
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < L; l++) T.p2[(size_t)(j * L + l) * N + i] = s[l] / mx[l];
-}
-
-template <int L>
-__device__ __forceinline__ void tr_p3(const TransportDev &T, const TrArgs &a, int j, int i) {
-  const GridDev &g = T.g;
-  const int N = g.N, E = g.E;
-  CellEdges c;
-  load_edges(g, i, c);
-  int nb[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) nb[q] = g.nbr[i * 6 + q];
-  double Pp[L], Pm[L];
-#pragma unroll
-  for (int l = 0; l < L; l++) { Pp[l] = 0; Pm[l] = 0; }
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    const int e = c.e[q];
-    if (e >= 0) {
-      const bool out = c.a[q] == i;
-      Stencil stn;
-      load_stencil(g, e, stn);
-#pragma unroll
-      for (int l = 0; l < L; l++) {
-        const size_t row = (size_t)(j * L + l);
-        const double *p = T.psi0 + row * N;
-        const double *p2 = T.p2 + row * N;
-        const double f = a.Fm[(size_t)l * E + e];
-        const double A = hoflux_s(f, p2, stn, p2[c.a[q]], p2[c.b[q]], a.beta) - upwind_v(f, p[c.a[q]], p[c.b[q]]);
-        if (out) {
-          T.A[row * E + e] = A;
-          if (A > 0) Pm[l] += A; else Pp[l] -= A;
-        } else {
-          if (A > 0) Pp[l] += A; else Pm[l] -= A;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < L; l++) {
-    const size_t row = (size_t)(j * L + l);
-    const double *p = T.psi0 + row * N;
-    const double *tt = T.td + row * N;
-    const double ti = tt[i];
-    double hi = fmax(p[i], ti), lo = fmin(p[i], ti);
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-      const int jn = nb[q];
-      if (jn >= 0) {
-        hi = fmax(hi, fmax(p[jn], tt[jn]));
-        lo = fmin(lo, fmin(p[jn], tt[jn]));
-      }
-    }
-    const double m1 = a.M1[(size_t)l * N + i];
-    const double qmax = (hi - ti) * m1, qmin = (ti - lo) * m1;
-    T.Rp[row * N + i] = Pp[l] > 0 ? fmin(1.0, qmax / Pp[l]) : 0.0;
-    T.Rm[row * N + i] = Pm[l] > 0 ? fmin(1.0, qmin / Pm[l]) : 0.0;
-  }
-}
-
-template <int L>
 __device__ __forceinline__ void tr_p4(const TransportDev &T, const TrArgs &a, int j, int i) {
   const GridDev &g = T.g;
   const int N = g.N, E = g.E;
@@ -305,9 +213,10 @@ __device__ __forceinline__ void tr_a_edge(const TransportDev &T, const TrArgs &a
   }
 }
 
-// cell pass of stage 1: M1 (tracer 0 stores it), td, p1 from the stage-1 edge fluxes
+// cell pass of stage 1: td and p1 from the stage-1 edge fluxes; with_mass: M1 formed here (tracer 0 stores it), else
+// the caller's M1 (Transport.step_many after mass_after)
 template <int L>
-__device__ __forceinline__ void tr_c1(const TransportDev &T, const TrArgs &a, int j, int i) {
+__device__ __forceinline__ void tr_c1(const TransportDev &T, const TrArgs &a, int j, int i, bool with_mass = true) {
   const GridDev &g = T.g;
   const int N = g.N, E = g.E;
   CellEdges c;
@@ -344,8 +253,10 @@ __device__ __forceinline__ void tr_c1(const TransportDev &T, const TrArgs &a, in
 #pragma unroll
   for (int l = 0; l < L; l++) {
     const size_t om = (size_t)l * N + i, o = (size_t)(j * L + l) * N + i;
-    if (j == 0) a.M1[om] = m1[l];
-    T.td[o] = td[l] / m1[l];
+    double mm = m1[l];
+    if (with_mass) { if (j == 0) a.M1[om] = mm; }
+    else mm = a.M1[om];
+    T.td[o] = td[l] / mm;
     T.p1[o] = s[l] / mx[l];
   }
 }
