@@ -35,7 +35,59 @@ struct GridDev {
   const double *le, *de, *areaCell, *areaV, *fV, *kite, *w, *d2wt;
   const float *w32, *d2wt32, *le32, *de32, *rde32, *rle32, *rA32, *rAV32, *kite32;
   const double *rA, *rde, *rAV;   // FP64 reciprocals (mixed form multiplies where the reference divides)
+  const int *eoeP;                // the TRiSK rows (eoe, w) padded to EOE_MAX entries per edge, pads id 0 weight 0
+  const double *wP;
+  const float *wP32;
 };
+
+// A cell's six slots of a per-cell table (int32: 24-byte rows; int8: 6-byte rows). Each table is its own allocation,
+// so rows are 8-byte (int32) or 2-byte (int8) aligned: three vector loads instead of six scalar ones, which in a
+// thread-per-cell pass cuts the L1 sector lookups of the row from six per thread to three.
+__device__ __forceinline__ void slots6(const int *__restrict__ t, int i, int out[6]) {
+  const int2 *p = reinterpret_cast<const int2 *>(t + (size_t)i * 6);
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const int2 v = p[q];
+    out[2 * q] = v.x;
+    out[2 * q + 1] = v.y;
+  }
+}
+
+__device__ __forceinline__ void signs6(const int8_t *__restrict__ t, int i, int out[6]) {
+  const char2 *p = reinterpret_cast<const char2 *>(t + (size_t)i * 6);
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const char2 v = p[q];
+    out[2 * q] = (signed char)v.x;
+    out[2 * q + 1] = (signed char)v.y;
+  }
+}
+
+// Edge e's padded TRiSK row: ids as five 8-byte loads, weights as five 16-byte (FP64) or 8-byte (FP32) loads.
+__device__ __forceinline__ void trisk_row(const GridDev &g, int e, int ix[EOE_MAX], double wv[EOE_MAX]) {
+  static_assert(EOE_MAX % 2 == 0, "padded TRiSK rows are read in pairs");
+  const int2 *pi = reinterpret_cast<const int2 *>(g.eoeP + (size_t)e * EOE_MAX);
+  const double2 *pw = reinterpret_cast<const double2 *>(g.wP + (size_t)e * EOE_MAX);
+#pragma unroll
+  for (int q = 0; q < EOE_MAX / 2; q++) {
+    const int2 a = pi[q];
+    const double2 b = pw[q];
+    ix[2 * q] = a.x; ix[2 * q + 1] = a.y;
+    wv[2 * q] = b.x; wv[2 * q + 1] = b.y;
+  }
+}
+
+__device__ __forceinline__ void trisk_row(const GridDev &g, int e, int ix[EOE_MAX], float wv[EOE_MAX]) {
+  const int2 *pi = reinterpret_cast<const int2 *>(g.eoeP + (size_t)e * EOE_MAX);
+  const float2 *pw = reinterpret_cast<const float2 *>(g.wP32 + (size_t)e * EOE_MAX);
+#pragma unroll
+  for (int q = 0; q < EOE_MAX / 2; q++) {
+    const int2 a = pi[q];
+    const float2 b = pw[q];
+    ix[2 * q] = a.x; ix[2 * q + 1] = a.y;
+    wv[2 * q] = b.x; wv[2 * q + 1] = b.y;
+  }
+}
 
 // Scratch and parameters of one Layers object (reference layers.py:36-92), by value in kernel parameters.
 struct LayersDev {

@@ -191,6 +191,18 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     for (int e = 0; e < E; e++) rle[e] = 1.0 / h->le[e];
     d.rle32 = upload_f32(g, rle.data(), E);
     d.kite32 = upload_f32(g, h->kite, (size_t)N * 6);
+    // the TRiSK rows padded to EOE_MAX entries per edge (pads: edge 0, weight 0, never summed): rows start on 8-byte
+    // (ids, FP32 weights) and 16-byte (FP64 weights) boundaries, so the slow tendency reads them as vectors
+    std::vector<int32_t> eoeP((size_t)E * EOE_MAX, 0);
+    std::vector<double> wP((size_t)E * EOE_MAX, 0.0);
+    for (int e = 0; e < E; e++)
+      for (int t = h->eoeStart[e]; t < h->eoeStart[e + 1]; t++) {
+        eoeP[(size_t)e * EOE_MAX + (t - h->eoeStart[e])] = h->eoe[t];
+        wP[(size_t)e * EOE_MAX + (t - h->eoeStart[e])] = h->w[t];
+      }
+    d.eoeP = upload(g, eoeP.data(), eoeP.size());
+    d.wP = upload(g, wP.data(), wP.size());
+    d.wP32 = upload_f32(g, wP.data(), wP.size());
     g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
     g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);
     g->h_cellSign.assign(h->cellSign, h->cellSign + (size_t)N * 6);

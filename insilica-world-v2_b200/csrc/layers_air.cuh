@@ -71,10 +71,10 @@ __device__ __forceinline__ void air_bern_cell(const LayersDev &M, const double *
   for (int k = L - 1; k >= 0; k--) { ph += M.S[(size_t)k * N + i] * P[k]; Phi[k] = ph; }
   int es[6];
   double c[6];
+  slots6(g.cellEdge, i, es);
 #pragma unroll
   for (int t = 0; t < 6; t++) {
-    const int e = g.cellEdge[i * 6 + t];
-    es[t] = e;
+    const int e = es[t];
     c[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
   }
   const double A = g.areaCell[i];
@@ -117,11 +117,13 @@ __device__ __forceinline__ void af_muphi_cell(const LayersDev &M, double tau, in
   const int N = g.N, E = g.E;
   int es[6];
   double c[6];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    es[s] = e;
-    c[s] = e >= 0 ? (double)g.cellSign[i * 6 + s] * g.le[e] : 0.0;
+    const int e = es[s];
+    c[s] = e >= 0 ? (double)sg[s] * g.le[e] : 0.0;
   }
   const double A = g.areaCell[i];
   double P[L];
@@ -171,8 +173,7 @@ __device__ __forceinline__ void air_scale_cell(const LayersDev &M, const StageAr
 #pragma unroll
   for (int k = 0; k < L; k++) out[k] = 0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdgeAsc[i * 6 + s];
+  slots6(g.cellEdgeAsc, i, es);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];

@@ -87,11 +87,13 @@ __device__ __forceinline__ void div_cell(const LayersDev &M, const double *__res
   const GridDev &g = M.g;
   int es[6];
   double c[6];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    es[s] = e;
-    c[s] = e >= 0 ? (double)g.cellSign[i * 6 + s] * g.le[e] : 0.0;
+    const int e = es[s];
+    c[s] = e >= 0 ? (double)sg[s] * g.le[e] : 0.0;
   }
   const double A = g.areaCell[i];
 #pragma unroll
@@ -151,10 +153,10 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
   for (int k = L - 1; k >= 0; k--) { s += h[(size_t)k * N + i]; z[k] = s; }
   int es[6];
   double c[6];
+  slots6(g.cellEdge, i, es);
 #pragma unroll
   for (int t = 0; t < 6; t++) {
-    const int e = g.cellEdge[i * 6 + t];
-    es[t] = e;
+    const int e = es[t];
     c[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
   }
   const double A = g.areaCell[i];
@@ -251,14 +253,14 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
   }
   // the row's neighbour ids and weights first (at most EOE_MAX, validated with the grid), then the gathers, all in
   // flight together; the sum runs in row order as the reference's loop does
-  const int m0 = g.eoeStart[e], cnt = g.eoeStart[e + 1] - m0;
+  const int cnt = g.eoeStart[e + 1] - g.eoeStart[e];
   int ix[EOE_MAX];
-#pragma unroll
-  for (int t = 0; t < EOE_MAX; t++) ix[t] = t < cnt ? g.eoe[m0 + t] : 0;
+  double wv[EOE_MAX];
+  trisk_row(g, e, ix, wv);
 #pragma unroll
   for (int t = 0; t < EOE_MAX; t++) {
     if (t < cnt) {
-      const double wm = g.w[m0 + t];
+      const double wm = wv[t];
       const double *pp = M.pk + (size_t)ix[t] * L * 3;
 #pragma unroll
       for (int k = 0; k < L; k++) {
@@ -290,7 +292,7 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
       // tide's drag (reference layers.cu:303-311)
       if (M.cd_bot > 0) {
         double vt = 0;
-        for (int t = 0; t < cnt; t++) vt += g.w[m0 + t] * M.pk[((size_t)ix[t] * L + k) * 3 + 1];
+        for (int t = 0; t < cnt; t++) vt += wv[t] * M.pk[((size_t)ix[t] * L + k) * 3 + 1];
         ck += M.cd_bot * sqrt(ue * ue + vt * vt);
       }
       if (M.cbot) ck += M.cbot[e];
@@ -346,13 +348,14 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, double tau, int 
   const double e0 = M.eta[i];
   M.eta_prev[i] = e0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
   double div = 0;
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
-    if (e >= 0) div += (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] * M.ub[e];
+    if (e >= 0) div += (double)sg[s] * g.le[e] * M.He[e] * M.ub[e];
   }
   M.eta[i] = e0 - (tau * div) / g.areaCell[i];
 }
@@ -380,15 +383,16 @@ __device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, in
   const GridDev &g = M.g;
   const double e0 = M.eta[i];
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
   // the slot coefficients sign l_e H_e are constant over the stage's sub-steps: formed by sub-step 0, then read back
   double c[6];
   if (j == 0) {
 #pragma unroll
     for (int s = 0; s < 6; s++) {
       const int e = es[s];
-      c[s] = e >= 0 ? (double)g.cellSign[i * 6 + s] * g.le[e] * M.He[e] : 0.0;
+      c[s] = e >= 0 ? (double)sg[s] * g.le[e] * M.He[e] : 0.0;
       M.cw[(size_t)i * 6 + s] = c[s];
     }
   } else {
@@ -423,8 +427,7 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &
 #pragma unroll
   for (int k = 0; k < L; k++) out[k] = 0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdgeAsc[i * 6 + s];
+  slots6(g.cellEdgeAsc, i, es);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
@@ -467,13 +470,14 @@ __device__ __forceinline__ void h_cell(const LayersDev &M, const StageArgs &a, i
 #pragma unroll
   for (int k = 0; k < L; k++) div[k] = 0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
     if (e < 0) continue;
-    const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
+    const double c = (double)sg[s] * g.le[e];
 #pragma unroll
     for (int k = 0; k < L; k++) div[k] += c * limited(M, k, e);
   }

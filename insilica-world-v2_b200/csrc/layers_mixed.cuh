@@ -52,11 +52,13 @@ __device__ __forceinline__ void div_cell(const LayersDev &M, const T *__restrict
   const GridDev &g = M.g;
   int es[6];
   float c[6];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdge[i * 6 + s];
-    es[s] = e;
-    c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] : 0.f;
+    const int e = es[s];
+    c[s] = e >= 0 ? (float)sg[s] * g.le32[e] : 0.f;
   }
   const float rA = g.rA32[i];
 #pragma unroll
@@ -116,10 +118,10 @@ __device__ __forceinline__ void bern_cell(const LayersDev &M, const double *__re
   for (int k = L - 1; k >= 0; k--) { s += h[(size_t)k * N + i]; z[k] = s; }
   int es[6];
   float c[6];
+  slots6(g.cellEdge, i, es);
 #pragma unroll
   for (int t = 0; t < 6; t++) {
-    const int e = g.cellEdge[i * 6 + t];
-    es[t] = e;
+    const int e = es[t];
     c[t] = e >= 0 ? g.le32[e] * g.de32[e] * 0.25f : 0.f;
   }
   const float rA = g.rA32[i];
@@ -202,14 +204,14 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
     qf[k] = p.z;
     Q[k] = 0.f;
   }
-  const int m0 = g.eoeStart[e], cnt = g.eoeStart[e + 1] - m0;
+  const int cnt = g.eoeStart[e + 1] - g.eoeStart[e];
   int ix[EOE_MAX];
-#pragma unroll
-  for (int t = 0; t < EOE_MAX; t++) ix[t] = t < cnt ? g.eoe[m0 + t] : 0;
+  float wv[EOE_MAX];
+  trisk_row(g, e, ix, wv);
 #pragma unroll
   for (int t = 0; t < EOE_MAX; t++) {
     if (t < cnt) {
-      const float wm = g.w32[m0 + t];
+      const float wm = wv[t];
       const float4 *pp = M.pk4 + (size_t)ix[t] * L;
 #pragma unroll
       for (int k = 0; k < L; k++) {
@@ -256,15 +258,16 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
   const GridDev &g = M.g;
   int es[6];
   float c[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
   float c0;
   if (j == 0) {                              // slot coefficients sign l_e H_e and c0, constant over the stage
     c0 = 0.f;
 #pragma unroll
     for (int s = 0; s < 6; s++) {
       const int e = es[s];
-      c[s] = e >= 0 ? (float)g.cellSign[i * 6 + s] * g.le32[e] * M.He32[e] : 0.f;
+      c[s] = e >= 0 ? (float)sg[s] * g.le32[e] * M.He32[e] : 0.f;
       M.cw32[(size_t)i * 6 + s] = c[s];
       if (e >= 0) c0 += c[s] * (float)M.ub0[e];
     }
@@ -301,8 +304,7 @@ __device__ __forceinline__ void scale_cell(const LayersDev &M, const MStageArgs 
 #pragma unroll
   for (int k = 0; k < L; k++) out[k] = 0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdgeAsc[i * 6 + s];
+  slots6(g.cellEdgeAsc, i, es);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
@@ -348,13 +350,14 @@ __device__ __forceinline__ void h_cell(const LayersDev &M, const MStageArgs &a, 
 #pragma unroll
   for (int k = 0; k < L; k++) div[k] = 0;
   int es[6];
-#pragma unroll
-  for (int s = 0; s < 6; s++) es[s] = g.cellEdge[i * 6 + s];
+  slots6(g.cellEdge, i, es);
+  int sg[6];
+  signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
     if (e < 0) continue;
-    const double c = (double)g.cellSign[i * 6 + s] * g.le[e];
+    const double c = (double)sg[s] * g.le[e];
 #pragma unroll
     for (int k = 0; k < L; k++) div[k] += c * limited(M, k, e);
   }

@@ -42,13 +42,22 @@ struct Stencil {
   double wt[8];
 };
 
+// The tables hold 8 entries per edge (32-byte index rows, 64-byte weight rows, each table its own allocation), so the
+// row is read as 8- and 16-byte vectors: a third of the L1 sector lookups of scalar loads in a thread-per-edge pass.
 __device__ __forceinline__ void load_stencil(const GridDev &g, int e, Stencil &st) {
-  st.o[0] = g.d2idx[e * 8 + 2];
-  st.o[1] = g.d2idx[e * 8 + 3];
-  st.o[2] = g.d2idx[e * 8 + 6];
-  st.o[3] = g.d2idx[e * 8 + 7];
+  const int2 lo = *reinterpret_cast<const int2 *>(g.d2idx + (size_t)e * 8 + 2);
+  const int2 hi = *reinterpret_cast<const int2 *>(g.d2idx + (size_t)e * 8 + 6);
+  st.o[0] = lo.x;
+  st.o[1] = lo.y;
+  st.o[2] = hi.x;
+  st.o[3] = hi.y;
+  const double2 *w = reinterpret_cast<const double2 *>(g.d2wt + (size_t)e * 8);
 #pragma unroll
-  for (int q = 0; q < 8; q++) st.wt[q] = g.d2wt[e * 8 + q];
+  for (int q = 0; q < 4; q++) {
+    const double2 v = w[q];
+    st.wt[2 * q] = v.x;
+    st.wt[2 * q + 1] = v.y;
+  }
 }
 
 // The 3rd-order flux of an edge (reference fused.cu:131-138, FP64 form: the stencil reads the 64-bit field itself):
@@ -71,10 +80,10 @@ struct CellEdges {
 };
 
 __device__ __forceinline__ void load_edges(const GridDev &g, int i, CellEdges &c) {
+  slots6(g.cellEdgeAsc, i, c.e);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
-    const int e = g.cellEdgeAsc[i * 6 + s];
-    c.e[s] = e;
+    const int e = c.e[s];
     c.a[s] = e >= 0 ? g.eI[e] : 0;
     c.b[s] = e >= 0 ? g.eJ[e] : 0;
   }
@@ -300,11 +309,8 @@ __device__ __forceinline__ void tr_c3(const TransportDev &T, const TrArgs &a, in
   const GridDev &g = T.g;
   const int N = g.N, E = g.E;
   int es[6], nb[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    es[q] = g.cellEdgeAsc[i * 6 + q];
-    nb[q] = g.nbr[i * 6 + q];
-  }
+  slots6(g.cellEdgeAsc, i, es);
+  slots6(g.nbr, i, nb);
   bool out[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = es[q] >= 0 && g.eI[es[q]] == i;

@@ -20,12 +20,16 @@ struct Stencil32 {
 };
 
 __device__ __forceinline__ void load_stencil(const GridDev &g, int e, Stencil32 &st) {
-  st.o[0] = g.d2idx[e * 8 + 2];
-  st.o[1] = g.d2idx[e * 8 + 3];
-  st.o[2] = g.d2idx[e * 8 + 6];
-  st.o[3] = g.d2idx[e * 8 + 7];
-#pragma unroll
-  for (int q = 0; q < 8; q++) st.wt[q] = g.d2wt32[e * 8 + q];
+  const int2 lo = *reinterpret_cast<const int2 *>(g.d2idx + (size_t)e * 8 + 2);
+  const int2 hi = *reinterpret_cast<const int2 *>(g.d2idx + (size_t)e * 8 + 6);
+  st.o[0] = lo.x;
+  st.o[1] = lo.y;
+  st.o[2] = hi.x;
+  st.o[3] = hi.y;
+  const float4 *w = reinterpret_cast<const float4 *>(g.d2wt32 + (size_t)e * 8);
+  const float4 a = w[0], b = w[1];
+  st.wt[0] = a.x; st.wt[1] = a.y; st.wt[2] = a.z; st.wt[3] = a.w;
+  st.wt[4] = b.x; st.wt[5] = b.y; st.wt[6] = b.z; st.wt[7] = b.w;
 }
 
 // f (mean - x - y) + |f| (y - x) beta: the mean part in FP64, the curvature correction in FP32.
@@ -197,11 +201,8 @@ __device__ __forceinline__ void tr_c3(const TransportDev &T, const TrArgs &a, in
   const GridDev &g = T.g;
   const int N = g.N, E = g.E;
   int es[6], nb[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) {
-    es[q] = g.cellEdgeAsc[i * 6 + q];
-    nb[q] = g.nbr[i * 6 + q];
-  }
+  slots6(g.cellEdgeAsc, i, es);
+  slots6(g.nbr, i, nb);
   bool out[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) out[q] = es[q] >= 0 && g.eI[es[q]] == i;
