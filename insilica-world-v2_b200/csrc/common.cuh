@@ -14,6 +14,9 @@ constexpr int LMAX = 8;          // layers per column (reference layers.py:30)
 constexpr int TRMAX = 16;        // tracers moved in one transport call
 constexpr int THREADS = 256;     // threads per block of the phase kernels
 constexpr int EOE_MAX = 10;      // TRiSK row length: the other edges of an edge's two cells (5 + 5 on hexagons)
+// The FP64 packed edge record: per edge, (h_e, u, q_e) of each layer, the edge's row padded to an even count of
+// doubles so that every row starts on a 16-byte boundary and is read as 16-byte pairs.
+__host__ __device__ constexpr int pk_stride(int L) { return (3 * L + 1) & ~1; }
 
 // Thrown inside the library, turned into a status at the C ABI.
 struct Error {

@@ -392,7 +392,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
     d.eta0 = dalloc(s, N); d.eta = dalloc(s, N); d.eta_prev = dalloc(s, N);
     d.h1 = dalloc(s, (size_t)L * N); d.h2 = dalloc(s, (size_t)L * N); d.u1 = dalloc(s, (size_t)L * E); d.u2 = dalloc(s, (size_t)L * E);
     d.D1 = dalloc(s, (size_t)L * N); d.Z1 = dalloc(s, (size_t)L * NV); d.L1 = dalloc(s, (size_t)L * E); d.L2 = dalloc(s, (size_t)L * E);
-    d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)3 * L * E);
+    d.hedge = dalloc(s, (size_t)L * E); d.diss = dalloc(s, E); d.pk = dalloc(s, (size_t)pk_stride(L) * E);
     d.ub2 = dalloc(s, E);
     d.cw = dalloc(s, (size_t)N * 6);
     d.hold = dalloc(s, (size_t)L * N);

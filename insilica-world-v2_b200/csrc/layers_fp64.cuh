@@ -221,17 +221,22 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
   const GridDev &g = M.g;
   const int N = g.N, E = g.E, NV = g.NV;
   const int a = g.eI[e], b = g.eJ[e], v1 = g.ev1[e], v2 = g.ev2[e];
-  double *pp = M.pk + (size_t)e * L * 3;
+  constexpr int PS = pk_stride(L);
+  double r[PS];
+  r[PS - 1] = 0.0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const size_t o = (size_t)k * E + e;
     const double hv = edge_hk<OPT>(M, k, a, b, h[(size_t)k * N + a], h[(size_t)k * N + b]);
     const double qv = 0.5 * (M.q[(size_t)k * NV + v1] + M.q[(size_t)k * NV + v2]);
     M.hedge[o] = hv;
-    pp[k * 3 + 0] = hv;
-    pp[k * 3 + 1] = u[o];
-    pp[k * 3 + 2] = qv;
+    r[k * 3 + 0] = hv;
+    r[k * 3 + 1] = u[o];
+    r[k * 3 + 2] = qv;
   }
+  double2 *pp = reinterpret_cast<double2 *>(M.pk + (size_t)e * PS);
+#pragma unroll
+  for (int q = 0; q < PS / 2; q++) pp[q] = make_double2(r[2 * q], r[2 * q + 1]);
   M.ub[e] = M.ub0[e];
   M.acc[e] = 0.0;
 }
@@ -243,7 +248,8 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
   double he[L], cap[L], qf[L], Q[L];
-  const double *pe = M.pk + (size_t)e * L * 3;
+  constexpr int PS = pk_stride(L);
+  const double *pe = M.pk + (size_t)e * PS;
 #pragma unroll
   for (int k = 0; k < L; k++) {
     he[k] = M.hedge[(size_t)k * E + e];
@@ -261,13 +267,20 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
   for (int t = 0; t < EOE_MAX; t++) {
     if (t < cnt) {
       const double wm = wv[t];
-      const double *pp = M.pk + (size_t)ix[t] * L * 3;
+      const double2 *pp = reinterpret_cast<const double2 *>(M.pk + (size_t)ix[t] * PS);
+      double r[PS];
+#pragma unroll
+      for (int q = 0; q < PS / 2; q++) {
+        const double2 v = pp[q];
+        r[2 * q] = v.x;
+        r[2 * q + 1] = v.y;
+      }
 #pragma unroll
       for (int k = 0; k < L; k++) {
-        double h2 = pp[k * 3 + 0];
+        double h2 = r[k * 3 + 0];
         if (h2 > cap[k]) h2 = cap[k];
-        const double F2 = h2 * pp[k * 3 + 1];
-        Q[k] += wm * F2 * 0.5 * (qf[k] + pp[k * 3 + 2]);
+        const double F2 = h2 * r[k * 3 + 1];
+        Q[k] += wm * F2 * 0.5 * (qf[k] + r[k * 3 + 2]);
       }
     }
   }
@@ -292,7 +305,7 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
       // tide's drag (reference layers.cu:303-311)
       if (M.cd_bot > 0) {
         double vt = 0;
-        for (int t = 0; t < cnt; t++) vt += wv[t] * M.pk[((size_t)ix[t] * L + k) * 3 + 1];
+        for (int t = 0; t < cnt; t++) vt += wv[t] * M.pk[(size_t)ix[t] * PS + k * 3 + 1];
         ck += M.cd_bot * sqrt(ue * ue + vt * vt);
       }
       if (M.cbot) ck += M.cbot[e];
