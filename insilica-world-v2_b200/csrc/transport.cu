@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(THREADS) k_td_out(const TransportDev T, const 
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T.g.N * a.rows) return;
   const int y = t / T.g.N, i = t - y * T.g.N, l = y % a.L, j = y / a.L;
-  a.tr[j][(size_t)l * T.g.N + i] = T.td[(size_t)y * T.g.N + i];
+  a.tr[j][(size_t)l * T.g.N + i] = T.td[fx(j, T.g.N, i, a.L) + l];
 }
 
 }  // namespace
@@ -140,9 +140,9 @@ int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int preci
     t->precision = precision;
     t->beta = beta;
     try {
-      const size_t R = (size_t)L * tracers, N = g->d.N, E = g->d.E;
+      const size_t R = (size_t)lp_of(L) * tracers, N = g->d.N, E = g->d.E;   // layers side by side, padded to even
       t->d.g = g->d;
-      t->d.psi0 = talloc(t, R * N); t->d.td = talloc(t, R * N); t->d.p1 = talloc(t, R * N); t->d.p2 = talloc(t, R * N);
+      t->d.td = talloc(t, R * N); t->d.p1 = talloc(t, R * N); t->d.p2 = talloc(t, R * N);
       t->d.Rp = talloc(t, R * N); t->d.Rm = talloc(t, R * N); t->d.A = talloc(t, R * E);
       if (precision == ISW_MIXED) {            // the batched step's mixed FCT: FP32 stage fields, fluxes and ratios
         auto f = [&](size_t n) { return reinterpret_cast<float *>(talloc(t, (n + 1) / 2)); };
