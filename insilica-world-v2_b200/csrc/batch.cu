@@ -82,13 +82,10 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], j, i);
   } else if (PH == PH_U) {
-    if (!d.tiled && j < d.n[st]) {
-      fp64::bt_u_edge_y(M, d.tau[st], i);
-      if (j == d.n[st] - 1) fp64::flux_edge<false>(M, stage_args(d, st), M.acc[i], i);
-    }
+    if (!d.tiled && j < d.n[st]) fp64::bt_u_edge_y(M, d.tau[st], i);
   } else if (PH == PH_C) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::scale_cell<LL, false>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
@@ -229,12 +226,9 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
     }
   }
   __syncthreads();
-  const StageArgs sa = stage_args(d, st);
   for (int e = threadIdx.x; e < eown; e += blockDim.x) {
-    const int ge = edges[e];
-    M.ub[ge] = EA[e].y;
-    M.acc[ge] = acc[e];
-    fp64::flux_edge<false>(M, sa, acc[e], ge);
+    M.ub[edges[e]] = EA[e].y;
+    M.acc[edges[e]] = acc[e];
   }
 }
 
