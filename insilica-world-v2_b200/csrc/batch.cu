@@ -81,11 +81,17 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i));
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], j, i);
-  } else if (PH == PH_U) {
-    if (!d.tiled && j < d.n[st]) fp64::bt_u_edge_y(M, d.tau[st], i);
+  } else if (PH == PH_U || PH == PH_UF) {
+    if (!d.tiled && j < d.n[st]) {
+      fp64::bt_u_edge_y(M, d.tau[st], i);
+      if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<false>(M, stage_args(d, st), M.acc[i], i);
+    }
   } else if (PH == PH_C) {
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::scale_cell<LL, false>(M, a, i));
+  } else if (PH == PH_CS) {
+    const StageArgs a = stage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
@@ -740,12 +746,15 @@ void enqueue_dyn(isw_batch *b, cudaStream_t st) {
     launch_phase<PH_S>(b, st, s, 0);
     const bool tiled = !b->groups.empty();
     launch_fast(b, st, s, DEFAULT_TIMEOUT_NS, -1);
+    // no tiled stack: the layer fluxes are formed in the last grid-wide sub-step, once per edge, and C sums them
     if (b->any_untiled)
       for (int j = 0; j < b->nsub[s]; j++) {
         launch_phase<PH_ETA>(b, st, s, j, !(tiled && j == 0));
-        launch_phase<PH_U>(b, st, s, j);
+        if (tiled) launch_phase<PH_U>(b, st, s, j);
+        else launch_phase<PH_UF>(b, st, s, j);
       }
-    launch_phase<PH_C>(b, st, s, 0, !tiled || b->any_untiled);
+    if (tiled) launch_phase<PH_C>(b, st, s, 0, b->any_untiled);
+    else launch_phase<PH_CS>(b, st, s, 0);
     launch_phase<PH_D>(b, st, s, 0);
   }
 }

@@ -74,11 +74,17 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
     ISW_BATCH_L(d.L, LMAXK, mixed::slow_edge<LL>(M, a.us, a.cdt, i));
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) mixed::bt_eta_cell(M, (float)d.tau[st], j, i);
-  } else if (PH == PH_U) {
-    if (!d.tiled && j < d.n[st]) mixed::bt_u_edge(M, (float)d.tau[st], i);
+  } else if (PH == PH_U || PH == PH_UF) {
+    if (!d.tiled && j < d.n[st]) {
+      mixed::bt_u_edge(M, (float)d.tau[st], i);
+      if (PH == PH_UF && j == d.n[st] - 1) mixed::flux_edge(M, mstage_args(d, st), M.acc[i], i);
+    }
   } else if (PH == PH_C) {
     const mixed::MStageArgs a = mstage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, mixed::scale_cell<LL>(M, a, i));
+  } else if (PH == PH_CS) {
+    const mixed::MStageArgs a = mstage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, mixed::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const mixed::MStageArgs a = mstage_args(d, st);
     if (kind == 0) ISW_BATCH_L(d.L, LMAXK, mixed::h_cell<LL>(M, a, i));
@@ -292,6 +298,8 @@ void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, con
     case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_U: launch_m<PH_U>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_C: launch_m<PH_C>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_UF: launch_m<PH_UF>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_CS: launch_m<PH_CS>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_D: launch_m<PH_D>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_POST: launch_m<PH_POST>(lmax, nb, st, pdl, desc, sc, stage, j); break;
     case PH_P2: launch_m<PH_P2>(lmax, nb, st, pdl, desc, sc, stage, j); break;

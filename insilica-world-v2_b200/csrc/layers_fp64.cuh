@@ -431,6 +431,54 @@ __device__ __forceinline__ void bt_u_edge_y(const LayersDev &M, double tau, int 
   M.ub[e] = v + tau * ((-(Y[g.eJ[e]] - Y[g.eI[e]])) / g.de[e] + M.G[e]);
 }
 
+// The layer fluxes of edge e once the stage's fast loop has finished (reference lay_flux, layers.cu:392-397), every
+// layer: F = h_e (u - ubar_s) + h_e acc / n, acc the sub-steps' sum of ubar. A batch with no tiled stack forms them in
+// the last grid-wide sub-step's edge pass, once per edge, and its phase C only sums them (scale_sum_cell); batches
+// with tiles recompute them in phase C (scale_cell: the tile kernel's tail has no spare parallelism for the gathers).
+template <bool OPT = true>
+__device__ __forceinline__ void flux_edge(const LayersDev &M, const StageArgs &a, double acc, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  const int ea = g.eI[e], eb = g.eJ[e];
+  const double ubs = M.ubs[e];
+  for (int k = 0; k < M.L; k++) {
+    const double he = edge_hk<OPT>(M, k, ea, eb, a.hs[(size_t)k * N + ea], a.hs[(size_t)k * N + eb]);
+    M.F[(size_t)k * E + e] = walled<OPT>(M, e) ? 0.0 : he * (a.us[(size_t)k * E + e] - ubs) + he * (acc * a.inv_n);
+  }
+}
+
+// phase C from the fluxes flux_edge stored: the same sums as scale_cell
+template <int L>
+__device__ __forceinline__ void scale_sum_cell(const LayersDev &M, const StageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double out[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) out[k] = 0;
+  int es[6];
+  slots6(g.cellEdgeAsc, i, es);
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = es[s];
+    if (e < 0) continue;
+    const bool mine = g.eI[e] == i;
+    const double le = g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const double f = M.F[(size_t)k * E + e] * le * a.cdt;
+      if (mine) { if (f > 0) out[k] += f; }
+      else if (!(f > 0)) out[k] -= f;
+    }
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double avail = a.h0[(size_t)k * N + i] - M.floor_;
+    const double cap = (avail > 0 ? avail : 0.0) * A;
+    M.scale[(size_t)k * N + i] = out[k] > cap ? cap / out[k] : 1.0;
+  }
+}
+
 // ---- stage phase C: layer fluxes and the floor limiter's scale ----
 template <int L, bool OPT = true>
 __device__ __forceinline__ void scale_cell(const LayersDev &M, const StageArgs &a, int i) {

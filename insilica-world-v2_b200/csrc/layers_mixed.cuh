@@ -295,6 +295,55 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) 
   M.dub[e] = v + tau * (M.G32[e] - (Y[g.eJ[e]] - Y[g.eI[e]]) * g.rde32[e]);
 }
 
+// The layer fluxes of edge e in the last grid-wide sub-step of a batch with no tiled stack, every layer: F (FP64,
+// summed by scale_sum_cell) and its FP32 copy (the limited flux of phase D), acc the sub-steps' FP64 sum; the same
+// values scale_cell forms
+__device__ __forceinline__ void flux_edge(const LayersDev &M, const MStageArgs &a, double acc, int e) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  const int ea = g.eI[e], eb = g.eJ[e];
+  const float ubs = M.ubs32[e];
+  const double ubm = M.ub0[e] + acc * a.inv_n;
+  for (int k = 0; k < M.L; k++) {
+    const double he = 0.5 * (a.hs[(size_t)k * N + ea] + a.hs[(size_t)k * N + eb]);
+    const double F = he * ((double)(a.us[(size_t)k * E + e] - ubs) + ubm);
+    M.F[(size_t)k * E + e] = F;
+    M.F32[(size_t)k * E + e] = (float)F;
+  }
+}
+
+// phase C from the fluxes flux_edge stored: the same sums as scale_cell
+template <int L>
+__device__ __forceinline__ void scale_sum_cell(const LayersDev &M, const MStageArgs &a, int i) {
+  const GridDev &g = M.g;
+  const int N = g.N, E = g.E;
+  double out[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) out[k] = 0;
+  int es[6];
+  slots6(g.cellEdgeAsc, i, es);
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    const int e = es[s];
+    if (e < 0) continue;
+    const bool mine = g.eI[e] == i;
+    const double le = g.le[e];
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const double f = M.F[(size_t)k * E + e] * le * a.cdt;
+      if (mine) { if (f > 0) out[k] += f; }
+      else if (!(f > 0)) out[k] -= f;
+    }
+  }
+  const double A = g.areaCell[i];
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double avail = a.h0[(size_t)k * N + i] - M.floor_;
+    const double cap = (avail > 0 ? avail : 0.0) * A;
+    M.scale32[(size_t)k * N + i] = out[k] > cap ? __double2float_rz(cap / out[k]) : 1.f;   // rounded toward zero
+  }
+}
+
 // ---- stage phase C: layer fluxes (FP64) and the floor limiter ----
 template <int L>
 __device__ __forceinline__ void scale_cell(const LayersDev &M, const MStageArgs &a, int i) {
