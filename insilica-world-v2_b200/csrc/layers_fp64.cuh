@@ -397,11 +397,12 @@ __device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, in
   const double e0 = M.eta[i];
   int es[6];
   slots6(g.cellEdge, i, es);
-  int sg[6];
-  signs6(g.cellSign, i, sg);
   // the slot coefficients sign l_e H_e are constant over the stage's sub-steps: formed by sub-step 0, then read back
+  // (48-byte rows: three 16-byte loads)
   double c[6];
   if (j == 0) {
+    int sg[6];
+    signs6(g.cellSign, i, sg);
 #pragma unroll
     for (int s = 0; s < 6; s++) {
       const int e = es[s];
@@ -409,8 +410,13 @@ __device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, in
       M.cw[(size_t)i * 6 + s] = c[s];
     }
   } else {
+    const double2 *cw = reinterpret_cast<const double2 *>(M.cw + (size_t)i * 6);
 #pragma unroll
-    for (int s = 0; s < 6; s++) c[s] = M.cw[(size_t)i * 6 + s];
+    for (int q = 0; q < 3; q++) {
+      const double2 v = cw[q];
+      c[2 * q] = v.x;
+      c[2 * q + 1] = v.y;
+    }
   }
   double div = 0;
 #pragma unroll

@@ -259,10 +259,10 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
   int es[6];
   float c[6];
   slots6(g.cellEdge, i, es);
-  int sg[6];
-  signs6(g.cellSign, i, sg);
   float c0;
   if (j == 0) {                              // slot coefficients sign l_e H_e and c0, constant over the stage
+    int sg[6];
+    signs6(g.cellSign, i, sg);
     c0 = 0.f;
 #pragma unroll
     for (int s = 0; s < 6; s++) {
@@ -273,8 +273,13 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
     }
     M.c0[i] = c0;
   } else {
+    const float2 *cw = reinterpret_cast<const float2 *>(M.cw32 + (size_t)i * 6);   // 24-byte rows: three 8-byte loads
 #pragma unroll
-    for (int s = 0; s < 6; s++) c[s] = M.cw32[(size_t)i * 6 + s];
+    for (int q = 0; q < 3; q++) {
+      const float2 v = cw[q];
+      c[2 * q] = v.x;
+      c[2 * q + 1] = v.y;
+    }
     c0 = M.c0[i];
   }
   const float d0 = M.deta[i];
