@@ -14,6 +14,8 @@
  *   isw_layers_step_air        the same with theta: the air branch (layers.py:134-136, 152-166, 187-192, 203-206)
  *   isw_layers_update_gfast    src/insilica/layers.py:104-109 Layers.update_gfast(h, theta)
  *   isw_layers_exchange        src/insilica/layers.py:214-232 Layers.exchange(wx, h, u, M, psi, theta, seq)
+ *   isw_layers_set_option      the attributes Layers.sig / .tide / .cbot / .cd_bot (layers.py:36-40, 139-149), set by
+ *                              ocean.py:88-90, 159, 245 and tides.py:64-69
  *   isw_layers_substeps        src/insilica/layers.py:99-102 Layers.substeps(h, dt)
  *   isw_layers_lap             src/insilica/layers.py:123-127 Layers._lap(u, out)   (used by lap_max, :111-121)
  *   isw_transport_create       src/insilica/transport.py:19-30 Transport(dg, layers, beta, tracers)
@@ -40,7 +42,8 @@ enum {
   ISW_EINVAL = 1,        /* bad argument: null handle or pointer, size or shape mismatch, out-of-range index table */
   ISW_ECUDA = 2,         /* a CUDA runtime call failed (the message names it) */
   ISW_ENOMEM = 3,        /* device or host allocation failed at create time */
-  ISW_EUNSUPPORTED = 4,  /* an option of the reference API this build does not implement (air, walls, shelf, ...) */
+  ISW_EUNSUPPORTED = 4,  /* a combination this build does not run: air layers or option branches in the mixed form or
+                          * in a batch (they step in the FP64 form, call by call) */
   ISW_ETIMEOUT = 5,      /* a bounded device-side wait gave up (persistent kernels); the context stays usable */
   ISW_ENOTFINITE = 6     /* reserved: a NaN/Inf budget */
 };
@@ -81,8 +84,9 @@ typedef struct isw_grid_host {
   const uint8_t *eKi, *eKj;               /* E */
 } isw_grid_host;
 
-/* Layers options (reference layers.py:36-37). Boussinesq layers only: the air, wall, shelf, shelf_bed, sig/zm, tide and
- * cd_bot/cbot options are not implemented (ISW_EUNSUPPORTED when the Python facade is asked for them). */
+/* Layers options (reference layers.py:36-37): Boussinesq or air layers, with the option branches below and the per-step
+ * fields of isw_layers_set_option. Air layers and option branches run in the FP64 form, call by call; the mixed form and
+ * batches take Boussinesq layers without options (ISW_EUNSUPPORTED otherwise). */
 typedef struct isw_layers_params {
   int L;                                  /* 1 .. 8 */
   double grav;
