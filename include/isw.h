@@ -18,6 +18,11 @@
  *                              ocean.py:88-90, 159, 245 and tides.py:64-69
  *   isw_layers_substeps        src/insilica/layers.py:99-102 Layers.substeps(h, dt)
  *   isw_layers_lap             src/insilica/layers.py:123-127 Layers._lap(u, out)   (used by lap_max, :111-121)
+ *   isw_layers_vmix_heat       src/insilica/world.py:317-318  core.k['vmix_heat'](grid, block, args) after the sea
+ *                              coupling (kernel kernels/layers.cu:596-621)
+ *   isw_layers_mask            src/insilica/layers.py:94-97   Layers.mask(a, rows) (kernel kernels/layers.cu:495-499),
+ *                              called by ocean.py:125
+ *   isw_layers_status          none: the status word of the one-stack batch a Layers steps through
  *   isw_transport_create       src/insilica/transport.py:19-30 Transport(dg, layers, beta, tracers)
  *   isw_transport_mass_after   src/insilica/transport.py:32-35 Transport.mass_after(M0, Fm, M1)
  *   isw_transport_step_many    src/insilica/transport.py:40-71 Transport.step_many(M0, M1, Fm, tracers, order)
@@ -45,7 +50,7 @@ enum {
   ISW_EUNSUPPORTED = 4,  /* a combination this build does not run: air layers or option branches in the mixed form or
                           * in a batch (they step in the FP64 form, call by call) */
   ISW_ETIMEOUT = 5,      /* a bounded device-side wait gave up (persistent kernels); the context stays usable */
-  ISW_ENOTFINITE = 6     /* reserved: a NaN/Inf budget */
+  ISW_ENOTFINITE = 6     /* a step left a NaN or Inf thickness (batched steps), or substeps met a non-finite column */
 };
 
 /* Precision forms. ISW_FP64: plain FP64, the reference's FP64 path bit for bit (1e-12 where exp() enters). ISW_MIXED:
@@ -124,6 +129,7 @@ const char *isw_last_error(void);
 int isw_version(void);
 
 int isw_grid_create(const isw_grid_host *g, int device, isw_grid **out);
+/* Destroy a grid only after every Layers and Transport handle made on it is destroyed. */
 int isw_grid_destroy(isw_grid *g);
 
 int isw_layers_create(isw_grid *g, const isw_layers_params *p, isw_layers **out);
@@ -148,6 +154,18 @@ int isw_layers_update_gfast(isw_layers *s, const double *h, const double *theta,
 int isw_layers_substeps(isw_layers *s, const double *h, double dt, int *out, void *stream);
 /* out (L x E) = the edge vector Laplacian of u (L x E). */
 int isw_layers_lap(isw_layers *s, const double *u, double *out, void *stream);
+/* The heat of kinetic energy removed at the edges returned to the layers' potential temperature (the reference's
+ * kernel-table entry core.k['vmix_heat'], called by world.py:317-318 after the sea coupling with the sea's dissipation):
+ * diss (E, J/m^2 per edge) gives each cell half of l_e d_e diss_e; each layer k of the column warms by q / (mu pibar_k)
+ * with pibar_k the layer's mass-mean Exner function from h (L x N, mass per area). theta (L x N) updated in place; grav,
+ * cp, kappa, p0 are the caller's (the world passes its gravity, core.cpa, core.kap and P0). Any precision form. */
+int isw_layers_vmix_heat(isw_layers *s, const double *h, const double *diss, double *theta, double grav, double cp,
+                         double kappa, double p0, void *stream);
+/* Zero the wall edges (wall[e] == 0) of the first `rows` rows (1..8) of an edge field a (rows x E); no-op without walls. */
+int isw_layers_mask(isw_layers *s, double *a, int rows, void *stream);
+/* The status word of the one-stack batch that isw_layers_step uses (as isw_batch_status; ISW_OK when the handle steps
+ * call by call). While it holds ISW_ETIMEOUT or ISW_ENOTFINITE, isw_layers_step refuses with that status. */
+int isw_layers_status(isw_layers *s, void *stream, int reset);
 
 int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int precision, isw_transport **out);
 int isw_transport_destroy(isw_transport *t);
@@ -195,8 +213,11 @@ int isw_batch_flush(isw_batch *b, void *stream);
 /* The batch's layout: registered stacks, fast-loop tiles, the exchange interval in use, the largest tile's shared memory
  * (bytes), the cooperative launches per stage, tile blocks per SM (0 when untiled). */
 int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long *smem_bytes, int *groups, int *blocks_per_sm);
-/* The batch's device status word (ISW_OK, or ISW_ETIMEOUT after a grid barrier's bounded wait ran out); synchronises
- * `stream`; reset != 0 clears it. */
+/* The batch's device status word: ISW_OK, ISW_ETIMEOUT after a grid barrier's bounded wait ran out, or ISW_ENOTFINITE
+ * after a step left a NaN or Inf thickness (checked for every cell and layer at the end of each step). The kernel that
+ * records a failure also writes it to a mapped host word, and isw_batch_step refuses to run (returning that status)
+ * until the word is cleared, so later steps never run on a half-updated state. Synchronises `stream`; reset != 0
+ * clears the word (restore the state first). */
 int isw_batch_status(isw_batch *b, void *stream, int reset);
 /* Failure-detection test: one step in which block 0 never arrives at the first grid barrier, so every other block's
  * bounded wait runs out after timeout_ns (1 ms .. 2 s) and the status word becomes ISW_ETIMEOUT. Test use only. */

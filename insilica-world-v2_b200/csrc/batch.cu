@@ -13,7 +13,10 @@
 // vmix + FCT stage-1 edge fluxes | P1 (receiving masses, td, p1) | P2E | P2 | P3E | P3 | P4 (and M <- M1).
 //
 // The tile kernel's grid barrier waits with an iteration-bounded, time-bounded spin (globaltimer): if a wait runs out
-// it records ISW_ETIMEOUT in the batch's status word and every block returns; the host reads the status.
+// it records ISW_ETIMEOUT in the batch's status word and every block returns. Phase D of the last stage checks every
+// new thickness and records ISW_ENOTFINITE for a NaN or Inf. The kernel that records a failure also writes it to a
+// mapped host word, and isw_batch_step refuses to run while that word is set (until isw_batch_status resets it), so a
+// caller that never polls cannot step on a half-updated state.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -94,8 +97,12 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
-    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
-    else ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
+    if (kind == 0) {
+      ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
+      if (st == 2) check_finite_column(d.h, M.g.N, d.L, i, sc.status);
+    } else {
+      ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
+    }
   } else if (PH == PH_VMIX) {
     if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
   } else if (PH == PH_HF1) {
@@ -134,7 +141,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
 // loop). The final barotropic wind and its accumulated sum go to ub and acc, which no round reads.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
-                                                    int rounds, GridBarrier *bar, int *status, long long timeout_ns,
+                                                    int rounds, GridBarrier *bar, BatchStatus *status, long long timeout_ns,
                                                     int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int cnt[2 * (FAST_KMAX + 1)];
@@ -280,7 +287,8 @@ struct isw_batch {
   size_t fast_smem = 0;
   int fast_bps = 2;                           // tile blocks per SM: 2 (512 threads each) or 1 (1024 threads)
   GridBarrier *bar = nullptr;
-  int *status = nullptr;
+  BatchStatus *status = nullptr;              // device status word (code + the mirror's device address)
+  int *status_host = nullptr;                 // mapped pinned host mirror of the code, written by the failing kernel
   int tile_k = 8;
   int tiles_enabled = 1;
   int mixed = -1;                             // the stacks' precision form (all alike): -1 before the first add
@@ -658,6 +666,7 @@ void rebuild(isw_batch *b) {
     ISW_CUDA(cudaMemcpy(b->d_refs, refs.data(), sizeof(TileRef) * refs.size(), cudaMemcpyHostToDevice));
   }
   Sched &sc = b->sc;
+  sc.status = b->status;
   sc.cell = b->d_chunks;
   sc.ncell = (int)cell.size();
   sc.edge = sc.cell + sc.ncell;
@@ -888,8 +897,12 @@ int isw_batch_create(int device, isw_batch **out) {
       ISW_CUDA(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device));
       ISW_CUDA(cudaMalloc(&b->bar, sizeof(GridBarrier)));
       ISW_CUDA(cudaMemset(b->bar, 0, sizeof(GridBarrier)));
-      ISW_CUDA(cudaMalloc(&b->status, sizeof(int)));
-      ISW_CUDA(cudaMemset(b->status, 0, sizeof(int)));
+      ISW_CUDA(cudaMalloc(&b->status, sizeof(BatchStatus)));
+      ISW_CUDA(cudaHostAlloc((void **)&b->status_host, sizeof(int), cudaHostAllocMapped));
+      *b->status_host = 0;
+      BatchStatus init{0, 0, nullptr};
+      ISW_CUDA(cudaHostGetDevicePointer((void **)&init.mirror, b->status_host, 0));
+      ISW_CUDA(cudaMemcpy(b->status, &init, sizeof(BatchStatus), cudaMemcpyHostToDevice));
       ISW_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
       ISW_CUDA(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
       ISW_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
@@ -897,6 +910,7 @@ int isw_batch_create(int device, isw_batch **out) {
     } catch (...) {
       cudaFree(b->bar);
       cudaFree(b->status);
+      if (b->status_host) cudaFreeHost(b->status_host);
       delete b;
       throw;
     }
@@ -921,9 +935,11 @@ int isw_batch_destroy(isw_batch *b) {
   cudaFree(b->d_refs);
   cudaFree(b->bar);
   cudaFree(b->status);
+  if (b->status_host) cudaFreeHost(b->status_host);
   for (auto &kv : b->tiles)
     for (void *p : kv.second->allocs) cudaFree(p);
   delete b;
+  (void)cudaGetLastError();         // a failure while freeing must not surface in the caller's next call
   return ISW_OK;
 }
 
@@ -1016,6 +1032,13 @@ int isw_batch_info(isw_batch *b, int *stacks, int *tiles, int *tile_k, long long
 int isw_batch_step(isw_batch *b, void *stream) {
   return guarded([&] {
     if (!b) fail(ISW_EINVAL, "batch.step: null handle");
+    const int code = *(volatile int *)b->status_host;
+    if (code == ISW_ETIMEOUT)
+      fail(code, "batch.step: refused: an earlier step's grid barrier timed out, so the state is half-updated; restore "
+                 "it and clear the status (isw_batch_status with reset) to step again");
+    if (code != ISW_OK)
+      fail(code, "batch.step: refused: an earlier step left a non-finite thickness; restore the state and clear the status "
+                 "(isw_batch_status with reset) to step again");
     ISW_CUDA(cudaSetDevice(b->device));
     step(b, (cudaStream_t)stream);
   });
@@ -1045,9 +1068,13 @@ int isw_batch_status(isw_batch *b, void *stream, int reset) {
     if (!b) fail(ISW_EINVAL, "batch.status: null handle");
     ISW_CUDA(cudaSetDevice(b->device));
     int st = 0;
-    ISW_CUDA(cudaMemcpyAsync(&st, b->status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    ISW_CUDA(cudaMemcpyAsync(&st, &b->status->code, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     ISW_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
-    if (reset) ISW_CUDA(cudaMemset(b->status, 0, sizeof(int)));
+    if (reset) {
+      ISW_CUDA(cudaMemset(&b->status->code, 0, sizeof(int)));
+      ISW_CUDA(cudaDeviceSynchronize());
+      *(volatile int *)b->status_host = 0;
+    }
     out = st;
   });
   return rc != ISW_OK ? rc : out;

@@ -43,10 +43,35 @@ struct TileRef {
   int s, p;
 };
 
+// The batch's status word on the device, and where a kernel that sets it also writes the code for the host: a mapped
+// pinned host word, so that the next isw_batch_step can refuse to run without synchronising the stream.
+struct BatchStatus {
+  int code;
+  int pad;
+  volatile int *mirror;
+};
+
+// Record the first failure of a step (later ones keep the first code) and publish it to the host.
+__device__ __forceinline__ void raise_status(BatchStatus *s, int code) {
+  if (atomicCAS(&s->code, 0, code) == 0 && s->mirror) {
+    *s->mirror = code;
+    __threadfence_system();
+  }
+}
+
 struct Sched {
   const Chunk *cell, *edge, *vert, *rows, *erows;   // rows: (tracer, cell) pairs; erows: (tracer, edge) pairs
   int ncell, nedge, nvert, nrows, nerows;
+  BatchStatus *status;
 };
+
+// The step's result check: every layer of cell i must hold a finite thickness after the last stage, else the batch's
+// status becomes ISW_ENOTFINITE (a NaN or Inf in a wind reaches the thicknesses through the layer fluxes in the same step).
+__device__ __forceinline__ void check_finite_column(const double *__restrict__ h, int N, int L, int i, BatchStatus *s) {
+  bool ok = true;
+  for (int k = 0; k < L; k++) ok = ok && isfinite(h[(size_t)k * N + i]);
+  if (!ok) raise_status(s, ISW_ENOTFINITE);
+}
 
 struct GridBarrier {
   unsigned count, gen;
@@ -59,13 +84,13 @@ __device__ __forceinline__ long long globaltimer() {
 }
 
 // Block-wide grid barrier with a bounded wait. Returns false once any block has recorded a failure.
-__device__ inline bool grid_sync(GridBarrier *b, int *status, long long timeout_ns, int skip_arrive) {
+__device__ inline bool grid_sync(GridBarrier *b, BatchStatus *status, long long timeout_ns, int skip_arrive) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     ok = 1;
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(b->gen), cnt(b->count);
-    cuda::atomic_ref<int, cuda::thread_scope_device> st(*status);
+    cuda::atomic_ref<int, cuda::thread_scope_device> st(status->code);
     const unsigned g0 = gen.load(cuda::memory_order_acquire);
     __threadfence();
     if (!skip_arrive && cnt.fetch_add(1u, cuda::memory_order_acq_rel) == gridDim.x - 1) {
@@ -79,8 +104,7 @@ __device__ inline bool grid_sync(GridBarrier *b, int *status, long long timeout_
         if ((it & 63) == 0) {
           if (st.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
           if (globaltimer() - t0 > timeout_ns) {
-            int z = 0;
-            st.compare_exchange_strong(z, (int)ISW_ETIMEOUT, cuda::memory_order_relaxed);
+            raise_status(status, ISW_ETIMEOUT);
             ok = 0;
             break;
           }
@@ -182,7 +206,7 @@ void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, con
                         int j);
 const void *fast_kernel_mixed(int bps);
 void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
-                       GridBarrier *bar, int *status, long long timeout_ns, int fault_block);
+                       GridBarrier *bar, BatchStatus *status, long long timeout_ns, int fault_block);
 
 }  // namespace bt
 }  // namespace isw

@@ -87,8 +87,12 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
     ISW_BATCH_L(d.L, LMAXK, mixed::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const mixed::MStageArgs a = mstage_args(d, st);
-    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, mixed::h_cell<LL>(M, a, i));
-    else ISW_BATCH_L(d.L, LMAXK, mixed::u_edge<LL>(M, a, i));
+    if (kind == 0) {
+      ISW_BATCH_L(d.L, LMAXK, mixed::h_cell<LL>(M, a, i));
+      if (st == 2) check_finite_column(d.h, M.g.N, d.L, i, sc.status);
+    } else {
+      ISW_BATCH_L(d.L, LMAXK, mixed::u_edge<LL>(M, a, i));
+    }
   } else if (PH == PH_VMIX) {
     if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
   } else if (PH == PH_HF1) {
@@ -126,7 +130,7 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
 // eown <= FAST_AMAX NT.
 template <int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict__ S, const TileRef *__restrict__ refs, int st,
-                                                      int rounds, GridBarrier *bar, int *status, long long timeout_ns,
+                                                      int rounds, GridBarrier *bar, BatchStatus *status, long long timeout_ns,
                                                       int fault_block) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int cnt[2 * (FAST_KMAX + 1)];
@@ -319,7 +323,7 @@ const void *fast_kernel_mixed(int bps) {
 }
 
 void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
-                       GridBarrier *bar, int *status, long long timeout_ns, int fault_block) {
+                       GridBarrier *bar, BatchStatus *status, long long timeout_ns, int fault_block) {
   if (bps == 2)
     ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_m<512, 2>, desc, refs, stage, rounds, bar, status, timeout_ns, fault_block));
   else

@@ -99,10 +99,9 @@ extern "C" int isw_dsum(const double *x, const double *y, long long n, double *o
 
 // ---- The deterministic sum without any allocation ----
 //
-// For callers that cannot allocate device memory when they sum: code running while a CUDA graph is being captured
-// (an allocation there is either refused or recorded into the graph), hosts that reserve all device memory up front
-// and forbid later cudaMalloc calls (an embedding framework with its own memory pool, a real-time loop that must not
-// stall on the allocator), and plugins whose host owns the device heap. The passes' partial sums live in one file-scope
+// For callers that cannot allocate device memory when they sum: hosts that reserve all device memory up front and
+// forbid later cudaMalloc calls (an embedding framework with its own memory pool, a real-time loop that must not stall
+// on the allocator), and plugins whose host owns the device heap. The passes' partial sums live in one file-scope
 // device array of a fixed size, sized for sums of up to 134,217,728 values (2^27). Every GPU that loads this library
 // holds the array until the process exits.
 //

@@ -247,6 +247,7 @@ int isw_grid_destroy(isw_grid *g) {
   cudaSetDevice(g->device);
   for (void *p : g->allocs) cudaFree(p);
   delete g;
+  (void)cudaGetLastError();         // a failure while freeing must not surface in the caller's next call
   return ISW_OK;
 }
 

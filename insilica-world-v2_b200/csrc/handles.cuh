@@ -17,6 +17,7 @@ struct isw_batch;
 
 struct isw_layers {
   isw_grid *grid;
+  int device = 0;                   // the grid's device (kept here so that destroy reads nothing of the grid)
   isw::LayersDev d;
   std::vector<void *> allocs;
   cudaStream_t cap;                 // private stream the step graphs are captured on
@@ -34,6 +35,7 @@ struct isw_layers {
 
 struct isw_transport {
   isw_grid *grid;
+  int device = 0;                   // the grid's device (kept here so that destroy reads nothing of the grid)
   isw::TransportDev d;
   int L, T, precision;
   double beta;

@@ -143,6 +143,22 @@ __global__ void __launch_bounds__(THREADS) k_vmix_heat(const LayersDev M, const 
   if (t < M.g.N) fp64::vmix_heat_cell<L>(M, h, theta, t);
 }
 
+// The heating kernel of the layers' kernel table as the world calls it after the sea coupling (reference
+// world.py:317-318 with kernels/layers.cu:596-621): the caller's per-edge dissipation and constants.
+template <int L>
+__global__ void __launch_bounds__(THREADS) k_heat(const GridDev g, const double *__restrict__ h, const double *__restrict__ diss,
+                                                  double grav, double cp, double kap, double p0, double *__restrict__ theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < g.N) fp64::heat_column<L>(g, h, diss, grav, cp, kap, p0, theta, t);
+}
+
+// rows of an edge field zeroed on the wall edges (reference kernels/layers.cu:495-499, lay_mask)
+__global__ void __launch_bounds__(THREADS) k_wall_mask(const double *__restrict__ wall, int E, int rows, double *__restrict__ a) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E || wall[e] != 0) return;
+  for (int k = 0; k < rows; k++) a[(size_t)k * E + e] = 0;
+}
+
 __global__ void __launch_bounds__(THREADS) k_bt_eta(const LayersDev M, double tau) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < M.g.N) fp64::bt_eta_cell(M, tau, t);
@@ -354,6 +370,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
   ISW_CUDA(cudaSetDevice(g->device));
   isw_layers *s = new isw_layers();
   s->grid = g;
+  s->device = g->device;
   try {
     LayersDev &d = s->d;
     std::memset(&d, 0, sizeof(d));
@@ -440,12 +457,13 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
 }
 
 void layers_destroy(isw_layers *s) {
-  cudaSetDevice(s->grid->device);
+  cudaSetDevice(s->device);
   if (s->solo) isw_batch_destroy(s->solo);
   for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);
   if (s->cap) cudaStreamDestroy(s->cap);
   for (void *p : s->allocs) cudaFree(p);
   delete s;
+  (void)cudaGetLastError();         // a failure while freeing must not surface in the caller's next call
 }
 
 // A step call by call through a private batch holding this one stack (rebuilt when the arrays, dt or nfast change): the
@@ -678,6 +696,42 @@ int isw_layers_substeps(isw_layers *s, const double *h, double dt, int *out, voi
     ISW_CUDA(cudaSetDevice(s->grid->device));
     *out = layers_substeps(s, h, dt, (cudaStream_t)stream);
   });
+}
+
+int isw_layers_vmix_heat(isw_layers *s, const double *h, const double *diss, double *theta, double grav, double cp,
+                         double kappa, double p0, void *stream) {
+  return guarded([&] {
+    if (!s) fail(ISW_EINVAL, "layers.vmix_heat: null handle");
+    if (!h || !diss || !theta) fail(ISW_EINVAL, "layers.vmix_heat: null array");
+    if (!(p0 > 0) || !(kappa > -1) || !std::isfinite(grav) || !std::isfinite(cp))
+      fail(ISW_EINVAL, "layers.vmix_heat: p0 must be positive, kappa > -1, grav and cp finite");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    const GridDev &g = s->d.g;
+    cudaStream_t st = (cudaStream_t)stream;
+    ISW_DISPATCH_L(s->d.L, (k_heat<LL><<<blocks_for(g.N), THREADS, 0, st>>>(g, h, diss, grav, cp, kappa, p0, theta)));
+    ISW_CUDA(cudaGetLastError());
+  });
+}
+
+int isw_layers_mask(isw_layers *s, double *a, int rows, void *stream) {
+  return guarded([&] {
+    if (!s || !a) fail(ISW_EINVAL, "layers.mask: null handle or array");
+    if (rows < 1 || rows > LMAX) fail(ISW_EINVAL, "layers.mask: rows outside 1..8");
+    if (!s->d.wall) return;                     // no walls: nothing to zero
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    const int E = s->d.g.E;
+    k_wall_mask<<<blocks_for(E), THREADS, 0, (cudaStream_t)stream>>>(s->d.wall, E, rows, a);
+    ISW_CUDA(cudaGetLastError());
+  });
+}
+
+int isw_layers_status(isw_layers *s, void *stream, int reset) {
+  if (!s) {
+    set_last_error("layers.status: null handle");
+    return ISW_EINVAL;
+  }
+  if (!s->solo) return ISW_OK;                  // only the batched one-stack path keeps a status word
+  return isw_batch_status(s->solo, stream, reset);
 }
 
 int isw_layers_lap(isw_layers *s, const double *u, double *out, void *stream) {

@@ -212,32 +212,44 @@ __device__ __forceinline__ void air_u_edge(const LayersDev &M, const StageArgs &
   }
 }
 
-// the interfacial stress's heat (diss, J/m^2 per edge) returned to theta, in proportion to each layer's mass
+// Heat of the kinetic energy removed at a cell's edges (reference kernels/layers.cu:596-621, vmix_heat): diss (J/m^2
+// per edge, over the edge's kite) gives each of its two cells half of l_e d_e diss_e; the cell's share per unit area
+// warms every layer of the column by the same amount per kilogram, d theta_k = q / (mu pibar_k), with pibar_k the
+// layer's mass-mean Exner function from the pressures at its top and bottom. Same operation order as the reference.
 template <int L>
-__device__ __forceinline__ void vmix_heat_cell(const LayersDev &M, const double *__restrict__ h, double *__restrict__ theta, int i) {
-  const GridDev &g = M.g;
+__device__ __forceinline__ void heat_column(const GridDev &g, const double *__restrict__ h, const double *__restrict__ diss,
+                                            double grav, double cp, double kap, double p0, double *__restrict__ theta, int i) {
   const int N = g.N;
+  int es[6];
+  slots6(g.cellEdge, i, es);
   double q = 0;
 #pragma unroll
-  for (int m = 0; m < 6; m++) {
-    const int e = g.cellEdge[i * 6 + m];
-    if (e >= 0) q += 0.5 * g.le[e] * g.de[e] * M.diss[e];
-  }
+  for (int m = 0; m < 6; m++)
+    if (es[m] >= 0) q += 0.5 * g.le[es[m]] * g.de[es[m]] * diss[es[m]];
   if (q == 0) return;
   q /= g.areaCell[i];
-  double mu = 0;
-#pragma unroll
-  for (int k = 0; k < L; k++) mu += h[(size_t)k * N + i];
-  double p = 0, xt = 0;
+  double mass[L], mu = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    const double pt = p;
-    p = p + M.grav * h[(size_t)k * N + i];
-    const double x = pow(p / M.p0, M.kap);
-    const double pib = M.cpa * (p * x - pt * xt) / ((M.kap + 1) * (p - pt));
-    theta[(size_t)k * N + i] += q / (mu * pib);
-    xt = x;
+    mass[k] = h[(size_t)k * N + i];
+    mu += mass[k];
   }
+  double pbot = 0, xtop = 0;          // pressure at the layer's bottom; (p_top / p0)^kappa
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const double ptop = pbot;
+    pbot = pbot + grav * mass[k];
+    const double xbot = pow(pbot / p0, kap);
+    const double pib = cp * (pbot * xbot - ptop * xtop) / ((kap + 1) * (pbot - ptop));
+    theta[(size_t)k * N + i] += q / (mu * pib);
+    xtop = xbot;
+  }
+}
+
+// the interfacial stress's heat (the step's own diss) returned to theta
+template <int L>
+__device__ __forceinline__ void vmix_heat_cell(const LayersDev &M, const double *__restrict__ h, double *__restrict__ theta, int i) {
+  heat_column<L>(M.g, h, M.diss, M.grav, M.cpa, M.kap, M.p0, theta, i);
 }
 
 template <int L>

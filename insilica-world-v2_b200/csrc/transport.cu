@@ -135,6 +135,7 @@ int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int preci
     ISW_CUDA(cudaSetDevice(g->device));
     isw_transport *t = new isw_transport();
     t->grid = g;
+    t->device = g->device;
     t->L = L;
     t->T = tracers;
     t->precision = precision;
@@ -159,9 +160,10 @@ int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int preci
 
 int isw_transport_destroy(isw_transport *t) {
   if (!t) return ISW_OK;
-  cudaSetDevice(t->grid->device);
+  cudaSetDevice(t->device);
   for (void *p : t->allocs) cudaFree(p);
   delete t;
+  (void)cudaGetLastError();         // a failure while freeing must not surface in the caller's next call
   return ISW_OK;
 }
 

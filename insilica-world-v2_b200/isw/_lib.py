@@ -56,6 +56,9 @@ isw_layers_set_option = _sig('isw_layers_set_option', I, [P, I, P, D])
 ISW_OPT_SIG, ISW_OPT_TIDE, ISW_OPT_CBOT, ISW_OPT_CD_BOT = 1, 2, 3, 4
 isw_layers_substeps = _sig('isw_layers_substeps', I, [P, P, D, ctypes.POINTER(I), P])
 isw_layers_lap = _sig('isw_layers_lap', I, [P, P, P, P])
+isw_layers_vmix_heat = _sig('isw_layers_vmix_heat', I, [P, P, P, P, D, D, D, D, P])
+isw_layers_mask = _sig('isw_layers_mask', I, [P, P, I, P])
+isw_layers_status = _sig('isw_layers_status', I, [P, P, I])
 isw_transport_create = _sig('isw_transport_create', I, [P, I, D, I, I, ctypes.POINTER(P)])
 isw_transport_destroy = _sig('isw_transport_destroy', I, [P])
 isw_transport_mass_after = _sig('isw_transport_mass_after', I, [P, P, P, P, P])

@@ -117,9 +117,11 @@ class Batch:
         _lib.check(_lib.isw_batch_flush(self._h, stream_of(self.device, stream)))
 
     def status(self, reset=False, stream=None):
-        """The device status word: 0, or ISW_ETIMEOUT (5) after a grid barrier's bounded wait ran out."""
+        """The device status word: 0, ISW_ETIMEOUT (5) after a grid barrier's bounded wait ran out, or ISW_ENOTFINITE (6)
+        after a step left a NaN or Inf thickness. While it is set, step() raises IswError with that status; reset clears
+        it (restore the state first)."""
         st = _lib.isw_batch_status(self._h, stream_of(self.device, stream), 1 if reset else 0)
-        if st not in (_lib.ISW_OK, _lib.ISW_ETIMEOUT):
+        if st not in (_lib.ISW_OK, _lib.ISW_ETIMEOUT, _lib.ISW_ENOTFINITE):
             _lib.check(st)
         return st
 

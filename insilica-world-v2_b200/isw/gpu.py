@@ -23,8 +23,9 @@ def set_precision(p):
     PRECISION = p
 
 
-def device_ptr(a, dtype=torch.float64, shape=None, name='array', device=None):
-    """Pointer of a C-contiguous device array of the given dtype and shape (checked); None stays None."""
+def device_ptr(a, dtype=torch.float64, shape=None, name='array', device=None, numel=None):
+    """Pointer of a C-contiguous device array of the given dtype and shape (or number of values; checked); None stays
+    None."""
     if a is None:
         return None
     if not isinstance(a, torch.Tensor):
@@ -40,6 +41,8 @@ def device_ptr(a, dtype=torch.float64, shape=None, name='array', device=None):
                     raise ValueError(f'{name}: not C-contiguous')
             if shape is not None and tuple(ai['shape']) != tuple(shape):
                 raise ValueError(f'{name}: shape {tuple(ai["shape"])}, want {tuple(shape)}')
+            if numel is not None and int(np.prod(ai['shape'], dtype=np.int64)) != numel:
+                raise ValueError(f'{name}: {int(np.prod(ai["shape"], dtype=np.int64))} values, want {numel}')
             return ai['data'][0]
         a = torch.from_dlpack(a)
     if not a.is_cuda:
@@ -50,6 +53,8 @@ def device_ptr(a, dtype=torch.float64, shape=None, name='array', device=None):
         raise ValueError(f'{name}: not contiguous')
     if shape is not None and tuple(a.shape) != tuple(shape):
         raise ValueError(f'{name}: shape {tuple(a.shape)}, want {tuple(shape)}')
+    if numel is not None and a.numel() != numel:
+        raise ValueError(f'{name}: {a.numel()} values, want {numel}')
     if device is not None and a.device.index != device:
         raise ValueError(f'{name}: on cuda:{a.device.index}, the grid is on cuda:{device}')
     return a.data_ptr()
@@ -96,6 +101,19 @@ class DeviceGrid:
     def handle(self):
         return self._h
 
+    def __getattr__(self, name):
+        """The grid's tables as device arrays under the reference's attribute names (gpu.py:58-63: int32 / int8 index
+        tables, FP64 geometry), made on first use, for callers that pass them to a kernel-table entry (world.py:317)."""
+        kinds = {**{k: torch.int32 for k in self.INT32}, **{k: torch.int8 for k in self.INT8},
+                 **{k: torch.float64 for k in self.REALS}}
+        if name not in kinds or 'host' not in self.__dict__:
+            raise AttributeError(name)
+        cache = self.__dict__.setdefault('_dev', {})
+        if name not in cache:
+            cache[name] = torch.as_tensor(np.ascontiguousarray(getattr(self.host, name)), dtype=kinds[name],
+                                          device=f'cuda:{self.device}')
+        return cache[name]
+
     def __del__(self):
         h = getattr(self, '_h', None)
         destroy = getattr(_lib, 'isw_grid_destroy', None) if _lib is not None else None
@@ -118,5 +136,6 @@ def dsum(x, y=None, stream=None):
             raise ValueError('dsum: x and y differ in size')
         py = device_ptr(y, name='y')
     out = ctypes.c_double()
-    _lib.check(_lib.isw_dsum(px, py, x.numel(), ctypes.byref(out), stream_of(x.device, stream)))
+    with torch.cuda.device(x.device):          # the sum allocates and launches on the current device: make it x's
+        _lib.check(_lib.isw_dsum(px, py, x.numel(), ctypes.byref(out), stream_of(x.device, stream)))
     return out.value

@@ -10,6 +10,7 @@ The option branches of Boussinesq layers are built in the FP64 form: thin walls 
 """
 import ctypes
 import math
+import weakref
 
 import numpy as np
 import torch
@@ -74,6 +75,7 @@ class Layers:
         self._h = h
         self.dmin = float(np.min(dg.host.de))
         self._L1 = None
+        self.k = KernelTable(self)
 
     def __del__(self):
         h = getattr(self, '_h', None)
@@ -134,6 +136,24 @@ class Layers:
     def _shapes(self):
         return (self.L, self.dg.N), (self.L, self.dg.E)
 
+    def mask(self, a, rows, stream=None):
+        """Zero the wall edges of the first `rows` rows of the edge field a (rows, E) in place; a no-op without walls
+        (reference layers.py:94-97)."""
+        if self._wall is None:
+            return
+        dev = self.dg.device
+        _lib.check(_lib.isw_layers_mask(self._h, device_ptr(a, name='a', device=dev, numel=int(rows) * self.dg.E), int(rows),
+                                        stream_of(dev, stream)))
+
+    def status(self, reset=False, stream=None):
+        """The status word of the one-stack batch this Layers steps through: 0, ISW_ETIMEOUT (5) after a fast-loop barrier
+        timed out, or ISW_ENOTFINITE (6) after a step left a NaN or Inf thickness. While it is set, step() raises; reset
+        clears it (restore the state first)."""
+        st = _lib.isw_layers_status(self._h, stream_of(self.dg.device, stream), 1 if reset else 0)
+        if st not in (_lib.ISW_OK, _lib.ISW_ETIMEOUT, _lib.ISW_ENOTFINITE):
+            _lib.check(st)
+        return st
+
     def step(self, h, u, dt, nfast, Fm=None, theta=None, stream=None):
         """One time-split RK3 step in place on h (L, N), u (L, E), with nfast fast sub-steps per full step (stage s takes
         ceil(c_s nfast)). Fm, if given, receives each layer's final-stage volume flux l dt F (m^3; for air layers the
@@ -142,6 +162,8 @@ class Layers:
         dev = self.dg.device
         if bool(self.air) != (theta is not None):
             raise ValueError('Layers.step: theta is required for air layers and only for them')
+        if self.nu4:
+            self.nu4dt = self.nu4 * dt             # the step's nabla^4 loss, booked as heat by an air exchange (layers.py:202)
         ph = device_ptr(h, shape=sh, name='h', device=dev)
         pu = device_ptr(u, shape=su, name='u', device=dev)
         pf = device_ptr(Fm, shape=su, name='Fm', device=dev)
@@ -229,3 +251,65 @@ class Layers:
         for k in range(1, self.L):
             pot += np.sum(gh.areaCell * self.gp[k - 1] * (z[k] ** 2 - b ** 2) / 2)
         return float(kin + pot)
+
+
+def _numel(a):
+    if isinstance(a, torch.Tensor):
+        return a.numel()
+    if hasattr(a, '__cuda_array_interface__'):
+        return int(np.prod(a.__cuda_array_interface__['shape'], dtype=np.int64))
+    return torch.from_dlpack(a).numel()
+
+
+class KernelTable:
+    """The entries of the reference's kernel table (``Layers.k``, layers.py:83-91) that its callers launch themselves,
+    with the reference's launch convention ``k[name](grid, block, args)``: ``'vmix_heat'`` (world.py:317-318, after the
+    sea coupling) and ``'lay_mask'``. The grid and block sizes are the caller's CuPy launch shape and are not needed: each
+    entry runs this core's kernel for the whole field. The arguments are read in the reference kernels' order, with
+    their device arrays' sizes checked; the grid tables passed must be this Layers' grid's."""
+
+    def __init__(self, core):
+        self._ref = weakref.ref(core)        # no reference cycle: a Layers is freed as soon as its last user lets go
+
+    @property
+    def _core(self):
+        c = self._ref()
+        if c is None:
+            raise RuntimeError('Layers.k: the Layers object is gone')
+        return c
+
+    def __contains__(self, name):
+        return name in ('vmix_heat', 'lay_mask')
+
+    def __getitem__(self, name):
+        if name == 'vmix_heat':
+            return self._vmix_heat
+        if name == 'lay_mask':
+            return self._lay_mask
+        raise KeyError(f'Layers.k[{name!r}]: only vmix_heat and lay_mask are launched by callers; the other kernels run '
+                       'inside this core\'s step')
+
+    def _vmix_heat(self, grid, block, args, stream=None, **kw):
+        """args = (N, L, h, diss, cellEdge, le, de, areaCell, grav, cp, kappa, p0, theta), the reference kernel's order."""
+        c = self._core
+        N, L, h, diss, cellEdge, le, de, areaCell, grav, cpa, kap, p0, theta = args
+        if int(N) != c.dg.N or int(L) != c.L:
+            raise ValueError(f'vmix_heat: N {int(N)}, L {int(L)}; this Layers has N {c.dg.N}, L {c.L}')
+        for nm, a, n in (('cellEdge', cellEdge, 6 * c.dg.N), ('le', le, c.dg.E), ('de', de, c.dg.E), ('areaCell', areaCell, c.dg.N)):
+            if _numel(a) != n:
+                raise ValueError(f'vmix_heat: {nm} has {_numel(a)} values, the grid {n}')
+        dev = c.dg.device
+        sh = (c.L, c.dg.N)
+        _lib.check(_lib.isw_layers_vmix_heat(c._h, device_ptr(h, shape=sh, name='h', device=dev),
+                                             device_ptr(diss, name='diss', device=dev, numel=c.dg.E),
+                                             device_ptr(theta, shape=sh, name='theta', device=dev), float(grav), float(cpa),
+                                             float(kap), float(p0), stream_of(dev, stream)))
+
+    def _lay_mask(self, grid, block, args, stream=None, **kw):
+        """args = (E, rows, wall, a), the reference kernel's order; the wall is this Layers' own."""
+        c = self._core
+        E, rows, wall, a = args
+        if int(E) != c.dg.E:
+            raise ValueError(f'lay_mask: E {int(E)}, the grid {c.dg.E}')
+        c.mask(a, int(rows), stream=stream)
+

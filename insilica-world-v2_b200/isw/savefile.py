@@ -24,10 +24,15 @@ def write(path, meta, arrays):
 
 
 def read(path):
-    """(meta, {name: array}); refuses other format versions."""
-    with zipfile.ZipFile(path) as z:
-        meta = json.loads(z.read('meta.json'))
-        if meta.get('formatVersion') != FORMAT_VERSION:
-            raise ValueError(f'save file format {meta.get("formatVersion")}, expected {FORMAT_VERSION}')
-        arrays = {n: np.lib.format.read_array(io.BytesIO(z.read(n + '.npy')), allow_pickle=False) for n in meta['arrays']}
-    return meta, arrays
+    """(meta, {name: array}) of a save file; a file written in another format version is refused (ValueError) before
+    any array is decoded."""
+    with zipfile.ZipFile(path) as archive:
+        meta = json.loads(archive.read('meta.json'))
+        found = meta.get('formatVersion')
+        if found != FORMAT_VERSION:
+            raise ValueError(f'{path}: this reader takes format version {FORMAT_VERSION} only, the file has {found!r}')
+        members = {}
+        for name in meta['arrays']:
+            with archive.open(name + '.npy') as f:
+                members[name] = np.lib.format.read_array(io.BytesIO(f.read()), allow_pickle=False)
+    return meta, members

@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import gpu
+from . import _lib, gpu
 from .batch import Batch
 from .ensemble import device_grids
 from .workload import Member, stack_bytes
@@ -211,6 +211,10 @@ class Server:
                 model_days += a['member'].dt / SECONDS_PER_DAY
                 if a['left'] == 0:
                     finished.append(a)
+            if finished:                                    # no result leaves while the batch reports a failed step
+                code = self.batch.status(stream=st)
+                if code != 0:
+                    raise _lib.IswError(code, 'serving: the batched step reported a failure; results withheld')
             for a in finished:
                 m, req = a['member'], a['req']
                 m.unregister()

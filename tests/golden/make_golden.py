@@ -3,9 +3,10 @@
 reference checkout) on a NumPy-backed CuPy stand-in (``fakecupy.py``) whose kernels are the reference's own CUDA C
 compiled for the host (``oracle/build_ref.py``), in the reference's FP64 form (``INSILICA_PRECISION=double``).
 
-Needs the reference sources (default /root/reference) and ``oracle/_ref`` built. Run from the repository root:
+Needs the reference sources (``--ref``, else where ``oracle/refpath.py`` finds them) and ``oracle/_ref`` built. Run
+from the repository root:
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--cache /tmp/isw-grid-cache]
+    python tests/golden/make_golden.py [--ref <reference checkout>] [--cache <grid cache directory>]
 
 Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
 - grid_n4.npz    the reference's level-4 grid (Hilbert order), the arrays the step, the tables and the states use
@@ -21,6 +22,8 @@ Fixtures written (compressed .npz; every array is stored with its SHA-256 too):
                  moves, plain and sequential; air layers after one step, with heating and the thin layers' wind
 - options_n4.npz the option branches on the reference's outcrop case: thin walls, the shelf with its bed flags,
                  per-cell buoyancy (sig, zm), a tide potential, the bottom's quadratic and internal-tide drag: 12 steps
+- vmixheat_n4.npz the world's call of the layers' heating kernel after the sea coupling (world.py:317-318:
+                 core.k['vmix_heat'] with the sea's per-edge dissipation), on the aquaplanet's air layers: two calls
 
 `--only NAME` writes one fixture (e.g. `--only airtheta`).
 """
@@ -59,10 +62,19 @@ def save(name, d):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
-    ap.add_argument('--cache', default='/tmp/isw-grid-cache')
+    ap.add_argument('--ref', default=None)
+    ap.add_argument('--cache', default=None, help='the reference grid cache (default: a temporary directory)')
     ap.add_argument('--only', default=None)
     a = ap.parse_args()
+    sys.path.insert(0, str(ROOT))
+    from oracle import refpath
+    if a.ref is None:
+        a.ref = refpath.reference_root()
+        if a.ref is None:
+            sys.exit('make_golden: reference checkout not found (pass --ref or set ISW_REFERENCE)')
+    if a.cache is None:
+        import tempfile
+        a.cache = tempfile.mkdtemp(prefix='isw-grid-cache-')
     os.environ['INSILICA_PRECISION'] = 'double'
     os.environ['INSILICA_CACHE'] = a.cache
     sys.path.insert(0, str(HERE))
@@ -89,6 +101,9 @@ def main():
         return
     if a.only == 'exchange':
         save('exchange_n4.npz', exchange(cp, g, dg, Layers, rcases, mycases))
+        return
+    if a.only == 'vmixheat':
+        save('vmixheat_n4.npz', vmix_heat(cp, g, dg, Layers, rcases))
         return
     save('grid_n4.npz', {k: getattr(base, k) for k in GRID_KEYS})
 
@@ -299,6 +314,28 @@ def air_theta(cp, g, dg, Layers, rcases, mycases):
             d.update(h1=h.get(), u1=u.get(), theta1=theta.get(), Fm1=Fm.get())
     core.update_gfast(h, theta)
     d.update(h=h.get(), u=u.get(), theta=theta.get(), Fm=Fm.get(), Gc=core.Gc.get())
+    return d
+
+
+def vmix_heat(cp, g, dg, Layers, rcases):
+    """The world's own call of the heating kernel from the layers' kernel table (world.py:317-318): after the sea
+    coupling, the kinetic energy the wind stress removed over the tick (the sea's per-edge dissipation, J/m^2) returns
+    as heat to the air layers' theta. Aquaplanet air layers (cases.aqua), seeded dissipation of the size a tick's wind
+    stress gives (log-uniform 0.1 .. 1e4 J/m^2, zero on a tenth of the edges), two calls in a row."""
+    from insilica.constants import P0
+    from insilica.gpu import grid_dims
+    h0, b, u0, x = rcases.aqua(g)
+    core = Layers(dg, 3, b=b, gprime=[0.0, 0.0], floor=10.0, air=dict(t_ref=288.0), vmix=5e-3)
+    rng = np.random.default_rng(11)
+    diss = np.exp(rng.uniform(np.log(0.1), np.log(1e4), g.E)) * (rng.uniform(size=g.E) > 0.1)
+    h, theta, dd = cp.asarray(h0), cp.asarray(x['theta']), cp.asarray(diss)
+    grav = 9.80616
+    d = dict(h=h0, diss=diss, theta0=x['theta'], grav=grav, cp=core.cpa, kappa=core.kap, p0=P0)
+    i32, R = np.int32, np.float64
+    for call in (1, 2):
+        core.k['vmix_heat'](*grid_dims(g.N), (i32(g.N), i32(3), h, dd, dg.cellEdge, dg.le, dg.de, dg.areaCell, R(grav),
+                                               R(core.cpa), R(core.kap), R(P0), theta))
+        d[f'theta{call}'] = theta.get()
     return d
 
 

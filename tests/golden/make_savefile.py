@@ -1,7 +1,7 @@
 """Write tests/golden/save_ref.zip with the REFERENCE's own save writer (src/insilica/io/save.py, imported from the
 reference checkout): fixed meta and arrays, so tests can check that isw.savefile writes the same bytes and reads it.
 
-    python tests/golden/make_savefile.py [--ref /root/reference]
+    python tests/golden/make_savefile.py [--ref <reference checkout>]
 """
 import argparse
 import sys
@@ -19,8 +19,14 @@ def content():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=None)
     a = ap.parse_args()
+    if a.ref is None:
+        sys.path.insert(0, str(HERE.parents[1]))
+        from oracle import refpath
+        a.ref = refpath.reference_root()
+        if a.ref is None:
+            sys.exit('make_savefile: reference checkout not found (pass --ref or set ISW_REFERENCE)')
     sys.path.insert(0, str(Path(a.ref) / 'src'))
     from insilica.io import save
     meta, arrays = content()

@@ -120,27 +120,82 @@ def test_batch_mixed_levels_equal_alone(dev, grid4):
             assert torch.equal(x, y)
 
 
-def test_barrier_timeout_reports_and_recovers(dev, grid4):
-    """A block that never arrives at a grid barrier: the others' bounded waits run out, the host reads ISW_ETIMEOUT,
-    and the next ordinary step runs normally (same result as a fresh run)."""
+def test_barrier_timeout_refuses_then_recovers(dev, grid4):
+    """A block that never arrives at a grid barrier: the others' bounded waits run out and the host reads ISW_ETIMEOUT.
+    While the status is set the batch refuses to step (ISW_ETIMEOUT, nothing launched), so a caller that never polls
+    cannot step on a half-updated state. Once reset, the SAME batch steps again and equals an untouched run of the same
+    member bit for bit (the timed-out launch wrote only the fast loop's scratch, which every step rebuilds from h, u)."""
+    from isw._lib import ISW_ETIMEOUT, IswError
     from isw.batch import Batch
     from isw.gpu import DeviceGrid
     from isw.workload import Member, planet_grid
     dg = DeviceGrid(planet_grid(grid4))
     batch = Batch(0)
-    Member(dg, 3, nfast=20, batch=batch)
-    batch.fault_test(timeout_s=0.05)
-    assert batch.status(reset=True) == 5
-    assert batch.status() == 0
-    fresh_batch = Batch(0)
-    a = Member(dg, 4, nfast=20, batch=fresh_batch)
+    a = Member(dg, 4, nfast=20, batch=batch)
     b = Member(dg, 4, nfast=20)
-    fresh_batch.step()
-    b.step()
+    batch.fault_test(timeout_s=0.05)
     torch.cuda.synchronize()
-    assert fresh_batch.status() == 0
+    with pytest.raises(IswError) as err:
+        batch.step()
+    assert err.value.status == ISW_ETIMEOUT
+    assert batch.status() == ISW_ETIMEOUT
+    assert batch.status(reset=True) == ISW_ETIMEOUT
+    assert batch.status() == 0
+    for _ in range(2):
+        batch.step()
+        b.step()
+    torch.cuda.synchronize()
+    assert batch.status() == 0
     for x, y in zip(a.state(), b.state()):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize('precision', ['double', 'mixed'])
+def test_nonfinite_thickness_reported_and_refused(dev, grid4, precision):
+    """A NaN written into one thickness from the host: the step that meets it records ISW_ENOTFINITE (checked for every
+    cell and layer at the step's end) and the batch refuses further steps until the status is reset; after the state is
+    restored and the status reset, the same batch steps on equal to an untouched run bit for bit. The Layers path
+    (one-stack batch) refuses the same way and reports through Layers.status."""
+    from isw import gpu
+    from isw._lib import ISW_ENOTFINITE, IswError
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    gpu.set_precision(precision)
+    try:
+        dg = DeviceGrid(planet_grid(grid4))
+        batch, other = Batch(0), Batch(0)
+        a = Member(dg, 5, nfast=20, batch=batch)
+        b = Member(dg, 5, nfast=20, batch=other)         # the untouched run: the same batched path
+        c = Member(dg, 5, nfast=20)
+    finally:
+        gpu.set_precision('double')
+    saved = [x.clone() for x in a.state()]
+    a.stacks[1].h[1, 17] = float('nan')
+    batch.step()
+    torch.cuda.synchronize()
+    assert batch.status() == ISW_ENOTFINITE
+    with pytest.raises(IswError) as err:
+        batch.step()
+    assert err.value.status == ISW_ENOTFINITE
+    for x, y in zip(a.state(), saved):
+        x.copy_(y)
+    assert batch.status(reset=True) == ISW_ENOTFINITE
+    for _ in range(2):
+        batch.step()
+        b.step()
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    for x, y in zip(a.state(), b.state()):
+        assert torch.equal(x, y)
+    s = c.stacks[0]
+    s.h[0, 5] = float('inf')
+    s.step()
+    torch.cuda.synchronize()
+    assert s.core.status() == ISW_ENOTFINITE
+    with pytest.raises(IswError):
+        s.step()
+    assert s.core.status(reset=True) == ISW_ENOTFINITE and s.core.status() == 0
 
 
 @pytest.mark.parametrize('k', [1, 2, 3, 4, 7, 8])

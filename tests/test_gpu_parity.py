@@ -282,6 +282,58 @@ def test_air_layers_golden(dev, isw, grid4):
         core.step(h, u, dt, nfast, Fm)                      # air layers need theta
 
 
+def test_world_vmix_heat_call_golden(dev, isw, grid4):
+    """The world's own launch of the layers' heating kernel after the sea coupling (reference world.py:317-318:
+    core.k['vmix_heat'](*grid_dims(N), (N, L, h, sea.diss, g.cellEdge, g.le, g.de, g.areaCell, grav, core.cpa,
+    core.kap, P0, theta))), made here exactly so with this core's Layers and DeviceGrid, against the reference kernel's
+    own result: theta after two calls to 1e-12 relative (and its increments to 1e-10; the kernel calls pow, whose last
+    bit may differ between the host's libm and CUDA's)."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    z = golden('vmixheat_n4')
+    g = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    core = layers.Layers(g, 3, gprime=[0.0, 0.0], floor=10.0, air=dict(t_ref=288.0), vmix=5e-3)
+    assert 'vmix_heat' in core.k and core.cpa == float(z['cp']) and core.kap == float(z['kappa'])
+    h, diss, theta = T(z['h'], dev), T(z['diss'], dev), T(z['theta0'], dev)
+    i32, R = np.int32, np.float64
+    grid_dims = ((g.N + 255) // 256, 1), (256,)
+    for call in (1, 2):
+        core.k['vmix_heat'](*grid_dims, (i32(g.N), i32(3), h, diss, g.cellEdge, g.le, g.de, g.areaCell, R(z['grav']),
+                                         R(core.cpa), R(core.kap), R(z['p0']), theta))
+        torch.cuda.synchronize()
+        got = theta.cpu().numpy()
+        assert rel(got, z[f'theta{call}']) <= REL, call
+        want_inc = z[f'theta{call}'] - (z['theta0'] if call == 1 else z['theta1'])
+        prev = z['theta0'] if call == 1 else z['theta1']
+        assert np.max(np.abs((got - prev) - want_inc)) <= 1e-10 * np.max(np.abs(want_inc))
+        theta = T(z[f'theta{call}'], dev)
+    with pytest.raises(ValueError):
+        core.k['vmix_heat'](*grid_dims, (i32(g.N), i32(2), h, diss, g.cellEdge, g.le, g.de, g.areaCell, R(9.8), R(1004.0),
+                                         R(0.28), R(1e5), theta))
+    with pytest.raises(KeyError):
+        core.k['lay_slow']
+
+
+def test_wall_mask(dev, isw, grid4):
+    """Layers.mask (reference layers.py:94-97, kernel lay_mask) zeroes the wall edges of the first rows of an edge
+    field and leaves every other value; a Layers without walls leaves the field unchanged."""
+    from isw import grid as G
+    gpu, layers, _ = isw
+    g = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    wall = (np.arange(g.E) % 7 != 3).astype(np.float64)
+    core = layers.Layers(g, 2, gprime=[0.02], wall=wall)
+    a = torch.arange(3 * g.E, dtype=torch.float64, device=dev).reshape(3, g.E) + 1.0
+    want = a.cpu().numpy().copy()
+    want[:2, wall == 0] = 0
+    core.mask(a[:2], 2)
+    core.k['lay_mask'](((g.E + 255) // 256, 1), (256,), (np.int32(g.E), np.int32(2), core.wall, a[:2]))
+    assert np.array_equal(a.cpu().numpy(), want)
+    plain = layers.Layers(g, 2, gprime=[0.02])
+    b = torch.ones(2, g.E, dtype=torch.float64, device=dev)
+    plain.mask(b, 2)
+    assert bool((b == 1).all())
+
+
 def test_exchange_golden(dev, isw, grid4):
     """The between-step exchange hook (Layers.exchange) after one step, against the reference's own: Boussinesq layers
     with seeded thickness moves, plain and sequential (h, u, M and the tracer); air layers with the momentum mixing's

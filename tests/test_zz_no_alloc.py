@@ -1,5 +1,5 @@
 """isw_dsum_static, the deterministic sum that allocates nothing (for callers that cannot allocate device memory at the
-call: during a graph capture, or under a host that owns the device heap), called through the C ABI: its result equals
+call: a host that reserved the device heap up front, or a plugin whose host owns it), called through the C ABI: its result equals
 isw_dsum's bit for bit (the tolerance the sum tests use), on two calls in a row sharing its fixed scratch array; sizes
 beyond the array are refused. This file sorts last so a run that stops at the first failure has run every other test."""
 import ctypes
