@@ -187,8 +187,9 @@ int isw_dsum_static(const double *x, const double *y, long long n, double *out, 
 /* Batched step: stacks (a Layers handle with its state h, u, Fm, and optionally a Transport with M, M1 and tracers)
  * registered once, then advanced together by isw_batch_step as ONE CUDA graph per step (one kernel per phase over every
  * stack; the barotropic sub-steps in shared-memory tiles, one cooperative kernel per stage): the RK3 step, the receiving
- * masses M1, the FCT step of every tracer, and M <- M1. Stacks may use different grids and layer counts; all stacks of a
- * batch share one precision form (ISW_EINVAL otherwise). Each stack's result is bit-identical to stepping it alone.
+ * masses M1, the FCT step of every tracer, and M <- M1. Stacks may use different grids, layer counts and precision
+ * forms: each phase is one kernel per form present, and in a batch holding both forms the fast-loop tiles serve the mixed
+ * stacks while the FP64 ones take the grid-wide sub-steps. Each stack's result is bit-identical to stepping it alone.
  * Registered pointers are borrowed until removed. */
 int isw_batch_create(int device, isw_batch **out);
 int isw_batch_destroy(isw_batch *b);

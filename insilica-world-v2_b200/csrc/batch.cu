@@ -280,7 +280,7 @@ struct isw_batch {
   StackDesc *d_desc = nullptr;
   Chunk *d_chunks = nullptr;
   TileRef *d_refs = nullptr;
-  Sched sc{};
+  Sched scf[2] = {};                          // chunk tables of the FP64 stacks [0] and the mixed ones [1]
   int lmax = 1, nstacks = 0, ntiles = 0, nsub[3] = {0, 0, 0}, kused = 0;
   std::vector<FastGroup> groups;              // cooperative launches of the fast loop (tiles [begin, begin + count))
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0;
@@ -291,7 +291,7 @@ struct isw_batch {
   int *status_host = nullptr;                 // mapped pinned host mirror of the code, written by the failing kernel
   int tile_k = 8;
   int tiles_enabled = 1;
-  int mixed = -1;                             // the stacks' precision form (all alike): -1 before the first add
+  int mixed = 0;                              // 1 when any stack is mixed: the tile kernels are then the mixed form's
   int tile_cells = 0;                         // packed layout's owned cells per tile (0: by blocks per SM)
   int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
   int layout = 0;                             // 0: choose; 1 shared; 2 packed
@@ -437,6 +437,12 @@ struct Tiling {
   std::vector<int> group;                      // group per slot
 };
 
+int form_of(const BatchSlot &sl) { return sl.layers->d.precision == ISW_MIXED ? 1 : 0; }
+
+// A batch holding stacks of both forms tiles the fast loop of its mixed stacks only (one tile kernel per batch); its
+// FP64 stacks take the grid-wide sub-step kernels.
+bool tiles_form(const isw_batch *b, const BatchSlot &sl) { return sl.used && form_of(sl) == b->mixed; }
+
 Tiling plan_shared(isw_batch *b, int bps) {
   Tiling t;
   t.bps = bps;
@@ -446,12 +452,12 @@ Tiling plan_shared(isw_batch *b, int bps) {
   const int slots = b->sms * bps;
   long long cells_total = 0;
   for (auto &sl : b->slots)
-    if (sl.used) cells_total += sl.layers->grid->d.N;
+    if (tiles_form(b, sl)) cells_total += sl.layers->grid->d.N;
   int kmin = b->tile_k;
   bool any = false;
   for (size_t q = 0; q < b->slots.size(); q++) {
     const BatchSlot &sl = b->slots[q];
-    if (!sl.used) continue;
+    if (!tiles_form(b, sl)) continue;
     const int N = sl.layers->grid->d.N;
     const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
     if (Pq * 16 > N) return Tiling{};          // tiles of at least 16 owned cells, for every stack
@@ -480,7 +486,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
   bool any = false;
   for (size_t q = 0; q < b->slots.size(); q++) {
     const BatchSlot &sl = b->slots[q];
-    if (!sl.used) continue;
+    if (!tiles_form(b, sl)) continue;
     const int N = sl.layers->grid->d.N;
     const int Pq = std::min(cap, std::max(1, (N + cells - 1) / cells));
     if (Pq * 16 > N) continue;
@@ -506,8 +512,11 @@ Tiling plan_packed(isw_batch *b, int bps) {
 
 void rebuild(isw_batch *b) {
   std::vector<StackDesc> desc;
-  std::vector<Chunk> cell, edge, vert, rows, erows;
+  std::vector<Chunk> cell[2], edge[2], vert[2], rows[2], erows[2];      // per form: [0] FP64 stacks, [1] mixed
   int nsub[3] = {0, 0, 0};
+  b->mixed = 0;
+  for (auto &sl : b->slots)
+    if (sl.used && form_of(sl) == 1) b->mixed = 1;
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
   int used = 0;
@@ -574,11 +583,12 @@ void rebuild(isw_batch *b) {
     auto chunks = [&](std::vector<Chunk> &v, int n) {
       for (int i = 0; i < n; i += THREADS) v.push_back(Chunk{s, i, std::min(n, i + THREADS)});
     };
-    chunks(cell, d.M.g.N);
-    chunks(edge, d.M.g.E);
-    chunks(vert, d.M.g.NV);
-    if (d.has_tr) chunks(rows, sl.ntr * d.M.g.N);       // (tracer, cell) pairs
-    if (d.has_tr) chunks(erows, sl.ntr * d.M.g.E);      // (tracer, edge) pairs
+    const int f = form_of(sl);
+    chunks(cell[f], d.M.g.N);
+    chunks(edge[f], d.M.g.E);
+    chunks(vert[f], d.M.g.NV);
+    if (d.has_tr) chunks(rows[f], sl.ntr * d.M.g.N);       // (tracer, cell) pairs
+    if (d.has_tr) chunks(erows[f], sl.ntr * d.M.g.E);      // (tracer, edge) pairs
     desc.push_back(d);
   }
   b->nstacks = (int)desc.size();
@@ -610,11 +620,13 @@ void rebuild(isw_batch *b) {
   b->dirty = false;
   if (desc.empty()) return;
   std::vector<Chunk> all;
-  all.insert(all.end(), cell.begin(), cell.end());
-  all.insert(all.end(), edge.begin(), edge.end());
-  all.insert(all.end(), vert.begin(), vert.end());
-  all.insert(all.end(), rows.begin(), rows.end());
-  all.insert(all.end(), erows.begin(), erows.end());
+  for (int f = 0; f < 2; f++) {
+    all.insert(all.end(), cell[f].begin(), cell[f].end());
+    all.insert(all.end(), edge[f].begin(), edge[f].end());
+    all.insert(all.end(), vert[f].begin(), vert[f].end());
+    all.insert(all.end(), rows[f].begin(), rows[f].end());
+    all.insert(all.end(), erows[f].begin(), erows[f].end());
+  }
   ISW_CUDA(cudaMalloc(&b->d_desc, sizeof(StackDesc) * desc.size()));
   ISW_CUDA(cudaMalloc(&b->d_chunks, sizeof(Chunk) * all.size()));
   ISW_CUDA(cudaMemcpy(b->d_chunks, all.data(), sizeof(Chunk) * all.size(), cudaMemcpyHostToDevice));
@@ -665,18 +677,22 @@ void rebuild(isw_batch *b) {
     ISW_CUDA(cudaMalloc(&b->d_refs, sizeof(TileRef) * refs.size()));
     ISW_CUDA(cudaMemcpy(b->d_refs, refs.data(), sizeof(TileRef) * refs.size(), cudaMemcpyHostToDevice));
   }
-  Sched &sc = b->sc;
-  sc.status = b->status;
-  sc.cell = b->d_chunks;
-  sc.ncell = (int)cell.size();
-  sc.edge = sc.cell + sc.ncell;
-  sc.nedge = (int)edge.size();
-  sc.vert = sc.edge + sc.nedge;
-  sc.nvert = (int)vert.size();
-  sc.rows = sc.vert + sc.nvert;
-  sc.nrows = (int)rows.size();
-  sc.erows = sc.rows + sc.nrows;
-  sc.nerows = (int)erows.size();
+  const Chunk *base = b->d_chunks;
+  for (int f = 0; f < 2; f++) {
+    Sched &sc = b->scf[f];
+    sc.status = b->status;
+    sc.cell = base;
+    sc.ncell = (int)cell[f].size();
+    sc.edge = sc.cell + sc.ncell;
+    sc.nedge = (int)edge[f].size();
+    sc.vert = sc.edge + sc.nedge;
+    sc.nvert = (int)vert[f].size();
+    sc.rows = sc.vert + sc.nvert;
+    sc.nrows = (int)rows[f].size();
+    sc.erows = sc.rows + sc.nrows;
+    sc.nerows = (int)erows[f].size();
+    base = sc.erows + sc.nerows;
+  }
   b->ntiles = (int)refs.size();
   size_t smax = 0;
   for (auto &fg : b->groups) smax = std::max(smax, fg.smem);
@@ -690,25 +706,30 @@ void rebuild(isw_batch *b) {
   b->lmax = kernel_lmax(lmax);
 }
 
-// A phase kernel over every stack. pdl: launched as a programmatic dependent of the kernel before it in the stream
-// (never directly after a cooperative tile launch, which keeps plain stream order).
+// A phase over every stack: one kernel per precision form present (the FP64 stacks' first). pdl: the first of them is
+// launched as a programmatic dependent of the kernel before it in the stream (never directly after a cooperative tile
+// launch, which keeps plain stream order); a second one always is.
 template <int PH>
 void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = true) {
-  const Sched &sc = b->sc;
-  const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
-                 (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
-  if (nb == 0) return;
-  if (!b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
-  pdl = pdl && b->pdl;
-  if (b->mixed == 1) {
-    launch_phase_mixed(PH, b->lmax, nb, st, pdl, b->cur, sc, stage, j);
-    return;
-  }
-  switch (b->lmax) {
-    case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, pdl, b->cur, sc, stage, j); break;
-    case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, pdl, b->cur, sc, stage, j); break;
-    case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, pdl, b->cur, sc, stage, j); break;
-    default: launch_phase_kernel(k_phase<PH, 8>, nb, st, pdl, b->cur, sc, stage, j); break;
+  bool first = true;
+  for (int f = 0; f < 2; f++) {
+    const Sched &sc = b->scf[f];
+    const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
+                   (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
+    if (nb == 0) continue;
+    if (!b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
+    const bool p = (first ? pdl : true) && b->pdl;
+    first = false;
+    if (f == 1) {
+      launch_phase_mixed(PH, b->lmax, nb, st, p, b->cur, sc, stage, j);
+      continue;
+    }
+    switch (b->lmax) {
+      case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, p, b->cur, sc, stage, j); break;
+      case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, p, b->cur, sc, stage, j); break;
+      case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, p, b->cur, sc, stage, j); break;
+      default: launch_phase_kernel(k_phase<PH, 8>, nb, st, p, b->cur, sc, stage, j); break;
+    }
   }
 }
 
@@ -959,10 +980,6 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
       if (tr->L != layers->d.L || tr->grid != layers->grid) fail(ISW_EINVAL, "batch.add: transport and layers differ in grid or L");
       if (tr->precision != layers->d.precision) fail(ISW_EINVAL, "batch.add: transport and layers differ in precision form");
     }
-    const int mixed = layers->d.precision == ISW_MIXED ? 1 : 0;
-    bool any = false;
-    for (auto &q : b->slots) any = any || q.used;
-    if (any && b->mixed != mixed) fail(ISW_EINVAL, "batch.add: a batch holds stacks of one precision form");
     ISW_CUDA(cudaSetDevice(b->device));
     settle(b);
     BatchSlot sl;
@@ -981,7 +998,6 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     while (k < b->slots.size() && b->slots[k].used) k++;
     if (k == b->slots.size()) b->slots.push_back(sl);
     else b->slots[k] = sl;
-    b->mixed = mixed;
     b->dirty = true;
     *slot = (int)k;
   });

@@ -4,7 +4,9 @@ vorticity) and mass drifts by the deterministic sum.
 
 - member(level, days): the stacked benchmark member (air 3 + ocean 2 layers, 3 tracers) in both forms from the same
   state; per stack the relative L2 (area-weighted) and Linf errors of h and u after `days`, and the relative drift of
-  every layer's volume and every tracer's mass over the run, in both forms.
+  every layer's volume and every tracer's mass over the run, in both forms. The mixed member runs its stacks as
+  mixed-form ensembles and serving do (the ocean stack at levels 4 and 5 in FP64: workload.FP64_IN_MIXED);
+  fp64_kinds=() measures the mixed form on every stack.
 - galewsky(level, days): the Galewsky jet (one layer, the reference's initial state) in both forms; L2/Linf of vertex
   vorticity and of h, and the mass drift.
 - w2(level, days): Williamson 2 (one layer, steady solid-body flow, dt 900 s at level 4) in both forms: h and u
@@ -43,7 +45,7 @@ def _masses(stack):
     return np.array(vol), np.array(trm)
 
 
-def member(level=6, days=10.0, seed=0, device=0):
+def member(level=6, days=10.0, seed=0, device=0, fp64_kinds=None):
     g = planet_grid(G.build(level, device=device))
     forms = {}
     for prec in ('double', 'mixed'):
@@ -53,7 +55,7 @@ def member(level=6, days=10.0, seed=0, device=0):
         finally:
             gpu.set_precision('double')
         b = Batch(device)
-        m = Member(dg, seed, batch=b)
+        m = Member(dg, seed, batch=b, fp64_kinds=fp64_kinds)
         forms[prec] = (m, b, [_masses(s) for s in m.stacks])
     steps = int(round(days * SECONDS_PER_DAY / forms['double'][0].dt))
     for _ in range(steps):
@@ -66,7 +68,7 @@ def member(level=6, days=10.0, seed=0, device=0):
         area = g.areaCell
         hd, hm, ud, um = sd.h.cpu().numpy(), sm.h.cpu().numpy(), sd.u.cpu().numpy(), sm.u.cpu().numpy()
         le_de = g.le * g.de                        # the edge area weight l_e d_e / 2 (the constant 1/2 cancels)
-        row = dict(stack=name, L=sd.L,
+        row = dict(stack=name, L=sd.L, form='double' if sm.core.precision == 0 else 'mixed',
                    h_l2=l2rel(area[None], hm, hd), h_linf=linf(hm, hd),
                    u_l2=l2rel(le_de[None], um, ud), u_linf=linf(um, ud),
                    h_rel_l2_plain=float(np.linalg.norm(hm - hd) / np.linalg.norm(hd)),

@@ -256,4 +256,4 @@ def stack_state(g, kind, seed, perturb=0.01, ntracers=3, topo=None, omega=OMEGA_
     tr = [rng.uniform(250.0, 310.0, (L, g.N)), 5e-3 * np.exp(0.5 * rng.standard_normal((L, g.N))),
           rng.uniform(0.0, 1.0, (L, g.N))][:ntracers]
     return dict(h=h, u=u, b=b, gprime=list(c['gprime']), stress=list(c['stress']), floor=c['floor'],
-                nu4=visc4(g, c['visc4_U']), vmix=c.get('vmix', 0.0), tracers=tr, L=L)
+                nu4=visc4(g, c['visc4_U']), vmix=c.get('vmix', 0.0), tracers=tr, L=L, kind=kind)

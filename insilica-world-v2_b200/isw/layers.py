@@ -30,11 +30,15 @@ KAPPA = R_DRY / CP_DRY
 class Layers:
     def __init__(self, dg, layers=1, b=None, grav=GRAV, gprime=(), drag=0.0, stress=0.0, nu4=0.0, floor=1.0, rotation=1.0,
                  div_damp=DIV_DAMP, air=None, vmix=0.0, thin=2.0, wall=None, thin_wind=0.0, shelf=0.0, vmix_cd=0.0,
-                 shelf_bed=False, batched=True):
+                 shelf_bed=False, batched=True, precision=None):
         """The reference's constructor (layers.py:36-37). batched (this core's): FP64 Boussinesq layers without option
         branches step through a private one-stack batch (tiled fast loop, one graph; bit-identical results); False keeps
-        the per-call kernels."""
-        if (wall is not None or shelf or shelf_bed) and dg.mixed:
+        the per-call kernels. precision (this core's): 'double' or 'mixed' for this object; None takes the grid's form
+        (the precision switch in force when the DeviceGrid was made)."""
+        if precision not in (None, 'double', 'mixed'):
+            raise ValueError(f'Layers: precision {precision!r}, want double or mixed')
+        mixed = dg.mixed if precision is None else precision == 'mixed'
+        if (wall is not None or shelf or shelf_bed) and mixed:
             raise NotImplementedError('Layers: walls and the shelf run in the FP64 form only')
         assert wall is None or not air, 'walls are for Boussinesq layers'
         assert 1 <= layers <= LMAX and len(gprime) == layers - 1
@@ -47,7 +51,7 @@ class Layers:
         self.air = air
         # the air's constants (reference layers.py:64-65: cp 1004.6, kappa, R 287.04 unless the air dict gives them)
         self.cpa, self.kap, self.rda = (air or {}).get('cp', CP_DRY), (air or {}).get('kappa', KAPPA), (air or {}).get('rd', R_DRY)
-        if air and dg.mixed:
+        if air and mixed:
             raise NotImplementedError('Layers: air layers run in the FP64 form only')
         self.shelf = float(shelf)
         self._wall = None if wall is None else np.ascontiguousarray(np.asarray(
@@ -55,7 +59,7 @@ class Layers:
         self.wall = None if wall is None else torch.as_tensor(self._wall, device=f'cuda:{dg.device}')
         self._opts = dict(sig=None, tide=None, cbot=None, cd_bot=0.0)
         self._zm = None
-        self.precision = _lib.ISW_MIXED if dg.mixed else _lib.ISW_FP64
+        self.precision = _lib.ISW_MIXED if mixed else _lib.ISW_FP64
         self._b_host = np.zeros(dg.N) if b is None else np.ascontiguousarray(np.asarray(
             b.detach().cpu().numpy() if isinstance(b, torch.Tensor) else b, dtype=np.float64))
         self.b = torch.as_tensor(self._b_host, device=f'cuda:{dg.device}')

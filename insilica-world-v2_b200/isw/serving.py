@@ -23,7 +23,7 @@ import torch
 from . import _lib, gpu
 from .batch import Batch
 from .ensemble import device_grids
-from .workload import Member, stack_bytes
+from .workload import Member, fp64_stack_kinds, stack_bytes
 
 SECONDS_PER_DAY = 86400.0
 
@@ -69,8 +69,10 @@ def poisson_requests(n, rate, seed=0, levels=(4, 5, 6, 7), days=(1.0, 30.0), lay
 
 
 def request_bytes(g, layers, ntracers, mixed):
+    """Device bytes of a request's member; in the mixed form the stacks FP64_IN_MIXED names for the level are FP64."""
     kinds = ('air',) if layers == 3 else ('air', 'ocean')
-    return sum(stack_bytes(g, 3 if k == 'air' else 2, ntracers, mixed) for k in kinds)
+    fk = fp64_stack_kinds(g.n) if mixed else ()
+    return sum(stack_bytes(g, 3 if k == 'air' else 2, ntracers, mixed and k not in fk) for k in kinds)
 
 
 class Server:

@@ -13,12 +13,17 @@ BETA = 0.25         # upwind weight of the 3rd-order flux (reference transport.p
 
 
 class Transport:
-    def __init__(self, dg, layers=1, beta=BETA, tracers=1):
+    def __init__(self, dg, layers=1, beta=BETA, tracers=1, precision=None):
+        """The reference's constructor (transport.py:19). precision (this core's): 'double' or 'mixed' for this object
+        (the form of the batched FCT passes); None takes the grid's form."""
         if not isinstance(dg, DeviceGrid):
             raise TypeError('Transport: dg must be an isw DeviceGrid')
+        if precision not in (None, 'double', 'mixed'):
+            raise ValueError(f'Transport: precision {precision!r}, want double or mixed')
         self.dg, self.L, self.beta, self.K = dg, layers, beta, tracers
         h = ctypes.c_void_p()
-        prec = _lib.ISW_MIXED if dg.mixed else _lib.ISW_FP64
+        mixed = dg.mixed if precision is None else precision == 'mixed'
+        prec = _lib.ISW_MIXED if mixed else _lib.ISW_FP64
         _lib.check(_lib.isw_transport_create(dg.handle, int(layers), float(beta), int(tracers), prec, ctypes.byref(h)))
         self._h = h
 

@@ -12,18 +12,33 @@ from .transport import Transport
 
 NFAST = 20
 
+# Stacks that the mixed form runs in FP64, by grid level. Measured against the FP64 form over 10 model days
+# (isw.accuracy.member): every stack of the mixed form stays within 1e-5 relative L2 in h and u except the ocean stack at
+# levels 4 and 5, whose jet over the coarse grid amplifies any perturbation by ~2.6x per model day: the FP64 form itself,
+# started from h x (1 + 1e-8 r), ends 1e-6 (h) and 1e-5 .. 1e-4 (u) away after 10 days, so FP32 momentum's rounding
+# (1e-7 relative per step in the balanced PV flux and pressure gradient) ends at 1e-5 .. 6e-4. Those stacks run in the
+# FP64 form inside mixed batches (a batch holds stacks of both forms); the air stacks and every finer level stay mixed.
+FP64_IN_MIXED = {4: ('ocean',), 5: ('ocean',)}
+
+
+def fp64_stack_kinds(level):
+    """The stack kinds a mixed-form member at this grid level runs in the FP64 form."""
+    return FP64_IN_MIXED.get(int(level), ())
+
 
 class Stack:
-    def __init__(self, dg, state, dt, nfast=NFAST, ntracers=None, device=None):
+    def __init__(self, dg, state, dt, nfast=NFAST, ntracers=None, device=None, precision=None):
+        """precision: 'double' or 'mixed' for this stack's Layers and Transport; None takes the grid's form."""
         self.dg, self.dt, self.nfast = dg, float(dt), int(nfast)
         dev = torch.device(f'cuda:{dg.device}' if device is None else device)
         s = state
         self.L = s['L']
+        self.kind = s.get('kind')
         self.core = Layers(dg, self.L, b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'],
-                           vmix=s.get('vmix', 0.0))
+                           vmix=s.get('vmix', 0.0), precision=precision)
         tr = s['tracers'] if ntracers is None else s['tracers'][:ntracers]
         self.T = len(tr)
-        self.tr = Transport(dg, layers=self.L, tracers=max(1, self.T))
+        self.tr = Transport(dg, layers=self.L, tracers=max(1, self.T), precision=precision)
         A = torch.as_tensor(dg.host.areaCell, dtype=torch.float64, device=dev)
         self.h = torch.as_tensor(np.ascontiguousarray(s['h']), dtype=torch.float64, device=dev)
         self.u = torch.as_tensor(np.ascontiguousarray(s['u']), dtype=torch.float64, device=dev)
@@ -68,15 +83,19 @@ class Stack:
 class Member:
     """One benchmark member: the air and ocean stacks of one seed on one grid (kinds=('air',) for the 3-layer form).
     batch: an isw.batch.Batch to register the stacks with (they are then advanced by Batch.step, all stacks in one
-    launch); None steps them call by call. init_device: synthesise the random initial fields on that CUDA device."""
+    launch); None steps them call by call. init_device: synthesise the random initial fields on that CUDA device.
+    fp64_kinds: the stack kinds to run in the FP64 form when the grid's form is mixed; None applies FP64_IN_MIXED, ()
+    keeps every stack mixed."""
 
     def __init__(self, dg, seed, ntracers=3, perturb=0.01, dt=None, nfast=NFAST, batch=None, kinds=('air', 'ocean'),
-                 init_device=None):
+                 init_device=None, fp64_kinds=None):
         g = dg.host
         dt = cases.stack_dt(g.n) if dt is None else dt
         topo = cases.topography(g, seed, device=init_device)
+        fk = _fp64_kinds(dg, fp64_kinds)
         self.stacks = [Stack(dg, cases.stack_state(g, kind, seed, perturb=perturb, ntracers=ntracers, topo=topo,
-                                                   device=init_device), dt, nfast)
+                                                   device=init_device), dt, nfast,
+                             precision='double' if kind in fk else None)
                        for kind in kinds]
         self.dt = float(dt)
         self.batch, self.slots = batch, []
@@ -85,12 +104,13 @@ class Member:
                 self.slots.append(s.register(batch))
 
     @classmethod
-    def from_states(cls, dg, states, dt=None, nfast=NFAST, batch=None):
+    def from_states(cls, dg, states, dt=None, nfast=NFAST, batch=None, fp64_kinds=None):
         """A member from prepared stack states (cases.stack_state dicts), e.g. initial conditions that came with a
-        request; nothing is synthesised here."""
+        request; nothing is synthesised here. fp64_kinds as for the constructor."""
         self = cls.__new__(cls)
         dt = cases.stack_dt(dg.host.n) if dt is None else dt
-        self.stacks = [Stack(dg, s, dt, nfast) for s in states]
+        fk = _fp64_kinds(dg, fp64_kinds)
+        self.stacks = [Stack(dg, s, dt, nfast, precision='double' if s.get('kind') in fk else None) for s in states]
         self.dt = float(dt)
         self.batch, self.slots = batch, []
         if batch is not None:
@@ -128,6 +148,12 @@ class Member:
         nu4 = any(s.core.nu4 for s in self.stacks)
         tr = any(s.T for s in self.stacks)
         return 1 + (3 if nu4 else 0) + 3 * 5 + (3 * info['groups'] if info['tiles'] else 2 * n) + 1 + (6 if tr else 0)
+
+
+def _fp64_kinds(dg, fp64_kinds):
+    if not dg.mixed:
+        return ()
+    return fp64_stack_kinds(dg.host.n) if fp64_kinds is None else tuple(fp64_kinds)
 
 
 def planet_grid(g, omega=cases.OMEGA_EARTH):

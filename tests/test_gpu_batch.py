@@ -222,6 +222,39 @@ def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
         assert torch.equal(x, y) and torch.equal(x, z)
 
 
+def test_batch_of_both_forms(dev, grid4):
+    """One batch holding FP64 and mixed stacks (each phase one kernel per form, the mixed stacks' fast loop in tiles, the
+    FP64 stacks' as grid-wide sub-steps): every FP64 stack equals the same stack in an FP64-only batch bit for bit, and
+    every mixed stack equals the same stack in a mixed-only batch bit for bit."""
+    from isw import gpu
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg = DeviceGrid(planet_grid(grid4))
+    gpu.set_precision('mixed')
+    try:
+        dgm = DeviceGrid(planet_grid(grid4))
+    finally:
+        gpu.set_precision('double')
+    both, only64, onlym = Batch(0), Batch(0), Batch(0)
+    a = [Member(dgm, 60, ntracers=2, batch=both, fp64_kinds=('ocean',)), Member(dg, 61, ntracers=2, batch=both)]
+    b = [Member(dg, 60, ntracers=2, batch=only64, kinds=('ocean',)), Member(dg, 61, ntracers=2, batch=only64)]
+    c = Member(dgm, 60, ntracers=2, batch=onlym, kinds=('air',), fp64_kinds=())
+    assert [s.core.precision for s in a[0].stacks] == [1, 0]
+    info = both.info()
+    assert info['tiles'] > 0, info
+    for _ in range(4):
+        for bt in (both, only64, onlym):
+            bt.step()
+    torch.cuda.synchronize()
+    for bt in (both, only64, onlym):
+        assert bt.status() == 0
+    pairs = list(zip(a[0].stacks[1].state(), b[0].stacks[0].state())) + list(zip(a[1].state(), b[1].state()))
+    pairs += list(zip(a[0].stacks[0].state(), c.stacks[0].state()))
+    for x, y in pairs:
+        assert torch.equal(x, y)
+
+
 @pytest.mark.parametrize('precision', ['double', 'mixed'])
 def test_packed_groups_equal_shared(dev, grid4, precision):
     """Eight members in the packed layout (tiles of about 64 owned cells, more tiles than one cooperative launch holds,
@@ -238,7 +271,7 @@ def test_packed_groups_equal_shared(dev, grid4, precision):
         packed.config(tiles=True, tile_k=4, layout='packed', tile_cells=64, blocks_per_sm=2)
         shared.config(tiles=True, tile_k=4, layout='shared')
         flat.config(tiles=False)
-        ms = [[Member(dg, 20 + i, ntracers=2, batch=bt) for i in range(8)] for bt in (packed, shared, flat)]
+        ms = [[Member(dg, 20 + i, ntracers=2, batch=bt, fp64_kinds=()) for i in range(8)] for bt in (packed, shared, flat)]
     finally:
         gpu.set_precision('double')
     info = packed.info()
