@@ -146,22 +146,41 @@ def ensure_oracle():
         M.build()
 
 
-def run_reference(args, rank):
-    """The reference arm: its own kernels (oracle/_ref) on the host cores, rank 0 only."""
+def member_config(args, g, world):
+    """The `config` of the member workload: the same dict in both arms, so their lines describe one workload."""
+    return dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s',
+                level=args.level, cells=int(g.N), edges=int(g.E), vertices=int(g.NV), parallelism=f'replicas x{world}',
+                l2='GPU arm: L2 flushed between timed steps (252 MB write); CPU arm: no GPU cache involved')
+
+
+def reference_grid(level):
+    """The reference's own level-n grid (oracle/_ref, built by its Python from its Lloyd positions), with the workload's
+    rotation; None where it was not built. Host arrays only: nothing of isw's device code is loaded."""
+    from oracle import build_ref
+    p = build_ref.grid_path(level)
+    if not p.exists():
+        return None
+    from isw import grid as G                # host-side container (NumPy), no device library
+    return G.for_planet(G.load(p), 6.371e6, 7.292e-5, 9.80616)
+
+
+def run_reference(args, rank, world):
+    """The reference arm: its own kernels (oracle/_ref, built for the host) in its step sequence, on its own grid
+    (oracle/_ref/grid_n<level>.npz), on the host cores, rank 0 only. Loads nothing of isw's device library."""
     if rank != 0:
         return
     from oracle import refkernels
     threads = os.cpu_count() or 1
-    out = dict(metric=metric_name(args.level), unit='model days/s', impl='reference', n_gpus=args.gpus, steps=args.steps,
-               warmup=args.warmup, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64', data='synthetic',
-               config=dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s'))
-    if not refkernels.available():
-        out['unavailable'] = 'oracle/_ref was not built (the reference sources were absent when build() ran)'
+    out = dict(metric=metric_name(args.level), unit='model days/s', impl='reference', n_gpus=world, steps=args.steps,
+               warmup=args.warmup, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64', data='synthetic')
+    g = reference_grid(args.level) if refkernels.available() else None
+    if g is None:
+        out['unavailable'] = ('oracle/_ref was not built (the reference sources were absent when build() ran)'
+                              if not refkernels.available() else f'oracle/_ref/grid_n{args.level}.npz was not built')
         print(json.dumps(out), flush=True)
         return
+    out['config'] = member_config(args, g, world)
     ensure_oracle()
-    import torch
-    g, _ = build_grid(args.level, 0 if torch.cuda.is_available() else 'cpu')
     step, dt = cpu_member(g, 0, 'reference')
     for _ in range(max(0, min(args.warmup, 1))):
         step()
@@ -169,7 +188,8 @@ def run_reference(args, rank):
     v = dt / SECONDS_PER_DAY / sec
     out.update(value=v, ms_per_step=sec * 1e3,
                cpu_baseline=dict(value=v, unit='model days/s', cores=threads, kind='reference',
-                                 sample=f'{n} full steps of the workload (reference kernels compiled for the host, OpenMP over blocks)'),
+                                 sample=f'{n} full steps of the workload (reference kernels compiled for the host, OpenMP over '
+                                        f'blocks, on the reference-built level-{args.level} grid)'),
                e2e=dict(value=v, unit='model days/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(out), flush=True)
 
@@ -189,6 +209,35 @@ def job_value(world, dt, ms):
     """Model days per second of the whole job: `world` replicas, each advancing dt seconds of model time per step of
     ms milliseconds (the max over ranks)."""
     return world * (dt / SECONDS_PER_DAY) / (ms / 1e3)
+
+
+def free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        return s.getsockname()[1]
+
+
+def spawn_ranks(n):
+    """Run this benchmark as n ranks on one node (torch.distributed.run, rendezvous on 127.0.0.1); its exit code."""
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1', f'--nproc-per-node={n}', '--master-addr', '127.0.0.1',
+           '--master-port', str(free_port()), str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def run_plumbing(args, rank, world, dist):
+    """The multi-rank path without a GPU: every rank times a fixed host loop as its 'step' (the ranks' times differ),
+    the job takes the slowest rank's time, and rank 0 prints the line with the whole job's value."""
+    t0 = time.perf_counter()
+    x = 0.0
+    for i in range(20000 * (rank + 1)):
+        x += i * 1e-9
+    ms = (time.perf_counter() - t0) * 1e3
+    ms_max = max_over_ranks(ms, dist, 'cpu')
+    if rank == 0:
+        print(json.dumps(dict(metric='rank plumbing (no GPU work)', value=job_value(world, 300.0, ms_max), unit='model days/s',
+                              n_gpus=world, steps=1, warmup=0, ms_per_step=ms_max, rank_ms=ms, scaling='weak',
+                              impl=args.impl)), flush=True)
 
 
 def fp64_step_seconds(keys, warmup=3, steps=10):
@@ -356,24 +405,37 @@ def main():
     ap.add_argument('--requests', type=int, default=48, help='serving: requests in the stream')
     ap.add_argument('--max-days', type=float, default=30.0, help='serving: longest horizon (model days)')
     ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--plumbing', action='store_true',
+                    help='the rank plumbing alone on the CPU (gloo): ranks, barrier, max over ranks, the job value; no GPU work')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.workload != 'member' and args.impl == 'isw':
         {'ensemble': run_ensemble, 'serving': run_serving, 'accuracy': run_accuracy, 'profile': run_profile}[args.workload](args)
         return
 
+    if args.gpus > 1 and 'WORLD_SIZE' not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))         # one process per GPU, as torchrun would start them
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world != args.gpus:
+        sys.exit(f'bench: {world} ranks for --gpus {args.gpus}')
     import torch
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+        if not args.plumbing:
+            torch.cuda.set_device(local)
+        dist.init_process_group('gloo' if args.plumbing else 'nccl', timeout=datetime.timedelta(seconds=600))
+    if args.plumbing:
+        run_plumbing(args, rank, world, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.impl == 'reference':
-        run_reference(args, rank)
+        run_reference(args, rank, world)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -511,11 +573,9 @@ def main():
     out = dict(metric=metric_name(args.level), value=value, unit='model days/s', n_gpus=world, steps=args.steps,
                warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
                data='synthetic', impl='isw',
-               config=dict(workload=f'level-{args.level} member: air 3 + ocean 2 layers, 3 tracers each, nfast 20, dt 300 s',
-                           level=args.level, cells=int(g.N), edges=int(g.E), vertices=int(g.NV), precision='fp64',
-                           launch='call by call' if args.percall else 'one CUDA graph per step (phase kernels + tiled fast loop)',
-                           tiles=layout,
-                           parallelism=f'replicas x{world}', l2='flushed between timed steps (252 MB write)'),
+               config=member_config(args, g, world),
+               layout=dict(precision='fp64', tiles=layout,
+                           launch='call by call' if args.percall else 'one CUDA graph per step (phase kernels + tiled fast loop)'),
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=traffic,
                              peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step'),
                e2e=dict(value=job_value(world, dt, e2e_ms), unit='model days/s',

@@ -372,6 +372,72 @@ def test_exchange_golden(dev, isw, grid4):
         assert e <= REL, ('air', name, e)
 
 
+def test_exchange_bit_exact(dev, isw, grid4):
+    """The exchange hook alone, bit for bit against the reference's own xch_cell / xch_edge / lay_mask (built for the
+    host in oracle/_ref) on seeded states: 2, 3 and 5 Boussinesq layers, moves of both signs and zero, all at once and
+    in flow order, with thin walls; air layers with a nearly empty layer taking its neighbours' wind (h, u, M, psi bit
+    for bit; theta, which goes through pow, to 1e-14)."""
+    from oracle import refkernels
+    if not refkernels.available():
+        pytest.skip('oracle/_ref not built')
+    from isw import grid as G
+    gpu, layers, _ = isw
+    K = refkernels.RefKernels()
+    g = G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616)
+    dg = gpu.DeviceGrid(g)
+    N, E = g.N, g.E
+    rng = np.random.default_rng(11)
+    i32, f64 = np.int32, np.float64
+    wall = (rng.random(E) > 0.05).astype(f64)
+
+    def ref(L, h, u, M, psi, wx, seq, hthin=0.0, floor=1.0, theta=None, cp=1004.6, kap=287.04 / 1004.6, mask=None):
+        h, u, M, psi = h.copy(), u.copy(), M.copy(), psi.copy()
+        hold = h.copy()
+        diss = np.zeros(E)
+        K.launch('xch_cell', ((N + 255) // 256,), (256,), (i32(N), i32(L), wx, g.areaCell, h, M, psi, i32(seq)))
+        K.launch('xch_edge', ((E + 255) // 256,), (256,), (i32(N), i32(E), i32(L), wx, hold, g.eI, g.eJ, u,
+                                                           diss if theta is not None else 0, 0, f64(0.0), f64(hthin), f64(floor)))
+        if mask is not None:
+            K.launch('lay_mask', ((E + 255) // 256,), (256,), (i32(E), i32(L), mask, u))
+        if theta is not None:
+            theta = theta.copy()
+            K.launch('vmix_heat', ((N + 255) // 256,), (256,), (i32(N), i32(L), h, diss, g.cellEdge, g.le, g.de, g.areaCell,
+                                                               f64(9.80616), f64(cp), f64(kap), f64(1.0e5), theta))
+        return h, u, M, psi, theta
+
+    for L, seq, walls in ((2, 0, False), (3, 0, True), (3, 1, True), (5, 1, False), (5, 0, False)):
+        h = 50.0 + 1000.0 * rng.random((L, N))
+        u = 20.0 * rng.standard_normal((L, E))
+        psi = rng.random((L, N))
+        M = h * g.areaCell[None]
+        wx = 10.0 * rng.standard_normal((L - 1, N))
+        wx[rng.random((L - 1, N)) < 0.2] = 0.0
+        core = layers.Layers(dg, L, gprime=[0.01] * (L - 1), wall=wall if walls else None)
+        want = ref(L, h, u, M, psi, np.ascontiguousarray(wx), seq, mask=wall if walls else None)
+        got = [T(a, dev) for a in (h, u, M, psi)]
+        core.exchange(T(wx, dev), *got, seq=bool(seq))
+        torch.cuda.synchronize()
+        for name, x, w in zip('h u M psi'.split(), got, want):
+            assert np.array_equal(x.cpu().numpy(), w), (L, seq, name, rel(x.cpu().numpy(), w))
+
+    L = 3                                   # air: mass per area, a nearly empty middle layer in a quarter of the cells
+    h = 2000.0 + 3000.0 * rng.random((L, N))
+    h[1, rng.random(N) < 0.25] = 12.0 + 50.0 * rng.random()
+    u = 15.0 * rng.standard_normal((L, E))
+    psi, theta = rng.random((L, N)), 250.0 + 60.0 * rng.random((L, N))
+    M = h * g.areaCell[None]
+    wx = 3.0 * rng.standard_normal((L - 1, N))
+    core = layers.Layers(dg, L, gprime=[0.0, 0.0], floor=10.0, thin_wind=100.0,
+                         air=dict(t_ref=288.0, cp=1004.6, kappa=287.04 / 1004.6, rd=287.04))
+    want = ref(L, h, u, M, psi, np.ascontiguousarray(wx), 0, hthin=100.0, floor=10.0, theta=theta)
+    got = [T(a, dev) for a in (h, u, M, psi, theta)]
+    core.exchange(T(wx, dev), *got[:4], theta=got[4])
+    torch.cuda.synchronize()
+    for name, x, w in zip('h u M psi'.split(), got, want):
+        assert np.array_equal(x.cpu().numpy(), w), ('air', name, rel(x.cpu().numpy(), w))
+    assert rel(got[4].cpu().numpy(), want[4]) <= 1e-14
+
+
 def test_option_branches_golden(dev, isw, grid4):
     """Every option branch of Boussinesq layers at once on the reference's outcrop case (walls, the shelf with its bed
     flags, per-cell buoyancy, a tide potential, the bottom's quadratic and internal-tide drag), set as the reference's

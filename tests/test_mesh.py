@@ -105,3 +105,41 @@ def test_gpu_lloyd(grid4):
     g6 = G.build(6, device=0)
     topo, worst = identities(g6)
     assert topo and worst <= 1e-12
+
+
+def _reference_grid6():
+    from oracle import build_ref
+    p = build_ref.grid_path(6)
+    if not p.exists():
+        pytest.skip('the reference-built level-6 grid (oracle/_ref) is not present')
+    from isw import grid as G
+    return G.load(p)
+
+
+def test_level6_tables_bit_exact_from_reference_positions():
+    """Level 6: from the positions the reference's own Lloyd iteration gave (tests/golden/pos_n6.npz), the mesh
+    builder reproduces every integer table of the grid the reference's own Python builds from them (oracle/_ref,
+    oracle/build_ref.py) bit for bit, and its geometry to 1e-14."""
+    from isw import grid as G
+    ref = _reference_grid6()
+    with np.load(GOLDEN / 'pos_n6.npz') as z:
+        v1 = z['pos']
+        assert int(z['lloydIters']) == int(ref.lloydIters)
+    g = G.build(6, pos_v1=v1, device='cpu')
+    for k in INTS:
+        a, b = np.asarray(getattr(g, k)), np.asarray(getattr(ref, k))
+        assert a.shape == b.shape and np.array_equal(a, b), k
+    for k in FLOATS:
+        a, b = np.asarray(getattr(g, k), dtype=float), np.asarray(getattr(ref, k), dtype=float)
+        assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b)), k
+
+
+def test_full_build_level6_lloyd_matches_reference():
+    """A full level-6 build on the host cores takes the reference's Lloyd iteration count (5412) and lands on its
+    positions to rounding."""
+    from isw import grid as G
+    with np.load(GOLDEN / 'pos_n6.npz') as z:
+        v1, iters = z['pos'], int(z['lloydIters'])
+    g = G.build(6, order='v1', device='cpu')
+    assert g.lloydIters == iters
+    assert np.max(np.abs(g.pos - v1)) <= 1e-13

@@ -44,3 +44,30 @@ def test_single_process_passes_through():
     import bench
     assert bench.max_over_ranks(3.5, None, 'cpu') == 3.5
     assert bench.job_value(1, 300.0, 1.0) == pytest.approx(300.0 / 86400.0 / 1e-3)
+
+
+def test_plain_gpus_2_call_starts_two_ranks():
+    """`bench.py --gpus 2` without torchrun starts the two ranks itself (torch.distributed.run on 127.0.0.1); their
+    plumbing runs on gloo here: rank 0 prints one line for the whole job, with the slowest rank's time."""
+    import json
+    import subprocess
+    env = dict(os.environ)
+    for k in ('WORLD_SIZE', 'RANK', 'LOCAL_RANK', 'MASTER_ADDR', 'MASTER_PORT'):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, str(ROOT / 'bench.py'), '--gpus', '2', '--plumbing'], env=env, cwd=ROOT,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith('{')]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d['n_gpus'] == 2
+    assert d['ms_per_step'] >= d['rank_ms']                 # rank 0 ran the shorter loop; the job takes the max
+    assert d['value'] == pytest.approx(2 * (300.0 / 86400.0) / (d['ms_per_step'] / 1e3))
+
+
+def test_rank_count_must_match_gpus():
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE='1', RANK='0', LOCAL_RANK='0')
+    r = subprocess.run([sys.executable, str(ROOT / 'bench.py'), '--gpus', '2', '--plumbing'], env=env, cwd=ROOT,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and '1 ranks for --gpus 2' in r.stderr
