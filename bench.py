@@ -12,10 +12,14 @@ spherical-harmonic terrain, 1% perturbations, random tracers); the grid is built
     python bench.py --workload accuracy    # mixed form against FP64: level-6 member 10 days, level-7 Galewsky 6 days
     python bench.py --workload profile --form double|mixed --steps 5   # untimed steps, for ncu launch lists
 
+On one GPU the line also carries `level7` (the same member at level 7, beyond the L2, both forms), `ensemble` (the
+64-member mixed ensemble, a few timed steps, with the sequential FP64 loop beside it) and `serving` (a shortened
+Poisson stream); `--no-configs` leaves them out.
+
 Under torchrun (N > 1) every rank advances its own member (replicas: the members are independent) and rank 0 prints
-one JSON line with the whole job's model days per second (the max step time over ranks). `--impl reference` times
-the reference's own kernels compiled for the host (oracle/_ref), driven through the reference's step sequence, on the
-host cores, rank 0 only.
+one JSON line with the whole job's model days per second (the max step time over ranks); `--gpus N` without torchrun
+starts the N ranks itself. `--impl reference` times the reference's own kernels compiled for the host (oracle/_ref),
+driven through the reference's step sequence on the reference's own level-6 grid, on the host cores, rank 0 only.
 """
 import argparse
 import json
@@ -112,7 +116,7 @@ def cpu_member(g, seed, backend):
     for kind in ('air', 'ocean'):
         s = cases.stack_state(g, kind, seed, ntracers=3, topo=topo)
         core = M.Layers(og, s['L'], b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'],
-                        vmix=s['vmix'], backend=backend)
+                        vmix=s['vmix'], vmix_cd=s.get('vmix_cd', 0.0), backend=backend)
         tr = M.Transport(og, layers=s['L'], tracers=3, backend=backend)
         h, u = s['h'].copy(), s['u'].copy()
         Mm = h * g.areaCell[None]
@@ -269,7 +273,7 @@ def fp64_step_seconds(keys, warmup=3, steps=10):
     return out
 
 
-def run_ensemble(args):
+def ensemble_result(steps, warmup, autotune_steps=3):
     """64 five-layer members (40 at level 5, 16 at level 6, 8 at level 7), seeds base + index, 0.5% perturbations, 2 FCT
     tracers, mixed precision, in one batch (one CUDA graph per step, tile layout by the autotuner); member-days/s
     against a sequential loop of the plain FP64 core over the same members."""
@@ -279,46 +283,57 @@ def run_ensemble(args):
     t = time.time()
     ens = Ensemble.build(levels, seed=100, perturb=0.005, ntracers=2, precision='mixed', device=0)
     t_build = time.time() - t
-    best, times = ens.batch.autotune(steps=3)
+    best, times = ens.batch.autotune(steps=autotune_steps)
     layout = ens.batch.info()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         ens.step()
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         e0.record(st)
-        for _ in range(args.steps):
+        for _ in range(steps):
             ens.step()
         e1.record(st)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     finite = all(bool(torch.isfinite(a).all()) for m in ens for a in m.state())
     value = ens.member_days_per_step() / (ms / 1e3)
+    launches = ens.members[0].launches() * steps
+    footprint = ens.footprint()
+    del ens
     base = fp64_step_seconds([(n, 5) for n in set(levels)])
-    seq = ens.member_days_per_step() / sum(base[(n, 5)] for n in levels)
-    out = dict(metric='ensemble member-days/s: 64 five-layer members (40 x level 5, 16 x level 6, 8 x level 7), mixed form',
-               value=value, unit='member-days/s', n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
-               higher_is_better=True, scaling='weak', vs_baseline=None,
-               dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
-               impl='isw',
-               config=dict(workload='config-4 ensemble: 64 members, air 3 + ocean 2 layers, 2 tracers, 0.5% perturbations',
-                           members=len(levels), stacks=layout['stacks'], tiles=layout, autotuned=best,
-                           device_bytes=ens.footprint(), l2='state far larger than L2 (no flush needed)'),
-               sequential_fp64=dict(value=seq, unit='member-days/s', ms_per_member_step={f'level{k[0]}': v * 1e3 for k, v in base.items()},
-                                    note='each member stepped alone on the plain FP64 core, one after another'),
-               speedup_vs_sequential_fp64=value / seq, gpu_launches=None, clocks=clk.summary(), finite=finite,
-               build_s=t_build, autotune_ms={str(k): v for k, v in times.items()})
-    print(json.dumps(out), flush=True)
+    days = sum(cases_dt(n) for n in levels) / SECONDS_PER_DAY
+    seq = days / sum(base[(n, 5)] for n in levels)
+    return dict(metric='ensemble member-days/s: 64 five-layer members (40 x level 5, 16 x level 6, 8 x level 7), mixed form',
+                value=value, unit='member-days/s', n_gpus=1, steps=steps, warmup=warmup, ms_per_step=ms,
+                higher_is_better=True, scaling='weak', vs_baseline=None,
+                dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
+                impl='isw',
+                config=dict(workload='ensemble: 64 members, air 3 + ocean 2 layers, 2 tracers, 0.5% perturbations',
+                            members=len(levels), l2='state far larger than L2 (no flush needed)'),
+                layout=dict(stacks=layout['stacks'], tiles=layout, autotuned=best), device_bytes=footprint,
+                sequential_fp64=dict(value=seq, unit='member-days/s', ms_per_member_step={f'level{k[0]}': v * 1e3 for k, v in base.items()},
+                                     note='each member stepped alone on the plain FP64 core, one after another'),
+                speedup_vs_sequential_fp64=value / seq, gpu_launches=launches, clocks=clk.summary(), finite=finite,
+                build_s=t_build, autotune_ms={str(k): v for k, v in times.items()})
 
 
-def run_serving(args):
-    """Seeded Poisson requests (rate 50 per second of the server's wall clock; level 4..7, horizon 1..30 model days
+def cases_dt(level):
+    from isw import cases
+    return cases.stack_dt(level)
+
+
+def run_ensemble(args):
+    print(json.dumps(ensemble_result(args.steps, args.warmup)), flush=True)
+
+
+def serving_result(requests, max_days, seed):
+    """Seeded Poisson requests (rate 50 per second of the server's wall clock; level 4..7, horizon 1..max_days model days
     log-uniform, 3 or 5 layers), served with continuous batching in the mixed form under a 150 GB budget; p50/p99
     time-to-completion and member-days/s, against the plain FP64 core serving the same stream one request at a time."""
-    import torch
     from isw.serving import Server, poisson_requests, sequential_baseline
-    reqs = poisson_requests(args.requests, 50.0, seed=args.seed, days=(1.0, args.max_days))
+    reqs = poisson_requests(requests, 50.0, seed=seed, days=(1.0, max_days))
     srv = Server(0, budget_bytes=150e9, precision='mixed', ntracers=2)
     srv.batch.config(layout='packed')
     for n in sorted({r.level for r in reqs}):          # grids and the requests' initial states exist before the clock starts
@@ -326,26 +341,30 @@ def run_serving(args):
     srv.prepare(reqs)
     with ClockSampler(0) as clk:
         results, stats = srv.run(reqs)
+    del srv
     base = fp64_step_seconds({(r.level, r.layers) for r in reqs})
-    from isw import cases
+
     def days_of(r):
-        dt = cases.stack_dt(r.level)
+        dt = cases_dt(r.level)
         n = max(1, int(math.ceil(r.days * SECONDS_PER_DAY / dt - 1e-9)))
         return n, n * dt / SECONDS_PER_DAY
     seq = sequential_baseline(reqs, base, days_of)
-    out = dict(metric='serving: p50/p99 time-to-completion (s) and member-days/s, Poisson stream of forecast requests, mixed form',
-               value=stats['member_days_per_s'], unit='member-days/s', p50_s=stats['p50_s'], p99_s=stats['p99_s'],
-               n_gpus=1, steps=stats['batched_steps'], warmup=0, higher_is_better=True, scaling='weak', vs_baseline=None,
-               dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
-               impl='isw',
-               config=dict(workload=f'config-5 serving: {args.requests} requests, Poisson rate 50/s (server wall clock), '
-                                    f'level 4..7, horizon 1..{args.max_days:g} model days log-uniform, 3 or 5 layers, 2 tracers',
-                           budget_bytes=150e9, seed=args.seed),
-               stats=stats,
-               sequential_fp64=dict(seq, note='the same stream served one request at a time (FIFO) on the plain FP64 core, '
-                                              'service times from measured per-step times'),
-               clocks=clk.summary())
-    print(json.dumps(out), flush=True)
+    return dict(metric='serving: p50/p99 time-to-completion (s) and member-days/s, Poisson stream of forecast requests, mixed form',
+                value=stats['member_days_per_s'], unit='member-days/s', p50_s=stats['p50_s'], p99_s=stats['p99_s'],
+                n_gpus=1, steps=stats['batched_steps'], warmup=0, higher_is_better=True, scaling='weak', vs_baseline=None,
+                dtype='f32 momentum, TRiSK operators and FCT corrections; f64 thickness, masses, budgets', data='synthetic',
+                impl='isw',
+                config=dict(workload=f'serving: {requests} requests, Poisson rate 50/s (server wall clock), '
+                                     f'level 4..7, horizon 1..{max_days:g} model days log-uniform, 3 or 5 layers, 2 tracers',
+                            budget_bytes=150e9, seed=seed),
+                stats=stats,
+                sequential_fp64=dict(seq, note='the same stream served one request at a time (FIFO) on the plain FP64 core, '
+                                               'service times from measured per-step times'),
+                clocks=clk.summary())
+
+
+def run_serving(args):
+    print(json.dumps(serving_result(args.requests, args.max_days, args.seed)), flush=True)
 
 
 def run_profile(args):
@@ -395,6 +414,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
     ap.add_argument('--percall', action='store_true', help='step call by call (one graph per stack) instead of the batched launch')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed precision form')
+    ap.add_argument('--no-configs', action='store_true', help='skip the level-7, ensemble and serving sub-measurements')
     ap.add_argument('--batched', type=int, default=8, help='members of the batched-core measurement (0: skip)')
     ap.add_argument('--workload', default='member', choices=('member', 'ensemble', 'serving', 'accuracy', 'profile'))
     ap.add_argument('--form', default='double', choices=('double', 'mixed'), help='profile: the precision form')
@@ -451,10 +471,10 @@ def main():
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
-    def make(precision):
+    def make(precision, grid=None):
         set_precision(precision)
         try:
-            dg = DeviceGrid(g, device=local)
+            dg = DeviceGrid(g if grid is None else grid, device=local)
             batch = None if args.percall else Batch(local)
             m = Member(dg, seed=rank, batch=batch)
         finally:
@@ -558,11 +578,12 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dist, dev)
     io_bytes = sum(a.numel() * a.element_size() for a in member.state())
 
-    bytes_step = 0
+    impl_bytes = 0
     for s in member.stacks:
         N, E, NV, nE2 = roofline.grid_sizes(g)
-        bytes_step += roofline.layers_step_bytes(N, E, NV, nE2, s.L, s.nfast, nu4=bool(s.core.nu4), vmix=bool(s.core.vmix))
-        bytes_step += roofline.transport_bytes(N, E, s.L, s.T)
+        impl_bytes += roofline.layers_step_bytes(N, E, NV, nE2, s.L, s.nfast, nu4=bool(s.core.nu4), vmix=bool(s.core.vmix))
+        impl_bytes += roofline.transport_bytes(N, E, s.L, s.T)
+    bytes_step = roofline.minimal_member_bytes(g.E, 'double')
     peak, peak_kind = peaks()
     achieved = bytes_step / (ms / 1e3) / 1e9
     traffic = None
@@ -577,7 +598,9 @@ def main():
                layout=dict(precision='fp64', tiles=layout,
                            launch='call by call' if args.percall else 'one CUDA graph per step (phase kernels + tiled fast loop)'),
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak, traffic=traffic,
-                             peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step'),
+                             peak_kind=peak_kind, algorithmic_bytes_per_step=bytes_step, unit_of_work='one member step',
+                             bytes_model='minimal phase decomposition (compulsory traffic)',
+                             implementation_bytes_per_step=impl_bytes),
                e2e=dict(value=job_value(world, dt, e2e_ms), unit='model days/s',
                         h2d_bytes_per_step=io_bytes, d2h_bytes_per_step=io_bytes),
                gpu_launches=member.launches() * args.steps, clocks=clk.summary(), finite=finite, grid_build_s=t_grid)
@@ -590,12 +613,42 @@ def main():
     if batched is not None:
         out['batched'] = batched
 
+    if world == 1 and not args.no_configs and not args.percall:
+        # the beyond-L2 member (level 7, both forms) and the ensemble and serving workloads, shortened to a few
+        # timed steps and a short request stream so that the default run stays within a few minutes
+        g7, _ = build_grid(7, local)
+        l7 = dict(level=7, cells=int(g7.N), edges=int(g7.E))
+        for form in ('double', 'mixed'):
+            m7, lay7 = make(form, g7)
+            t7 = timed(m7)
+            l7[form] = dict(ms_per_step=t7, value=job_value(1, m7.dt, t7), unit='model days/s', layout=lay7,
+                            finite=all(bool(torch.isfinite(a).all()) for a in m7.state()))
+            if form == 'double':
+                a7 = roofline.minimal_member_bytes(g7.E, 'double') / (t7 / 1e3) / 1e9
+                l7[form]['roofline'] = dict(achieved=a7, peak=peak, unit='GB/s', frac=a7 / peak,
+                                            algorithmic_bytes_per_step=roofline.minimal_member_bytes(g7.E, 'double'))
+            del m7
+        l7['mixed_vs_fp64'] = l7['mixed']['value'] / l7['double']['value']
+        out['level7'] = l7
+        keep = ('metric', 'value', 'unit', 'ms_per_step', 'steps', 'warmup', 'p50_s', 'p99_s', 'config', 'layout',
+                'sequential_fp64', 'speedup_vs_sequential_fp64', 'device_bytes', 'finite', 'gpu_launches', 'stats')
+        ens = ensemble_result(steps=5, warmup=3, autotune_steps=2)
+        out['ensemble'] = {k: v for k, v in ens.items() if k in keep}
+        srv = serving_result(requests=24, max_days=3.0, seed=args.seed)
+        out['serving'] = {k: v for k, v in srv.items() if k in keep}
+        out['serving']['note'] = 'a shortened stream (24 requests, horizons 1..3 model days); --workload serving runs the full one'
+
     if rank == 0 and world == 1 and not args.no_cpu:
         ensure_oracle()
         step, _ = cpu_member(g, 0, 'oracle')
         sec, n = time_cpu(step, budget_s=15.0, max_steps=50)
         out['cpu_baseline'] = dict(value=dt / SECONDS_PER_DAY / sec, unit='model days/s', cores=os.cpu_count() or 1, kind='port',
                                    sample=f'{n} full steps of the same member (the C oracle, OpenMP on all host threads)')
+        # the single-process leg: the same kernels as whole-array NumPy operations, one process, no threads
+        step, _ = cpu_member(g, 0, 'numpy')
+        sec, n = time_cpu(step, budget_s=8.0, max_steps=5)
+        out['cpu_baseline_numpy'] = dict(value=dt / SECONDS_PER_DAY / sec, unit='model days/s', cores=1, kind='port',
+                                         sample=f'{n} full steps of the same member (the oracle kernels in NumPy, one process)')
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

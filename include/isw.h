@@ -204,6 +204,11 @@ int isw_batch_step(isw_batch *b, void *stream);
  * 64..4096, 0 = by blocks per SM; stacks packed into cooperative launches of at most SMs x blocks-per-SM tiles).
  * blocks_per_sm: 0 choose, 1 (1024-thread tiles) or 2 (512-thread tiles). */
 int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, int tile_cells, int blocks_per_sm);
+/* The grid-wide sub-steps of the untiled stacks (persistent != 0): one cooperative launch per stage and precision form
+ * whose co-resident blocks run every sub-step, meeting at a bounded grid barrier after each cell pass and each edge pass,
+ * instead of two kernel launches per sub-step (0, the default). Results are bit-identical either way. This core's own
+ * layout choice: no counterpart in the reference (whose Layers.step launches two kernels per sub-step, layers.py:168-175). */
+int isw_batch_grid_loop(isw_batch *b, int persistent);
 /* Pipelined steps (on != 0): each isw_batch_step queues a step's dynamics beside the previous step's transport (two
  * branches of one graph, the step's layer fluxes Fm double-buffered), so the registered masses M and tracers lag the
  * dynamics by one step until isw_batch_flush, which completes the last step's transport and puts its Fm in the

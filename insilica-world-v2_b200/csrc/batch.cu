@@ -245,6 +245,46 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
   }
 }
 
+// The grid-wide fast loop of stage `st` for the untiled FP64 stacks as ONE cooperative launch of co-resident blocks: each
+// sub-step every block walks its share of the cell chunks (the eta pass), all blocks meet at the bounded grid barrier,
+// walk the edge chunks (the ubar pass; with flux != 0 a stack's last sub-step also forms its layer fluxes, as PH_UF
+// does) and meet again. The per-item arithmetic is PH_ETA's and PH_U's / PH_UF's, which otherwise take two launches
+// per sub-step; the barrier's acquire makes every block's writes of one pass visible to the next pass.
+__global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restrict__ S, const Sched sc, int st, int nsub,
+                                                        int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
+  __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
+  const StackDesc &d = *reinterpret_cast<const StackDesc *>(buf);
+  int cur = -1;
+  auto select = [&](int s) {                 // the chunk's stack descriptor in shared memory (s is block-uniform)
+    if (s == cur) return;
+    __syncthreads();
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(S + s);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(buf);
+    for (int w = threadIdx.x; w < (int)(sizeof(StackDesc) / 8); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    cur = s;
+  };
+  for (int j = 0; j < nsub; j++) {
+    for (int c = blockIdx.x; c < sc.ncell; c += gridDim.x) {
+      const Chunk ch = sc.cell[c];
+      select(ch.s);
+      const int i = ch.begin + (int)threadIdx.x;
+      if (i < ch.end && !d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(d.M, d.tau[st], j, i);
+    }
+    if (!grid_sync(bar, status, timeout_ns, 0)) return;
+    for (int c = blockIdx.x; c < sc.nedge; c += gridDim.x) {
+      const Chunk ch = sc.edge[c];
+      select(ch.s);
+      const int i = ch.begin + (int)threadIdx.x;
+      if (i < ch.end && !d.tiled && j < d.n[st]) {
+        fp64::bt_u_edge_y(d.M, d.tau[st], i);
+        if (flux && j == d.n[st] - 1) fp64::flux_edge<false>(d.M, stage_args(d, st), d.M.acc[i], i);
+      }
+    }
+    if (!grid_sync(bar, status, timeout_ns, 0)) return;
+  }
+}
+
 }  // namespace
 }  // namespace isw
 
@@ -296,6 +336,9 @@ struct isw_batch {
   int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
   int layout = 0;                             // 0: choose; 1 shared; 2 packed
   bool pdl = true;                            // programmatic dependent launch between phase kernels
+  bool fast_grid = false;                     // untiled stacks' sub-steps: one cooperative launch per stage (k_fast_grid)
+  int untiled_form[2] = {0, 0};               // per form (FP64, mixed): any untiled stack
+  int grid_blocks[2] = {0, 0};                // per form: co-resident blocks of the cooperative grid-wide fast loop
   // pipelined steps: step n's dynamics beside step n-1's transport (two branches of one graph), Fm double-buffered.
   // desc[q] describes a step whose dynamics write Fm_q and whose transport reads it: Fm_0 the registered Fm, Fm_1 fm_alt
   bool pipeline = false, primed = false;
@@ -518,6 +561,7 @@ void rebuild(isw_batch *b) {
   for (auto &sl : b->slots)
     if (sl.used && form_of(sl) == 1) b->mixed = 1;
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
+  int untiled[2] = {0, 0};
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
   int used = 0;
   for (auto &sl : b->slots) used += sl.used ? 1 : 0;
@@ -584,6 +628,7 @@ void rebuild(isw_batch *b) {
       for (int i = 0; i < n; i += THREADS) v.push_back(Chunk{s, i, std::min(n, i + THREADS)});
     };
     const int f = form_of(sl);
+    if (!d.tiled) untiled[f] = 1;
     chunks(cell[f], d.M.g.N);
     chunks(edge[f], d.M.g.E);
     chunks(vert[f], d.M.g.NV);
@@ -655,6 +700,8 @@ void rebuild(isw_batch *b) {
       b->groups.clear();
       any_untiled = 1;
       for (auto &d : desc) d.tiled = 0;
+      for (auto &sl : b->slots)
+        if (sl.used) untiled[form_of(sl)] = 1;
     }
   }
   ISW_CUDA(cudaMemcpy(b->d_desc, desc.data(), sizeof(StackDesc) * desc.size(), cudaMemcpyHostToDevice));
@@ -704,6 +751,15 @@ void rebuild(isw_batch *b) {
   b->any_tr = any_tr;
   b->any_untiled = any_untiled;
   b->lmax = kernel_lmax(lmax);
+  for (int f = 0; f < 2; f++) {
+    b->untiled_form[f] = untiled[f];
+    b->grid_blocks[f] = 0;
+    if (!untiled[f]) continue;
+    int per = 0;
+    const void *fn = f == 0 ? (const void *)k_fast_grid : fast_grid_kernel_mixed();
+    ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, THREADS, 0));
+    b->grid_blocks[f] = std::max(1, per) * b->sms;
+  }
 }
 
 // A phase over every stack: one kernel per precision form present (the FP64 stacks' first). pdl: the first of them is
@@ -761,6 +817,31 @@ void launch_fast(isw_batch *b, cudaStream_t st, int stage, long long timeout_ns,
   }
 }
 
+// The untiled stacks' sub-steps of stage `stage` as one cooperative launch per form present (flux: the last sub-step
+// also forms the layer fluxes, for a batch whose phase C only sums them).
+void launch_fast_grid(isw_batch *b, cudaStream_t st, int stage, bool flux) {
+  for (int f = 0; f < 2; f++) {
+    const Sched &sc = b->scf[f];
+    if (!b->untiled_form[f] || sc.ncell == 0) continue;
+    if (!b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
+    ISW_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->grid_blocks[f]);
+    cfg.blockDim = dim3(THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (f == 0)
+      ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status,
+                                  DEFAULT_TIMEOUT_NS));
+    else
+      launch_fast_grid_mixed(cfg, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status, DEFAULT_TIMEOUT_NS);
+  }
+}
+
 // The dynamics of one step (through the last stage's D). The first kernel and the first after a tile launch (or a
 // memset) take plain stream order; the others are programmatic dependents of the kernel before them.
 void enqueue_dyn(isw_batch *b, cudaStream_t st) {
@@ -777,14 +858,18 @@ void enqueue_dyn(isw_batch *b, cudaStream_t st) {
     const bool tiled = !b->groups.empty();
     launch_fast(b, st, s, DEFAULT_TIMEOUT_NS, -1);
     // no tiled stack: the layer fluxes are formed in the last grid-wide sub-step, once per edge, and C sums them
-    if (b->any_untiled)
+    const bool grid_loop = b->any_untiled && b->fast_grid;
+    if (grid_loop) {
+      launch_fast_grid(b, st, s, !tiled);
+    } else if (b->any_untiled) {
       for (int j = 0; j < b->nsub[s]; j++) {
         launch_phase<PH_ETA>(b, st, s, j, !(tiled && j == 0));
         if (tiled) launch_phase<PH_U>(b, st, s, j);
         else launch_phase<PH_UF>(b, st, s, j);
       }
-    if (tiled) launch_phase<PH_C>(b, st, s, 0, b->any_untiled);
-    else launch_phase<PH_CS>(b, st, s, 0);
+    }
+    if (tiled) launch_phase<PH_C>(b, st, s, 0, b->any_untiled && !grid_loop);
+    else launch_phase<PH_CS>(b, st, s, 0, !grid_loop);
     launch_phase<PH_D>(b, st, s, 0);
   }
 }
@@ -1027,6 +1112,16 @@ int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, in
     b->layout = layout;
     b->tile_cells = tile_cells;
     b->force_bps = blocks_per_sm;
+    b->dirty = true;
+  });
+}
+
+int isw_batch_grid_loop(isw_batch *b, int persistent) {
+  return guarded([&] {
+    if (!b) fail(ISW_EINVAL, "batch.grid_loop: null handle");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
+    b->fast_grid = persistent != 0;
     b->dirty = true;
   });
 }

@@ -205,6 +205,9 @@ struct Dom {
 void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage,
                         int j);
 const void *fast_kernel_mixed(int bps);
+const void *fast_grid_kernel_mixed();
+void launch_fast_grid_mixed(const cudaLaunchConfig_t &cfg, const StackDesc *desc, const Sched &sc, int stage, int nsub,
+                            int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns);
 void launch_fast_mixed(int bps, const cudaLaunchConfig_t &cfg, const StackDesc *desc, const TileRef *refs, int stage, int rounds,
                        GridBarrier *bar, BatchStatus *status, long long timeout_ns, int fault_block);
 

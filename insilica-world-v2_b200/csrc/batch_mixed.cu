@@ -318,6 +318,54 @@ void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, con
   }
 }
 
+namespace {
+
+// The grid-wide fast loop of stage `st` for the untiled mixed stacks as one cooperative launch (batch.cu's k_fast_grid
+// with the mixed form's per-item arithmetic: PH_ETA's and PH_U's / PH_UF's of k_phase_m).
+__global__ void __launch_bounds__(THREADS) k_fast_grid_m(const StackDesc *__restrict__ S, const Sched sc, int st, int nsub,
+                                                          int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
+  __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
+  const StackDesc &d = *reinterpret_cast<const StackDesc *>(buf);
+  int cur = -1;
+  auto select = [&](int s) {                 // the chunk's stack descriptor in shared memory (s is block-uniform)
+    if (s == cur) return;
+    __syncthreads();
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(S + s);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(buf);
+    for (int w = threadIdx.x; w < (int)(sizeof(StackDesc) / 8); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    cur = s;
+  };
+  for (int j = 0; j < nsub; j++) {
+    for (int c = blockIdx.x; c < sc.ncell; c += gridDim.x) {
+      const Chunk ch = sc.cell[c];
+      select(ch.s);
+      const int i = ch.begin + (int)threadIdx.x;
+      if (i < ch.end && !d.tiled && j < d.n[st]) mixed::bt_eta_cell(d.M, (float)d.tau[st], j, i);
+    }
+    if (!grid_sync(bar, status, timeout_ns, 0)) return;
+    for (int c = blockIdx.x; c < sc.nedge; c += gridDim.x) {
+      const Chunk ch = sc.edge[c];
+      select(ch.s);
+      const int i = ch.begin + (int)threadIdx.x;
+      if (i < ch.end && !d.tiled && j < d.n[st]) {
+        mixed::bt_u_edge(d.M, (float)d.tau[st], i);
+        if (flux && j == d.n[st] - 1) mixed::flux_edge(d.M, mstage_args(d, st), d.M.acc[i], i);
+      }
+    }
+    if (!grid_sync(bar, status, timeout_ns, 0)) return;
+  }
+}
+
+}  // namespace
+
+const void *fast_grid_kernel_mixed() { return (const void *)k_fast_grid_m; }
+
+void launch_fast_grid_mixed(const cudaLaunchConfig_t &cfg, const StackDesc *desc, const Sched &sc, int stage, int nsub,
+                            int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
+  ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid_m, desc, sc, stage, nsub, flux, bar, status, timeout_ns));
+}
+
 const void *fast_kernel_mixed(int bps) {
   return bps == 2 ? (const void *)k_fast_m<512, 2> : (const void *)k_fast_m<1024, 1>;
 }

@@ -45,21 +45,29 @@ class Batch:
 
     LAYOUTS = {'auto': 0, 'shared': 1, 'packed': 2}
 
-    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0):
+    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0, persistent=False):
         """The fast loop in shared-memory tiles exchanging every k <= tile_k sub-steps (the largest that fits), or
         grid-wide passes; layout 'shared' (one cooperative launch, tiles in proportion to each stack's cells), 'packed'
-        (tiles of about tile_cells owned cells, stacks packed into launches) or 'auto'; blocks_per_sm 1, 2 or 0 (auto)."""
-        self._config = dict(tiles=tiles, tile_k=tile_k, layout=layout, tile_cells=tile_cells, blocks_per_sm=blocks_per_sm)
+        (tiles of about tile_cells owned cells, stacks packed into launches) or 'auto'; blocks_per_sm 1, 2 or 0 (auto).
+        persistent: the grid-wide passes of untiled stacks as one cooperative launch per stage (co-resident blocks meeting
+        at a grid barrier after every pass) instead of two launches per sub-step."""
+        self._config = dict(tiles=tiles, tile_k=tile_k, layout=layout, tile_cells=tile_cells, blocks_per_sm=blocks_per_sm,
+                            persistent=persistent)
         _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k), self.LAYOUTS[layout], int(tile_cells),
                                          int(blocks_per_sm)))
+        _lib.check(_lib.isw_batch_grid_loop(self._h, 1 if persistent else 0))
+
+    @property
+    def persistent(self):
+        return bool(getattr(self, '_config', {}).get('persistent', False))
 
     def info(self):
         """The current layout: stacks, tiles, exchange interval k, the largest tile's shared memory (bytes), cooperative
-        launches per stage (groups), tile blocks per SM."""
+        launches per stage (groups), tile blocks per SM, and whether untiled stacks run the persistent grid-wide loop."""
         v = [ctypes.c_int() for _ in range(3)] + [ctypes.c_longlong()] + [ctypes.c_int() for _ in range(2)]
         _lib.check(_lib.isw_batch_info(self._h, *[ctypes.byref(x) for x in v]))
         return dict(stacks=v[0].value, tiles=v[1].value, tile_k=v[2].value, smem=v[3].value, groups=v[4].value,
-                    blocks_per_sm=v[5].value)
+                    blocks_per_sm=v[5].value, persistent=self.persistent)
 
     def autotune(self, steps=5, candidates=None, stream=None):
         """Choose the fast-loop layout by timing: each candidate configuration (layout, blocks per SM, exchange interval,
@@ -73,7 +81,7 @@ class Batch:
             arrays += [a for a in (h, u, Fm, M, M1) + tuple(tracers) if a is not None]
         saved = [a.clone() for a in arrays]
         if candidates is None:
-            candidates = [dict(tiles=False)]
+            candidates = [dict(tiles=False), dict(tiles=False, persistent=True)]
             for layout, bps, k in itertools.product(('shared', 'packed'), (1, 2), (2, 3, 4, 6, 8)):
                 cells = (0,) if layout == 'shared' else ((256, 512) if bps == 2 else (512, 1024))
                 for c in cells:
@@ -84,7 +92,7 @@ class Batch:
         for cand in candidates:
             self.config(**cand)
             lay = self.info()
-            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'])
+            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'], lay['persistent'])
             if key in seen:                       # the same layout as an earlier candidate
                 continue
             seen.add(key)

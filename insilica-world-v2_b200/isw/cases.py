@@ -206,24 +206,27 @@ def balanced_layers(g, H, ujets, gprime, b, floor, omega, grav=GRAV, M=20000):
 STACKS = {
     # three Boussinesq air layers of 2.5 / 3.5 / 4 km with jets 30 / 25 / 20 m/s at 45N. g' 2 and 1 m/s^2 keep the
     # grid-scale internal wave inside RK3's stability range at the stacks' step (stack_dt). The interfacial stress
-    # (5e-4 m/s: a 40-day decay between km-thick layers) locks a layer pressed to its floor over a peak to its neighbour
+    # (5e-4 m/s: a 40-day decay between km-thick layers) locks a layer pressed to its floor over a peak to its neighbour;
+    # its quadratic part (cd 1e-3, the reference's Earth-preset interface drag) stops the wind of a layer squeezed to its
+    # floor at a front from running away (without it some seeds blow up within days at levels 6 and 7)
     'air': dict(H=(2500.0, 3500.0, 4000.0), U=(30.0, 25.0, 20.0), gprime=(2.0, 1.0), base=0.0, floor=1.0,
-                stress=(0.0, 0.0, 0.0), visc4_U=20.0, knee=800.0, cap=1500.0, vmix=5e-4),
+                stress=(0.0, 0.0, 0.0), visc4_U=20.0, knee=800.0, cap=1500.0, vmix=5e-4, vmix_cd=1e-3),
     # two ocean layers of 100 / 3900 m over a flat 4 km basin floor; one barotropic 20 m/s jet (the lower layer's scaled
     # by 1 + g'/g so the interface stays parallel to the surface); bottom stress, and the reference ocean's interfacial
     # stress (its interface_stress 5e-4, reference ocean.py:32), which keeps a top layer thinned to its floor locked to the
     # layer below instead of running away. The terrain stays under the air stack only: a 20 m/s barotropic jet over
     # 2 km of random relief outruns the step within a day.
     'ocean': dict(H=(100.0, 3900.0), U=(20.0, 20.0 * (1 + 0.016 / GRAV)), gprime=(0.016,), base=-4000.0, floor=1.0,
-                  stress=(0.0, 2.5e-4), visc4_U=0.5, vmix=5e-4, flat=True),
+                  stress=(0.0, 2.5e-4), visc4_U=0.5, vmix=5e-4, vmix_cd=1e-3, flat=True),
 }
 
 
 def stack_dt(n):
-    """The stacked workloads' step: 300 s at n = 6, doubling per coarser level. The grid-scale internal wave carried
-    by the 30 m/s jet, (c1 + U) k_max dt with c1 = 64 m/s and k_max^2 the vector Laplacian's largest eigenvalue, then
-    stays near 1.2, inside RK3's sqrt(3)."""
-    return 1200.0 * 2.0 ** (4 - n)
+    """The stacked workloads' step: 300 s at n = 6, doubling per coarser level; 120 s at n = 7. The grid-scale internal
+    wave carried by the 30 m/s jet, (c1 + U) k_max dt with c1 = 64 m/s and k_max^2 the vector Laplacian's largest
+    eigenvalue, then stays near 1.2 through level 6, inside RK3's sqrt(3); at level 7 the resolved fronts carry faster
+    winds (50-80 m/s), and 150 s let some seeds' air stacks blow up within days where 120 s holds them 30 days."""
+    return 120.0 * 2.0 ** (7 - n) if n >= 7 else 1200.0 * 2.0 ** (4 - n)
 
 
 def compress_peaks(t, knee, cap):
@@ -256,4 +259,4 @@ def stack_state(g, kind, seed, perturb=0.01, ntracers=3, topo=None, omega=OMEGA_
     tr = [rng.uniform(250.0, 310.0, (L, g.N)), 5e-3 * np.exp(0.5 * rng.standard_normal((L, g.N))),
           rng.uniform(0.0, 1.0, (L, g.N))][:ntracers]
     return dict(h=h, u=u, b=b, gprime=list(c['gprime']), stress=list(c['stress']), floor=c['floor'],
-                nu4=visc4(g, c['visc4_U']), vmix=c.get('vmix', 0.0), tracers=tr, L=L, kind=kind)
+                nu4=visc4(g, c['visc4_U']), vmix=c.get('vmix', 0.0), vmix_cd=c.get('vmix_cd', 0.0), tracers=tr, L=L, kind=kind)

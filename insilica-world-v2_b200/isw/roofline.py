@@ -1,16 +1,34 @@
-"""Algorithmic bytes of one step: the compulsory DRAM traffic of the core's phase decomposition.
+"""Algorithmic bytes of one step.
+
+The roofline numerator (``minimal_member_bytes``) is the compulsory DRAM traffic of the MINIMAL phase decomposition of
+the benchmark member (air stack L = 3 + ocean stack L = 2, three FCT tracers each, nfast = 20): a phase boundary only
+where a grid-wide dependency forces one (the step's free surface; per stage the cells-and-vertices pass, the edges
+pass, two passes per barotropic sub-step, the flux limiter and the update; five FCT cell passes), each array charged
+once per phase at its stored width. At level 6 that is 870.7 MB for the air stack and 804.5 MB for the ocean stack
+per step in the FP64 form, 738 MB and 687 MB in the mixed form; other levels scale with the edge count.
+
+``layers_step_bytes`` / ``transport_bytes`` count the same way over THIS core's own decomposition, which has more
+phases (the packed edge record between E and S, phase C apart from D, the FCT's edge-flux passes), so they charge
+more bytes (1,954 MB for the level-6 member): a figure for comparing the core's phases, not the roofline's.
 
 Each phase (one grid-wide pass between two grid-wide dependencies) is charged every array it reads or writes once, at
 its stored width, as if nothing stayed on chip between phases: index tables int32 (signs and slots int8), geometry and
 state FP64. A gather that touches a neighbour's value is not charged again (the array is charged once per phase).
-This is the roofline numerator: achieved = bytes / measured time, against the measured HBM copy bandwidth. At level 6
-a member's working set (tens of MB) fits in the 126 MB L2, so the DRAM bytes ncu reports fall below this figure and
-achieved can exceed the HBM peak: the phases then run from L2.
+achieved = minimal bytes / measured time, against the measured HBM copy bandwidth. At level 6 a member's working set
+(tens of MB) fits in the 126 MB L2, so the DRAM bytes ncu reports fall below these figures: the phases run from L2.
 """
 
 import math
 
 I4, I1, F8 = 4, 1, 8
+
+LEVEL6_EDGES = 122880
+MINIMAL_MEMBER_BYTES_L6 = {'double': 870.7e6 + 804.5e6, 'mixed': 738e6 + 687e6}
+
+
+def minimal_member_bytes(E, form='double'):
+    """Compulsory bytes of one member step (air 3 + ocean 2 layers, 3 tracers each, nfast 20) on a grid of E edges."""
+    return MINIMAL_MEMBER_BYTES_L6[form] * E / LEVEL6_EDGES
 
 
 def layers_step_bytes(N, E, NV, nE2, L, nfast, nu4=True, vmix=False, Fm=True):

@@ -51,6 +51,7 @@ class Result:
     admitted: float
     done: float
     state: list = field(default_factory=list, repr=False)   # host copies of h, u (and M, tracers) per stack
+    error: str = ''         # empty for a completed forecast; else why the request was dropped
 
     @property
     def latency(self):
@@ -207,16 +208,26 @@ class Server:
             self.batch.step(st)
             st.synchronize()
             steps += 1
+            code = self.batch.status(stream=st)             # the host mirror of the status word: no device sync
+            if code == _lib.ISW_ENOTFINITE:
+                # a forecast whose state went non-finite: drop it with an error result; the step ran every other stack
+                # to completion with its own arithmetic, so they carry on once the status is cleared
+                for a in [a for a in active if not a['member'].finite()]:
+                    a['member'].unregister()
+                    active.remove(a)
+                    used -= a['bytes']
+                    req = a['req']
+                    results.append(Result(req.rid, req.level, req.layers, req.days, a['steps'], req.arrival, a['admitted'],
+                                          clock() - t0, error=f'non-finite thickness after {a["steps"] - a["left"] + 1} steps'))
+                self.batch.status(reset=True, stream=st)
+            elif code != 0:
+                raise _lib.IswError(code, 'serving: the batched step reported a failure; results withheld')
             finished = []
             for a in active:
                 a['left'] -= 1
                 model_days += a['member'].dt / SECONDS_PER_DAY
                 if a['left'] == 0:
                     finished.append(a)
-            if finished:                                    # no result leaves while the batch reports a failed step
-                code = self.batch.status(stream=st)
-                if code != 0:
-                    raise _lib.IswError(code, 'serving: the batched step reported a failure; results withheld')
             for a in finished:
                 m, req = a['member'], a['req']
                 m.unregister()
@@ -227,8 +238,9 @@ class Server:
                                       clock() - t0, state if self.keep_state else []))
                 del m, a
         wall = clock() - t0
-        lat = np.array([r.latency for r in results]) if results else np.zeros(1)
-        stats = dict(requests=len(results), batched_steps=steps, wall_s=wall, model_days=model_days,
+        done = [r for r in results if not r.error]
+        lat = np.array([r.latency for r in done]) if done else np.zeros(1)
+        stats = dict(requests=len(done), failed=len(results) - len(done), batched_steps=steps, wall_s=wall, model_days=model_days,
                      member_days_per_s=model_days / wall if wall > 0 else 0.0,
                      p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)), max_s=float(lat.max()))
         return results, stats

@@ -35,7 +35,7 @@ class Stack:
         self.L = s['L']
         self.kind = s.get('kind')
         self.core = Layers(dg, self.L, b=s['b'], gprime=s['gprime'], stress=s['stress'], nu4=s['nu4'], floor=s['floor'],
-                           vmix=s.get('vmix', 0.0), precision=precision)
+                           vmix=s.get('vmix', 0.0), vmix_cd=s.get('vmix_cd', 0.0), precision=precision)
         tr = s['tracers'] if ntracers is None else s['tracers'][:ntracers]
         self.T = len(tr)
         self.tr = Transport(dg, layers=self.L, tracers=max(1, self.T), precision=precision)
@@ -128,6 +128,10 @@ class Member:
     def state(self):
         return [a for s in self.stacks for a in s.state()]
 
+    def finite(self):
+        """Whether every stack's thicknesses are finite (a device reduction; synchronises)."""
+        return all(bool(torch.isfinite(s.h).all()) for s in self.stacks)
+
     def unregister(self):
         if self.batch is not None:
             for slot in self.slots:
@@ -147,7 +151,8 @@ class Member:
         n = sum(max(1, int(np.ceil(c * self.stacks[0].nfast))) for c in (1 / 3, 1 / 2, 1.0))
         nu4 = any(s.core.nu4 for s in self.stacks)
         tr = any(s.T for s in self.stacks)
-        return 1 + (3 if nu4 else 0) + 3 * 5 + (3 * info['groups'] if info['tiles'] else 2 * n) + 1 + (6 if tr else 0)
+        fast = 3 * info['groups'] if info['tiles'] else (3 if info['persistent'] else 2 * n)
+        return 1 + (3 if nu4 else 0) + 3 * 5 + fast + 1 + (6 if tr else 0)
 
 
 def _fp64_kinds(dg, fp64_kinds):

@@ -4,9 +4,10 @@ NumPy + ctypes over a kernel backend.
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py``,
 never by the product.
 
-Backends (the same kernel argument lists, so one driver runs both):
-- ``'oracle'``: this project's plain-C restatement ``oracle/oracle.c`` (``liboracle.so``),
-- ``'reference'``: the reference's own kernels compiled for the host (``oracle/_ref``, see ``build_ref.py``).
+Backends (the same kernel argument lists, so one driver runs them all):
+- ``'oracle'``: this project's plain-C restatement ``oracle/oracle.c`` (``liboracle.so``, OpenMP),
+- ``'reference'``: the reference's own kernels compiled for the host (``oracle/_ref``, see ``build_ref.py``),
+- ``'numpy'``: the same kernels as whole-array NumPy operations in one process (``oracle/numpy_kernels.py``).
 
 The driver follows the reference call sequence line by line:
 - ``Layers.__init__``  reference ``src/insilica/layers.py:36-92`` (Boussinesq options: gprime, drag, stress, nu4, floor,
@@ -114,7 +115,11 @@ _BACKENDS = {}
 
 def kernels(backend='oracle'):
     if backend not in _BACKENDS:
-        _BACKENDS[backend] = OracleKernels() if backend == 'oracle' else ReferenceKernels()
+        if backend == 'numpy':
+            from oracle.numpy_kernels import NumpyKernels
+            _BACKENDS[backend] = NumpyKernels()
+        else:
+            _BACKENDS[backend] = OracleKernels() if backend == 'oracle' else ReferenceKernels()
     return _BACKENDS[backend]
 
 

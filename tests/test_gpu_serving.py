@@ -92,3 +92,37 @@ def test_checkpoint_resume_equals_uninterrupted(dev, grids, tmp_path):
         assert res[rid].steps == ref[rid].steps
         for x, y in zip(res[rid].state, ref[rid].state):
             assert torch.equal(x, y)
+
+
+def test_nonfinite_request_dropped_others_complete(dev, grids):
+    """A request whose state goes non-finite (a NaN planted in its initial thickness, on the host) is dropped with an
+    error result after its first step; the batch's status is cleared and the other requests complete with the same
+    results as when served without it, bit for bit."""
+    import numpy as np
+    from isw import cases
+    from isw.serving import Request, Server
+
+    def reqs(with_bad):
+        out = [Request(0, 0.0, 4, 0.1, 5, seed=71), Request(2, 0.0, 5, 0.05, 3, seed=73)]
+        if with_bad:
+            g = grids[4].host
+            topo = cases.topography(g, 72)
+            bad = Request(1, 0.0, 4, 0.2, 3, seed=72)
+            bad.state = [cases.stack_state(g, 'air', 72, perturb=0.01, ntracers=2, topo=topo)]
+            bad.state[0]['h'][1, 17] = np.nan
+            out.insert(1, bad)
+        return out
+    res = {}
+    for name in ('clean', 'with_bad'):
+        srv = Server(0, budget_bytes=150e9, precision='mixed', ntracers=2, grids=grids, keep_state=True)
+        srv.batch.config(layout='packed')
+        results, stats = srv.run(reqs(name == 'with_bad'))
+        assert srv.batch.status() == 0
+        res[name] = {r.rid: r for r in results}
+        if name == 'with_bad':
+            assert stats['failed'] == 1 and stats['requests'] == 2
+            assert res[name][1].error.startswith('non-finite thickness after 1 steps')
+    for rid in (0, 2):
+        assert not res['with_bad'][rid].error
+        for x, y in zip(res['clean'][rid].state, res['with_bad'][rid].state):
+            assert torch.equal(x, y)
