@@ -316,7 +316,7 @@ def ensemble_result(steps, warmup, autotune_steps=3):
                 sequential_fp64=dict(value=seq, unit='member-days/s', ms_per_member_step={f'level{k[0]}': v * 1e3 for k, v in base.items()},
                                      note='each member stepped alone on the plain FP64 core, one after another'),
                 speedup_vs_sequential_fp64=value / seq, gpu_launches=launches, clocks=clk.summary(), finite=finite,
-                build_s=t_build, autotune_ms={str(k): v for k, v in times.items()})
+                build_s=t_build, autotune_ms={str(dict(k)): round(v, 4) for k, v in sorted(times.items(), key=lambda x: x[1])[:6]})
 
 
 def cases_dt(level):
@@ -335,7 +335,6 @@ def serving_result(requests, max_days, seed):
     from isw.serving import Server, poisson_requests, sequential_baseline
     reqs = poisson_requests(requests, 50.0, seed=seed, days=(1.0, max_days))
     srv = Server(0, budget_bytes=150e9, precision='mixed', ntracers=2)
-    srv.batch.config(layout='packed')
     for n in sorted({r.level for r in reqs}):          # grids and the requests' initial states exist before the clock starts
         srv._grid(n)
     srv.prepare(reqs)
@@ -528,10 +527,11 @@ def main():
                 set_precision('double')
             ens = Ensemble.build([args.level] * args.batched, seed=rank * 1000, perturb=0.01, ntracers=3, precision=form,
                                  device=local, grids=grids)
-            tuned, _ = ens.batch.autotune(steps=2)
+            tuned, tried = ens.batch.autotune(steps=2)
             t_b = timed(ens)
             batched[form] = dict(value=world * ens.member_days_per_step() / (t_b / 1e3), unit='member-days/s',
                                  ms_per_step=t_b, layout=ens.batch.info(), autotuned=tuned,
+                                 autotune_ms={str(dict(k)): round(v, 4) for k, v in sorted(tried.items(), key=lambda x: x[1])[:6]},
                                  finite=all(bool(torch.isfinite(a).all()) for m_ in ens for a in m_.state()))
             del ens
 
@@ -631,7 +631,8 @@ def main():
         l7['mixed_vs_fp64'] = l7['mixed']['value'] / l7['double']['value']
         out['level7'] = l7
         keep = ('metric', 'value', 'unit', 'ms_per_step', 'steps', 'warmup', 'p50_s', 'p99_s', 'config', 'layout',
-                'sequential_fp64', 'speedup_vs_sequential_fp64', 'device_bytes', 'finite', 'gpu_launches', 'stats')
+                'sequential_fp64', 'speedup_vs_sequential_fp64', 'device_bytes', 'finite', 'gpu_launches', 'stats',
+                'autotune_ms')
         ens = ensemble_result(steps=5, warmup=3, autotune_steps=2)
         out['ensemble'] = {k: v for k, v in ens.items() if k in keep}
         srv = serving_result(requests=24, max_days=3.0, seed=args.seed)

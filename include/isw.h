@@ -195,6 +195,13 @@ int isw_batch_create(int device, isw_batch **out);
 int isw_batch_destroy(isw_batch *b);
 int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *M, double *M1,
                   double *const *tracers, int ntr, double dt, int nfast, int *slot);
+/* The same for air layers (a Layers created with air != 0), which also carry their potential temperature theta (L x N,
+ * FP64, updated in place by the interfacial stress's heat): the batched step runs the air branch (reference
+ * layers.py:134-136, 152-166, 187-206) in the FP64 form, grid-wide (no tiles), with the stress's heat returned to theta
+ * before the transport reads the tracers (theta may be one of them, as in world.py:291-301). Bit-identical to
+ * isw_layers_step_air followed by the transport calls. A batch holding air stacks does not pipeline. */
+int isw_batch_add_air(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *theta,
+                      double *M, double *M1, double *const *tracers, int ntr, double dt, int nfast, int *slot);
 int isw_batch_remove(isw_batch *b, int slot);
 int isw_batch_step(isw_batch *b, void *stream);
 /* Tuning (the autotuner's knobs; results are the same under every setting). The barotropic fast loop runs in

@@ -30,6 +30,7 @@
 #include "batch.cuh"
 #include "common.cuh"
 #include "handles.cuh"
+#include "layers_air.cuh"
 #include "layers_fp64.cuh"
 #include "tiles.cuh"
 #include "transport_fp64.cuh"
@@ -54,14 +55,23 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   pdl_wait();
   pdl_trigger();
   const int i = ch.begin + (int)threadIdx.x;
+  if (PH == PH_S && d.s_stage) {             // the block stages its rows' distinct neighbour records, then computes
+    extern __shared__ __align__(16) double stg[];
+    const StageArgs a = stage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, fp64::stage_pk<LL>(d.M, ch.begin / THREADS, stg));
+    __syncthreads();
+    if (i < ch.end) ISW_BATCH_L(d.L, LMAXK, (fp64::slow_edge<LL, false, true>(d.M, a.us, a.cdt, i, nullptr, stg)));
+    return;
+  }
   if (i >= ch.end) return;
   const LayersDev &M = d.M;
   if (PH == PH_INIT) {
     if (kind == 0) {
-      ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
+      if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_stiff_cell<LL>(M, d.h, d.theta, i));
+      else ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
       if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, fp64::div_cell<LL>(M, d.u, i));
     } else if (kind == 1) {
-      ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
+      if (!M.air) ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
     } else if (M.nu4 != 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::curl_vertex<LL>(M, d.u, i));
     }
@@ -74,37 +84,57 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     }
   } else if (PH == PH_A) {
     const StageArgs a = stage_args(d, st);
-    if (kind == 0) ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL, false>(M, a.hs, a.us, i));
-    else ISW_BATCH_L(d.L, LMAXK, fp64::pv_vertex<LL>(M, a.hs, a.us, i));
+    if (kind == 0) {
+      if (M.air) {
+        ISW_BATCH_L(d.L, LMAXK, fp64::air_bern_cell<LL>(M, a.hs, a.us, d.theta, i));
+        ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_cell<LL>(M, a.h0, i));
+      } else {
+        ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL, false>(M, a.hs, a.us, i));
+      }
+    } else {
+      ISW_BATCH_L(d.L, LMAXK, fp64::pv_vertex<LL>(M, a.hs, a.us, i));
+    }
   } else if (PH == PH_E) {
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL, false>(M, a.hs, a.us, i));
+    if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_edge<LL>(M, a.u0, i));
   } else if (PH == PH_S) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i, M.air ? d.theta : nullptr));
   } else if (PH == PH_ETA) {
-    if (!d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(M, d.tau[st], j, i);
+    if (!d.tiled && j < d.n[st]) {
+      if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
+      else fp64::bt_eta_cell_y(M, d.tau[st], j, i);
+    }
   } else if (PH == PH_U || PH == PH_UF) {
     if (!d.tiled && j < d.n[st]) {
-      fp64::bt_u_edge_y(M, d.tau[st], i);
-      if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<false>(M, stage_args(d, st), M.acc[i], i);
+      if (M.air) {
+        ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(M, d.tau[st], i));
+      } else {
+        fp64::bt_u_edge_y(M, d.tau[st], i);
+        if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<false>(M, stage_args(d, st), M.acc[i], i);
+      }
     }
-  } else if (PH == PH_C) {
+  } else if (PH == PH_C || PH == PH_CS) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::scale_cell<LL, false>(M, a, i));
-  } else if (PH == PH_CS) {
-    const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
+    if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
+    else if (PH == PH_C) ISW_BATCH_L(d.L, LMAXK, (fp64::scale_cell<LL, false>(M, a, i)));
+    else ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
       if (st == 2) check_finite_column(d.h, M.g.N, d.L, i, sc.status);
+    } else if (M.air) {
+      ISW_BATCH_L(d.L, LMAXK, fp64::air_u_edge<LL>(M, a, i));
     } else {
       ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
     }
   } else if (PH == PH_VMIX) {
     if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
+  } else if (PH == PH_VHEAT) {
+    if (M.air && d.theta && (M.vmix != 0 || M.vmix_cd != 0) && d.L > 1)
+      ISW_BATCH_L(d.L, LMAXK, fp64::vmix_heat_cell<LL>(M, d.h, d.theta, i));
   } else if (PH == PH_HF1) {
     ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
   } else if (PH == PH_POST) {
@@ -250,6 +280,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
 // walk the edge chunks (the ubar pass; with flux != 0 a stack's last sub-step also forms its layer fluxes, as PH_UF
 // does) and meet again. The per-item arithmetic is PH_ETA's and PH_U's / PH_UF's, which otherwise take two launches
 // per sub-step; the barrier's acquire makes every block's writes of one pass visible to the next pass.
+template <int LMAXK>
 __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restrict__ S, const Sched sc, int st, int nsub,
                                                         int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
   __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
@@ -269,7 +300,10 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       const Chunk ch = sc.cell[c];
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
-      if (i < ch.end && !d.tiled && j < d.n[st]) fp64::bt_eta_cell_y(d.M, d.tau[st], j, i);
+      if (i < ch.end && !d.tiled && j < d.n[st]) {
+        if (d.M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(d.M, d.tau[st], i));
+        else fp64::bt_eta_cell_y(d.M, d.tau[st], j, i);
+      }
     }
     if (!grid_sync(bar, status, timeout_ns, 0)) return;
     for (int c = blockIdx.x; c < sc.nedge; c += gridDim.x) {
@@ -277,11 +311,24 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        fp64::bt_u_edge_y(d.M, d.tau[st], i);
-        if (flux && j == d.n[st] - 1) fp64::flux_edge<false>(d.M, stage_args(d, st), d.M.acc[i], i);
+        if (d.M.air) {
+          ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(d.M, d.tau[st], i));
+        } else {
+          fp64::bt_u_edge_y(d.M, d.tau[st], i);
+          if (flux && j == d.n[st] - 1) fp64::flux_edge<false>(d.M, stage_args(d, st), d.M.acc[i], i);
+        }
       }
     }
     if (!grid_sync(bar, status, timeout_ns, 0)) return;
+  }
+}
+
+const void *fast_grid_kernel(int lmax) {
+  switch (lmax) {
+    case 2: return (const void *)k_fast_grid<2>;
+    case 3: return (const void *)k_fast_grid<3>;
+    case 5: return (const void *)k_fast_grid<5>;
+    default: return (const void *)k_fast_grid<8>;
   }
 }
 
@@ -295,6 +342,7 @@ struct BatchSlot {
   isw_layers *layers = nullptr;
   isw_transport *tr = nullptr;
   double *h = nullptr, *u = nullptr, *Fm = nullptr, *M = nullptr, *M1 = nullptr;
+  double *theta = nullptr;                  // air layers: the layers' potential temperature (L x N), else null
   double *tracers[TRMAX] = {};
   int ntr = 0;
   double dt = 0;
@@ -323,7 +371,7 @@ struct isw_batch {
   Sched scf[2] = {};                          // chunk tables of the FP64 stacks [0] and the mixed ones [1]
   int lmax = 1, nstacks = 0, ntiles = 0, nsub[3] = {0, 0, 0}, kused = 0;
   std::vector<FastGroup> groups;              // cooperative launches of the fast loop (tiles [begin, begin + count))
-  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0;
+  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, any_air = 0;
   size_t fast_smem = 0;
   int fast_bps = 2;                           // tile blocks per SM: 2 (512 threads each) or 1 (1024 threads)
   GridBarrier *bar = nullptr;
@@ -338,6 +386,7 @@ struct isw_batch {
   bool pdl = true;                            // programmatic dependent launch between phase kernels
   bool fast_grid = false;                     // untiled stacks' sub-steps: one cooperative launch per stage (k_fast_grid)
   int untiled_form[2] = {0, 0};               // per form (FP64, mixed): any untiled stack
+  size_t s_smem[2] = {0, 0};                  // per form: dynamic shared memory of the slow-tendency launch (staging)
   int grid_blocks[2] = {0, 0};                // per form: co-resident blocks of the cooperative grid-wide fast loop
   // pipelined steps: step n's dynamics beside step n-1's transport (two branches of one graph), Fm double-buffered.
   // desc[q] describes a step whose dynamics write Fm_q and whose transport reads it: Fm_0 the registered Fm, Fm_1 fm_alt
@@ -484,7 +533,7 @@ int form_of(const BatchSlot &sl) { return sl.layers->d.precision == ISW_MIXED ? 
 
 // A batch holding stacks of both forms tiles the fast loop of its mixed stacks only (one tile kernel per batch); its
 // FP64 stacks take the grid-wide sub-step kernels.
-bool tiles_form(const isw_batch *b, const BatchSlot &sl) { return sl.used && form_of(sl) == b->mixed; }
+bool tiles_form(const isw_batch *b, const BatchSlot &sl) { return sl.used && !sl.layers->d.air && form_of(sl) == b->mixed; }
 
 Tiling plan_shared(isw_batch *b, int bps) {
   Tiling t;
@@ -560,8 +609,9 @@ void rebuild(isw_batch *b) {
   b->mixed = 0;
   for (auto &sl : b->slots)
     if (sl.used && form_of(sl) == 1) b->mixed = 1;
-  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, lmax = 1;
+  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, any_air = 0, lmax = 1;
   int untiled[2] = {0, 0};
+  size_t s_smem[2] = {0, 0};
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
   int used = 0;
   for (auto &sl : b->slots) used += sl.used ? 1 : 0;
@@ -590,6 +640,8 @@ void rebuild(isw_batch *b) {
     std::memset(&d, 0, sizeof(d));
     d.M = sl.layers->d;
     d.h = sl.h; d.u = sl.u; d.Fm = sl.Fm; d.Mm = sl.M;
+    d.theta = sl.theta;
+    if (d.M.air) any_air = 1;
     d.dt = sl.dt;
     d.L = d.M.L;
     lmax = std::max(lmax, d.L);
@@ -624,6 +676,13 @@ void rebuild(isw_batch *b) {
       for (int st = 0; st < 3; st++) gsub[g][st] = std::max(gsub[g][st], (d.n[st] + best.K[q] - 1) / best.K[q]);
     }
     if (!d.tiled) any_untiled = 1;
+    {                                            // the mixed form's slow tendency stages its neighbour records when they fit
+      // (measured: S 80.0 -> 76.2 us a level-6 member step in the mixed form; 97.4 -> 113.1 in FP64, whose 80-byte
+      // records are staged about twice per block against the L1 hits of direct gathers, so FP64 gathers directly)
+      const size_t need = (size_t)d.M.g.sMax * (size_t)d.L * sizeof(float4);
+      d.s_stage = form_of(sl) == 1 && need <= S_STAGE_MAX ? 1 : 0;
+      if (d.s_stage) s_smem[form_of(sl)] = std::max(s_smem[form_of(sl)], need);
+    }
     auto chunks = [&](std::vector<Chunk> &v, int n) {
       for (int i = 0; i < n; i += THREADS) v.push_back(Chunk{s, i, std::min(n, i + THREADS)});
     };
@@ -750,13 +809,21 @@ void rebuild(isw_batch *b) {
   b->any_vmix = any_vmix;
   b->any_tr = any_tr;
   b->any_untiled = any_untiled;
+  b->any_air = any_air;
   b->lmax = kernel_lmax(lmax);
+  b->s_smem[0] = s_smem[0];
+  b->s_smem[1] = s_smem[1];
+  if (s_smem[0] > 48 * 1024)
+    for (const void *fn : {(const void *)k_phase<PH_S, 2>, (const void *)k_phase<PH_S, 3>, (const void *)k_phase<PH_S, 5>,
+                           (const void *)k_phase<PH_S, 8>})
+      ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_smem[0]));
+  if (s_smem[1] > 48 * 1024) slow_phase_smem_mixed(s_smem[1]);
   for (int f = 0; f < 2; f++) {
     b->untiled_form[f] = untiled[f];
     b->grid_blocks[f] = 0;
     if (!untiled[f]) continue;
     int per = 0;
-    const void *fn = f == 0 ? (const void *)k_fast_grid : fast_grid_kernel_mixed();
+    const void *fn = f == 0 ? fast_grid_kernel(b->lmax) : fast_grid_kernel_mixed();
     ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, THREADS, 0));
     b->grid_blocks[f] = std::max(1, per) * b->sms;
   }
@@ -777,14 +844,15 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = tr
     const bool p = (first ? pdl : true) && b->pdl;
     first = false;
     if (f == 1) {
-      launch_phase_mixed(PH, b->lmax, nb, st, p, b->cur, sc, stage, j);
+      launch_phase_mixed(PH, b->lmax, nb, st, p, PH == PH_S ? b->s_smem[1] : 0, b->cur, sc, stage, j);
       continue;
     }
+    const size_t smem = PH == PH_S ? b->s_smem[0] : 0;
     switch (b->lmax) {
-      case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, p, b->cur, sc, stage, j); break;
-      case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, p, b->cur, sc, stage, j); break;
-      case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, p, b->cur, sc, stage, j); break;
-      default: launch_phase_kernel(k_phase<PH, 8>, nb, st, p, b->cur, sc, stage, j); break;
+      case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, p, smem, b->cur, sc, stage, j); break;
+      case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, p, smem, b->cur, sc, stage, j); break;
+      case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, p, smem, b->cur, sc, stage, j); break;
+      default: launch_phase_kernel(k_phase<PH, 8>, nb, st, p, smem, b->cur, sc, stage, j); break;
     }
   }
 }
@@ -834,10 +902,15 @@ void launch_fast_grid(isw_batch *b, cudaStream_t st, int stage, bool flux) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (f == 0)
-      ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status,
-                                  DEFAULT_TIMEOUT_NS));
-    else
+    if (f == 0) {
+      const int fl = flux ? 1 : 0, ns = b->nsub[stage];
+      switch (b->lmax) {
+        case 2: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<2>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
+        case 3: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<3>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
+        case 5: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<5>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
+        default: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<8>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
+      }
+    } else
       launch_fast_grid_mixed(cfg, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status, DEFAULT_TIMEOUT_NS);
   }
 }
@@ -889,14 +962,29 @@ void enqueue_tr_tail(isw_batch *b, cudaStream_t st) {
 void enqueue(isw_batch *b, cudaStream_t st) {
   b->cur = b->d_desc;
   enqueue_dyn(b, st);
-  if (b->any_vmix || b->any_tr) launch_phase<PH_POST>(b, st, 0, 0);
-  if (b->any_tr) enqueue_tr_tail(b, st);
+  if (b->any_air) {
+    // air stacks: the interfacial stress's heat goes back to theta before the transport reads the tracers (theta is
+    // one of them in the reference's world tick, world.py:291-301), so the stress, its heat and the stage-1 edge fluxes
+    // are three passes here
+    if (b->any_vmix) {
+      launch_phase<PH_VMIX>(b, st, 0, 0);
+      launch_phase<PH_VHEAT>(b, st, 0, 0);
+    }
+    if (b->any_tr) {
+      launch_phase<PH_HF1>(b, st, 0, 0);
+      enqueue_tr_tail(b, st);
+    }
+  } else {
+    if (b->any_vmix || b->any_tr) launch_phase<PH_POST>(b, st, 0, 0);
+    if (b->any_tr) enqueue_tr_tail(b, st);
+  }
   ISW_CUDA(cudaGetLastError());
 }
 
 // Pipelined: the dynamics of the step described by `dyn` (with its interfacial stress) on `st`, and beside it on the
 // side stream the transport of the step described by `tr` (the previous one); either may be null.
 void enqueue_pipelined(isw_batch *b, cudaStream_t st, const StackDesc *dyn, const StackDesc *tr) {
+  if (b->any_air) fail(ISW_EUNSUPPORTED, "batch: air stacks step in the plain order (the stress's heat precedes the transport)");
   const bool trans = tr && b->any_tr;
   if (trans && dyn) {
     ISW_CUDA(cudaEventRecord(b->ev_fork, st));
@@ -1049,12 +1137,15 @@ int isw_batch_destroy(isw_batch *b) {
   return ISW_OK;
 }
 
-int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *M, double *M1,
-                  double *const *tracers, int ntr, double dt, int nfast, int *slot) {
+namespace {
+
+int batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *theta, double *M,
+              double *M1, double *const *tracers, int ntr, double dt, int nfast, int *slot) {
   return guarded([&] {
     if (!b || !layers || !h || !u || !Fm || !slot) fail(ISW_EINVAL, "batch.add: null argument");
     if (layers->grid->device != b->device) fail(ISW_EINVAL, "batch.add: the stack is on another device");
-    if (layers->d.air) fail(ISW_EUNSUPPORTED, "batch.add: air layers step call by call (isw_layers_step_air)");
+    if (layers->d.air && !theta) fail(ISW_EINVAL, "batch.add: air layers need their theta (isw_batch_add_air)");
+    if (!layers->d.air && theta) fail(ISW_EINVAL, "batch.add: theta is for air layers");
     if (layers->d.wall || layers->d.ob || layers->d.shelf > 0 || layers->d.sig || layers->d.tide || layers->d.cbot ||
         layers->d.cd_bot > 0)
       fail(ISW_EUNSUPPORTED, "batch.add: the option branches (walls, shelf, sig, tide, bottom drag) step call by call");
@@ -1072,6 +1163,8 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     sl.layers = layers;
     sl.tr = tr;
     sl.h = h; sl.u = u; sl.Fm = Fm; sl.M = M; sl.M1 = M1;
+    sl.theta = theta;
+    if (layers->d.air && layers->d.nu4 != 0) layers->nu4dt = layers->d.nu4 * dt;   // the step's nabla^4 loss (exchange heat)
     sl.ntr = tr ? ntr : 0;
     for (int j = 0; j < sl.ntr; j++) {
       if (!tracers[j]) fail(ISW_EINVAL, "batch.add: null tracer");
@@ -1086,6 +1179,18 @@ int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h
     b->dirty = true;
     *slot = (int)k;
   });
+}
+
+}  // namespace
+
+int isw_batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *M, double *M1,
+                  double *const *tracers, int ntr, double dt, int nfast, int *slot) {
+  return batch_add(b, layers, tr, h, u, Fm, nullptr, M, M1, tracers, ntr, dt, nfast, slot);
+}
+
+int isw_batch_add_air(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, double *u, double *Fm, double *theta,
+                      double *M, double *M1, double *const *tracers, int ntr, double dt, int nfast, int *slot) {
+  return batch_add(b, layers, tr, h, u, Fm, theta, M, M1, tracers, ntr, dt, nfast, slot);
 }
 
 int isw_batch_remove(isw_batch *b, int slot) {

@@ -28,8 +28,10 @@ struct StackDesc {
   TransportDev T;
   TrArgs tr;                 // M0 = the stack's M, M1, Fm, tracers, L, rows, beta
   double *h, *u, *Fm, *Mm;
+  double *theta;             // air layers: potential temperature (L x N); null for Boussinesq layers
   double dt;
   int L, has_tr, tiled;
+  int s_stage;               // the slow tendency stages its blocks' neighbour records in shared memory
   int n[3];
   double cdt[3], tau[3], inv_n[3];
   TileSetDev tiles;
@@ -163,11 +165,12 @@ __device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s
 
 // The FCT step's passes: POST (edges: interfacial stress; (tracer, edge): stage-1 fluxes), P1 (cells: M1, td, p1),
 // P2E (stage-2 fluxes), P2 (cells: p2), P3E (antidiffusive fluxes), P3 (cells: ratios), P4 (cells: limited update).
-// A pipelined batch splits POST into VMIX (edges, the dynamics' last pass) and HF1 ((tracer, edge), the transport's first).
+// A pipelined batch splits POST into VMIX (edges, the dynamics' last pass) and HF1 ((tracer, edge), the transport's first);
+// a batch with air stacks runs VMIX, VHEAT (cells: the stress's heat back to theta) and HF1 in place of POST.
 // PH_UF / PH_CS: the grid-wide edge sub-step that also forms the layer fluxes on a stack's last sub-step, and phase C
 // summing them; used by batches with no tiled stack in place of PH_U / PH_C.
 enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4,
-             PH_P1, PH_P2E, PH_P3E, PH_VMIX, PH_HF1, PH_UF, PH_CS };
+             PH_P1, PH_P2E, PH_P3E, PH_VMIX, PH_HF1, PH_UF, PH_CS, PH_VHEAT };
 
 // Programmatic dependent launch between phase kernels: a phase kernel is launched while the previous one drains; it
 // stages only constant data (its stack descriptor) before waiting for the previous grid's completion and memory
@@ -176,10 +179,11 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <class... KA, class... A>
-void launch_phase_kernel(void (*kern)(KA...), int nb, cudaStream_t st, bool pdl, A... args) {
+void launch_phase_kernel(void (*kern)(KA...), int nb, cudaStream_t st, bool pdl, size_t smem, A... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)nb);
   cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -193,7 +197,7 @@ void launch_phase_kernel(void (*kern)(KA...), int nb, cudaStream_t st, bool pdl,
 template <int PH>
 struct Dom {
   static constexpr bool cell = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A || PH == PH_ETA || PH == PH_C || PH == PH_D ||
-                               PH == PH_CS;
+                               PH == PH_CS || PH == PH_VHEAT;
   static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
                                PH == PH_D || PH == PH_POST || PH == PH_VMIX || PH == PH_UF;
   static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
@@ -202,8 +206,11 @@ struct Dom {
 };
 
 
-void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage,
-                        int j);
+constexpr size_t S_STAGE_MAX = 64 * 1024;   // the slow tendency's staged neighbour records: at most this per block
+
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, size_t smem, const StackDesc *desc,
+                        const Sched &sc, int stage, int j);
+void slow_phase_smem_mixed(size_t bytes);
 const void *fast_kernel_mixed(int bps);
 const void *fast_grid_kernel_mixed();
 void launch_fast_grid_mixed(const cudaLaunchConfig_t &cfg, const StackDesc *desc, const Sched &sc, int stage, int nsub,

@@ -44,6 +44,14 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
   pdl_wait();
   pdl_trigger();
   const int i = ch.begin + (int)threadIdx.x;
+  if (PH == PH_S && d.s_stage) {             // the block stages its rows' distinct neighbour records, then computes
+    extern __shared__ __align__(16) float4 stg4[];
+    const mixed::MStageArgs a = mstage_args(d, st);
+    ISW_BATCH_L(d.L, LMAXK, mixed::stage_pk4<LL>(d.M, ch.begin / THREADS, stg4));
+    __syncthreads();
+    if (i < ch.end) ISW_BATCH_L(d.L, LMAXK, (mixed::slow_edge<LL, true>(d.M, a.us, a.cdt, i, stg4)));
+    return;
+  }
   if (i >= ch.end) return;
   const LayersDev &M = d.M;
   if (PH == PH_INIT) {
@@ -278,42 +286,49 @@ __global__ void __launch_bounds__(NT, MINB) k_fast_m(const StackDesc *__restrict
 }
 
 template <int PH>
-void launch_m(int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage, int j) {
+void launch_m(int lmax, int nb, cudaStream_t st, bool pdl, size_t smem, const StackDesc *desc, const Sched &sc, int stage,
+              int j) {
   switch (lmax) {
-    case 2: launch_phase_kernel(k_phase_m<PH, 2>, nb, st, pdl, desc, sc, stage, j); break;
-    case 3: launch_phase_kernel(k_phase_m<PH, 3>, nb, st, pdl, desc, sc, stage, j); break;
-    case 5: launch_phase_kernel(k_phase_m<PH, 5>, nb, st, pdl, desc, sc, stage, j); break;
-    default: launch_phase_kernel(k_phase_m<PH, 8>, nb, st, pdl, desc, sc, stage, j); break;
+    case 2: launch_phase_kernel(k_phase_m<PH, 2>, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case 3: launch_phase_kernel(k_phase_m<PH, 3>, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case 5: launch_phase_kernel(k_phase_m<PH, 5>, nb, st, pdl, smem, desc, sc, stage, j); break;
+    default: launch_phase_kernel(k_phase_m<PH, 8>, nb, st, pdl, smem, desc, sc, stage, j); break;
   }
 }
 
 }  // namespace
 
-void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, const StackDesc *desc, const Sched &sc, int stage,
-                        int j) {
+void slow_phase_smem_mixed(size_t bytes) {
+  for (const void *fn : {(const void *)k_phase_m<PH_S, 2>, (const void *)k_phase_m<PH_S, 3>, (const void *)k_phase_m<PH_S, 5>,
+                         (const void *)k_phase_m<PH_S, 8>})
+    ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+void launch_phase_mixed(int ph, int lmax, int nb, cudaStream_t st, bool pdl, size_t smem, const StackDesc *desc,
+                        const Sched &sc, int stage, int j) {
   switch (ph) {
-    case PH_INIT: launch_m<PH_INIT>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_LAPE1: launch_m<PH_LAPE1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_LAPCV: launch_m<PH_LAPCV>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_LAPE2: launch_m<PH_LAPE2>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_A: launch_m<PH_A>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_E: launch_m<PH_E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_S: launch_m<PH_S>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_U: launch_m<PH_U>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_C: launch_m<PH_C>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_UF: launch_m<PH_UF>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_CS: launch_m<PH_CS>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_D: launch_m<PH_D>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_POST: launch_m<PH_POST>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P2: launch_m<PH_P2>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P3: launch_m<PH_P3>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P4: launch_m<PH_P4>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P1: launch_m<PH_P1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_VMIX: launch_m<PH_VMIX>(lmax, nb, st, pdl, desc, sc, stage, j); break;
-    case PH_HF1: launch_m<PH_HF1>(lmax, nb, st, pdl, desc, sc, stage, j); break;
+    case PH_INIT: launch_m<PH_INIT>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_LAPE1: launch_m<PH_LAPE1>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_LAPCV: launch_m<PH_LAPCV>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_LAPE2: launch_m<PH_LAPE2>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_A: launch_m<PH_A>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_E: launch_m<PH_E>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_S: launch_m<PH_S>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_ETA: launch_m<PH_ETA>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_U: launch_m<PH_U>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_C: launch_m<PH_C>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_UF: launch_m<PH_UF>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_CS: launch_m<PH_CS>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_D: launch_m<PH_D>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_POST: launch_m<PH_POST>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P2: launch_m<PH_P2>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P3: launch_m<PH_P3>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P4: launch_m<PH_P4>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P1: launch_m<PH_P1>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P2E: launch_m<PH_P2E>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_P3E: launch_m<PH_P3E>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_VMIX: launch_m<PH_VMIX>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
+    case PH_HF1: launch_m<PH_HF1>(lmax, nb, st, pdl, smem, desc, sc, stage, j); break;
     default: break;
   }
 }

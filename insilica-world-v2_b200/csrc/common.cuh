@@ -41,6 +41,11 @@ struct GridDev {
   const int *eoeP;                // the TRiSK rows (eoe, w) padded to EOE_MAX entries per edge, pads id 0 weight 0
   const double *wP;
   const float *wP32;
+  // neighbour staging of the slow tendency: block c of THREADS edges names the distinct edges sList[sOff[c] ..
+  // sOff[c + 1]) in its rows; sLoc (E x EOE_MAX) gives each row entry's position in that list; sMax the longest list
+  const int *sOff, *sList;
+  const int16_t *sLoc;
+  int sMax;
 };
 
 // A cell's six slots of a per-cell table (int32: 24-byte rows; int8: 6-byte rows). Each table is its own allocation,
@@ -88,6 +93,35 @@ __device__ __forceinline__ void trisk_row(const GridDev &g, int e, int ix[EOE_MA
     const int2 a = pi[q];
     const float2 b = pw[q];
     ix[2 * q] = a.x; ix[2 * q + 1] = a.y;
+    wv[2 * q] = b.x; wv[2 * q + 1] = b.y;
+  }
+}
+
+// Edge e's row entries as positions in its block's staged neighbour list (five 4-byte loads).
+__device__ __forceinline__ void trisk_loc(const GridDev &g, int e, int loc[EOE_MAX]) {
+  const short2 *p = reinterpret_cast<const short2 *>(g.sLoc + (size_t)e * EOE_MAX);
+#pragma unroll
+  for (int q = 0; q < EOE_MAX / 2; q++) {
+    const short2 v = p[q];
+    loc[2 * q] = v.x;
+    loc[2 * q + 1] = v.y;
+  }
+}
+
+__device__ __forceinline__ void trisk_weights(const GridDev &g, int e, double wv[EOE_MAX]) {
+  const double2 *pw = reinterpret_cast<const double2 *>(g.wP + (size_t)e * EOE_MAX);
+#pragma unroll
+  for (int q = 0; q < EOE_MAX / 2; q++) {
+    const double2 b = pw[q];
+    wv[2 * q] = b.x; wv[2 * q + 1] = b.y;
+  }
+}
+
+__device__ __forceinline__ void trisk_weights(const GridDev &g, int e, float wv[EOE_MAX]) {
+  const float2 *pw = reinterpret_cast<const float2 *>(g.wP32 + (size_t)e * EOE_MAX);
+#pragma unroll
+  for (int q = 0; q < EOE_MAX / 2; q++) {
+    const float2 b = pw[q];
     wv[2 * q] = b.x; wv[2 * q + 1] = b.y;
   }
 }

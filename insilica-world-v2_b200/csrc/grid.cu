@@ -2,6 +2,7 @@
 //
 // Every index table is validated on the host before it reaches the device: each entry is in range (or a -1 pad where
 // the reference pads), so the kernels may gather through them without bounds checks.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <sstream>
@@ -203,6 +204,32 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     d.eoeP = upload(g, eoeP.data(), eoeP.size());
     d.wP = upload(g, wP.data(), wP.size());
     d.wP32 = upload_f32(g, wP.data(), wP.size());
+    // the slow tendency's neighbour staging: for each block of THREADS consecutive edges, the distinct edges its TRiSK
+    // rows name (ascending), and per edge the position of each row entry in its block's list (pads 0, never read)
+    {
+      const int nch = (E + THREADS - 1) / THREADS;
+      std::vector<int32_t> off(nch + 1, 0), list;
+      std::vector<int16_t> loc((size_t)E * EOE_MAX, 0);
+      std::vector<int32_t> ids;
+      int smax = 0;
+      for (int c = 0; c < nch; c++) {
+        const int e0 = c * THREADS, e1 = std::min(E, e0 + THREADS);
+        ids.assign(eoeP.begin() + (size_t)e0 * EOE_MAX, eoeP.begin() + (size_t)e1 * EOE_MAX);
+        std::sort(ids.begin(), ids.end());
+        ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+        for (int e = e0; e < e1; e++)
+          for (int t = 0; t < h->eoeStart[e + 1] - h->eoeStart[e]; t++)
+            loc[(size_t)e * EOE_MAX + t] = (int16_t)(std::lower_bound(ids.begin(), ids.end(), eoeP[(size_t)e * EOE_MAX + t]) - ids.begin());
+        list.insert(list.end(), ids.begin(), ids.end());
+        off[c + 1] = (int32_t)list.size();
+        smax = std::max(smax, (int)ids.size());
+      }
+      if (smax > 32767) fail(ISW_EINVAL, "grid.create: a block's TRiSK neighbours exceed the staging table's range");
+      d.sOff = upload(g, off.data(), off.size());
+      d.sList = upload(g, list.data(), list.size());
+      d.sLoc = upload(g, loc.data(), loc.size());
+      d.sMax = smax;
+    }
     g->h_nbr.assign(h->nbr, h->nbr + (size_t)N * 6);
     g->h_cellEdge.assign(h->cellEdge, h->cellEdge + (size_t)N * 6);
     g->h_cellSign.assign(h->cellSign, h->cellSign + (size_t)N * 6);

@@ -242,9 +242,24 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 }
 
 // ---- stage phase S: slow tendencies ----
-template <int L, bool OPT = true>
+
+// Copy into shared memory the packed records of the distinct edges named by the rows of edge block c (sList), as
+// 16-byte pairs: every thread of the block takes part; the caller synchronises before reading.
+template <int L>
+__device__ __forceinline__ void stage_pk(const LayersDev &M, int c, double *stg) {
+  constexpr int PS = pk_stride(L), P2 = PS / 2;
+  const int b0 = M.g.sOff[c], n2 = (M.g.sOff[c + 1] - b0) * P2;
+  double2 *dst = reinterpret_cast<double2 *>(stg);
+  for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+    const int r = q / P2;
+    dst[q] = reinterpret_cast<const double2 *>(M.pk + (size_t)M.g.sList[b0 + r] * PS)[q - r * P2];
+  }
+}
+// STG: the neighbours' packed records come from `stg`, this block's staged copy of the distinct records its edges'
+// rows name (stage_pk), instead of from M.pk; the same values in the same order.
+template <int L, bool OPT = true, bool STG = false>
 __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__restrict__ u, double dts, int e,
-                                          const double *__restrict__ theta = nullptr) {
+                                          const double *__restrict__ theta = nullptr, const double *stg = nullptr) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
   double he[L], cap[L], qf[L], Q[L];
@@ -262,12 +277,17 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
   const int cnt = g.eoeStart[e + 1] - g.eoeStart[e];
   int ix[EOE_MAX];
   double wv[EOE_MAX];
-  trisk_row(g, e, ix, wv);
+  if (STG) {
+    trisk_loc(g, e, ix);
+    trisk_weights(g, e, wv);
+  } else {
+    trisk_row(g, e, ix, wv);
+  }
 #pragma unroll
   for (int t = 0; t < EOE_MAX; t++) {
     if (t < cnt) {
       const double wm = wv[t];
-      const double2 *pp = reinterpret_cast<const double2 *>(M.pk + (size_t)ix[t] * PS);
+      const double2 *pp = reinterpret_cast<const double2 *>((STG ? stg : M.pk) + (size_t)ix[t] * PS);
       double r[PS];
 #pragma unroll
       for (int q = 0; q < PS / 2; q++) {
@@ -305,7 +325,7 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const double *__re
       // tide's drag (reference layers.cu:303-311)
       if (M.cd_bot > 0) {
         double vt = 0;
-        for (int t = 0; t < cnt; t++) vt += wv[t] * M.pk[(size_t)ix[t] * PS + k * 3 + 1];
+        for (int t = 0; t < cnt; t++) vt += wv[t] * (STG ? stg : M.pk)[(size_t)ix[t] * PS + k * 3 + 1];
         ck += M.cd_bot * sqrt(ue * ue + vt * vt);
       }
       if (M.cbot) ck += M.cbot[e];

@@ -189,8 +189,21 @@ __device__ __forceinline__ void edge_hq(const LayersDev &M, const double *__rest
 }
 
 // ---- stage phase S: slow tendencies in FP32; the pressure gradient from the FP64 B ----
+// Copy into shared memory the packed records (every layer's float4) of the distinct edges named by the rows of edge
+// block c; every thread of the block takes part, the caller synchronises before reading.
 template <int L>
-__device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__restrict__ u, double dts, int e) {
+__device__ __forceinline__ void stage_pk4(const LayersDev &M, int c, float4 *stg) {
+  const int b0 = M.g.sOff[c], n = (M.g.sOff[c + 1] - b0) * L;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int r = q / L;
+    stg[q] = M.pk4[(size_t)M.g.sList[b0 + r] * L + (q - r * L)];
+  }
+}
+
+// STG: the neighbours' records come from `stg` (stage_pk4) instead of M.pk4; the same values in the same order.
+template <int L, bool STG = false>
+__device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__restrict__ u, double dts, int e,
+                                          const float4 *stg = nullptr) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
   float he[L], cap[L], qf[L], Q[L];
@@ -207,12 +220,17 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
   const int cnt = g.eoeStart[e + 1] - g.eoeStart[e];
   int ix[EOE_MAX];
   float wv[EOE_MAX];
-  trisk_row(g, e, ix, wv);
+  if (STG) {
+    trisk_loc(g, e, ix);
+    trisk_weights(g, e, wv);
+  } else {
+    trisk_row(g, e, ix, wv);
+  }
 #pragma unroll
   for (int t = 0; t < EOE_MAX; t++) {
     if (t < cnt) {
       const float wm = wv[t];
-      const float4 *pp = M.pk4 + (size_t)ix[t] * L;
+      const float4 *pp = (STG ? stg : M.pk4) + (size_t)ix[t] * L;
 #pragma unroll
       for (int k = 0; k < L; k++) {
         const float4 p = pp[k];

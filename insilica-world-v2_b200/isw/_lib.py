@@ -71,6 +71,7 @@ isw_mesh_destroy = _sig('isw_mesh_destroy', I, [P])
 isw_batch_create = _sig('isw_batch_create', I, [I, ctypes.POINTER(P)])
 isw_batch_destroy = _sig('isw_batch_destroy', I, [P])
 isw_batch_add = _sig('isw_batch_add', I, [P, P, P, P, P, P, P, P, ctypes.POINTER(P), I, D, I, ctypes.POINTER(I)])
+isw_batch_add_air = _sig('isw_batch_add_air', I, [P, P, P, P, P, P, P, P, P, ctypes.POINTER(P), I, D, I, ctypes.POINTER(I)])
 isw_batch_remove = _sig('isw_batch_remove', I, [P, I])
 isw_batch_step = _sig('isw_batch_step', I, [P, P])
 isw_batch_config = _sig('isw_batch_config', I, [P, I, I, I, I, I])

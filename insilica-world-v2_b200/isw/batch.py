@@ -24,19 +24,27 @@ class Batch:
             destroy(h)
             self._h = None
 
-    def add(self, core, h, u, Fm, tr=None, M=None, M1=None, tracers=(), dt=None, nfast=None):
+    def add(self, core, h, u, Fm, tr=None, M=None, M1=None, tracers=(), dt=None, nfast=None, theta=None):
         """Register a stack: its Layers `core` and state (h, u, Fm), and optionally its Transport `tr` with M, M1 and the
-        tracers. Returns the slot. The arrays are borrowed until remove()."""
+        tracers. Air layers also give their theta (L, N), updated in place as Layers.step(..., theta=) does. Returns the
+        slot. The arrays are borrowed until remove()."""
         L, N, E, dev = core.L, core.dg.N, core.dg.E, self.device
+        if bool(core.air) != (theta is not None):
+            raise ValueError('Batch.add: theta is given exactly for air layers')
         ptrs = (ctypes.c_void_p * max(1, len(tracers)))(*[device_ptr(t, shape=(L, N), name='tracer', device=dev) for t in tracers])
         slot = ctypes.c_int()
-        _lib.check(_lib.isw_batch_add(self._h, core._h, tr._h if tr is not None else None,
-                                      device_ptr(h, shape=(L, N), name='h', device=dev), device_ptr(u, shape=(L, E), name='u', device=dev),
-                                      device_ptr(Fm, shape=(L, E), name='Fm', device=dev),
-                                      device_ptr(M, shape=(L, N), name='M', device=dev) if tr is not None else None,
-                                      device_ptr(M1, shape=(L, N), name='M1', device=dev) if tr is not None else None,
-                                      ptrs, len(tracers), float(dt), int(nfast), ctypes.byref(slot)))
-        self._keep[slot.value] = (core, tr, h, u, Fm, M, M1, tuple(tracers))
+        common = (device_ptr(h, shape=(L, N), name='h', device=dev), device_ptr(u, shape=(L, E), name='u', device=dev),
+                  device_ptr(Fm, shape=(L, E), name='Fm', device=dev))
+        tail = (device_ptr(M, shape=(L, N), name='M', device=dev) if tr is not None else None,
+                device_ptr(M1, shape=(L, N), name='M1', device=dev) if tr is not None else None,
+                ptrs, len(tracers), float(dt), int(nfast), ctypes.byref(slot))
+        trh = tr._h if tr is not None else None
+        if theta is None:
+            _lib.check(_lib.isw_batch_add(self._h, core._h, trh, *common, *tail))
+        else:
+            _lib.check(_lib.isw_batch_add_air(self._h, core._h, trh, *common,
+                                              device_ptr(theta, shape=(L, N), name='theta', device=dev), *tail))
+        self._keep[slot.value] = (core, tr, h, u, Fm, M, M1, tuple(tracers) + ((theta,) if theta is not None else ()))
         return slot.value
 
     def remove(self, slot):

@@ -88,6 +88,9 @@ class Server:
         self.keep_state = keep_state
         self.grids = grids or {}
         self.batch = Batch(self.device)
+        # a serving batch changes at every admission and completion: grid-wide sub-steps in one cooperative launch per
+        # stage need no tiles rebuilt for each new mix (the layout the autotuner picks for mixed-level ensembles)
+        self.batch.config(tiles=False, persistent=True)
 
     def _grid(self, level):
         if level not in self.grids:

@@ -346,3 +346,62 @@ def test_pipelined_equals_plain(dev, grid4, precision):
             assert torch.equal(x, y)
     finally:
         gpu.set_precision('double')
+
+
+def _air_world(dg, z, dev, batched_core=True):
+    """Air layers from the reference's aquaplanet golden case with a tracer and theta moved by the transport (the
+    reference's world tick moves theta with its tracers, world.py:291-301)."""
+    from isw.layers import Layers
+    from isw.transport import Transport
+    L = int(z['h0'].shape[0])
+    core = Layers(dg, L, b=z['b'], gprime=[0.0] * (L - 1), stress=list(z['stress']), nu4=float(z['nu4']),
+                  floor=float(z['floor']), vmix=float(z['vmix']),
+                  air=dict(t_ref=288.0, cp=float(z['cp']), kappa=float(z['kappa']), rd=float(z['rd'])))
+    st = dict(core=core, tr=Transport(dg, layers=L, tracers=2), h=T(z['h0'], dev), u=T(z['u0'], dev),
+              theta=T(z['theta0'], dev))
+    st['M'] = (st['h'] * T(dg.host.areaCell, dev)[None]).contiguous()
+    st['M1'] = torch.zeros_like(st['M'])
+    st['Fm'] = torch.zeros_like(st['u'])
+    st['trc'] = [T(np.stack([np.linspace(0.0, 1.0, dg.N)] * L), dev), st['theta']]
+    core.update_gfast(st['h'], st['theta'])
+    return st
+
+
+@pytest.mark.parametrize('persistent', [False, True])
+def test_air_stack_in_batch_equals_per_call(dev, grid4, persistent):
+    """Air layers registered in a batch (isw_batch_add_air) beside a Boussinesq stack: 12 batched steps equal 12 ticks
+    of Layers.step(theta=) + mass_after + step_many([psi, theta]) + M <- M1 call by call, bit for bit (h, u, M, Fm,
+    the tracer and theta), with the grid-wide sub-steps as two launches each or as one persistent launch per stage;
+    the Boussinesq stack equals its own call-by-call run."""
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    dg = DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    za, zb = golden('airtheta_n4'), golden('air3_n4')
+    dt, nfast = float(za['dt']), int(za['nfast'])
+    ref = _air_world(dg, za, dev)
+    for _ in range(12):
+        ref['core'].step(ref['h'], ref['u'], dt, nfast, ref['Fm'], theta=ref['theta'])
+        ref['tr'].mass_after(ref['M'], ref['Fm'], ref['M1'])
+        ref['tr'].step_many(ref['M'], ref['M1'], ref['Fm'], ref['trc'], order=3)
+        ref['M'].copy_(ref['M1'])
+    bous_ref = make_stack(dg, zb, dev)
+    percall(bous_ref, float(zb['dt']), int(zb['nfast']), 12)
+    air = _air_world(dg, za, dev)
+    bous = make_stack(dg, zb, dev)
+    batch = Batch(0)
+    batch.config(tiles=False, persistent=persistent)
+    batch.add(air['core'], air['h'], air['u'], air['Fm'], tr=air['tr'], M=air['M'], M1=air['M1'], tracers=air['trc'],
+              dt=dt, nfast=nfast, theta=air['theta'])
+    batch.add(bous['core'], bous['h'], bous['u'], bous['Fm'], tr=bous['tr'], M=bous['M'], M1=bous['M1'],
+              tracers=bous['trc'], dt=float(zb['dt']), nfast=int(zb['nfast']))
+    for _ in range(12):
+        batch.step()
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    for x, y in zip(fields(air) + [air['theta']], fields(ref) + [ref['theta']]):
+        assert torch.equal(x, y)
+    for x, y in zip(fields(bous), fields(bous_ref)):
+        assert torch.equal(x, y)
+    with pytest.raises(ValueError):
+        batch.add(air['core'], air['h'], air['u'], air['Fm'], dt=dt, nfast=nfast)        # air layers need theta
