@@ -40,7 +40,9 @@ using namespace bt;
 namespace {
 
 
-template <int PH, int LMAXK>
+// AIR: the kernel also carries the air branch (instantiated only for batches holding air stacks, so the Boussinesq
+// phases keep their register count).
+template <int PH, int LMAXK, bool AIR>
 __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
   int b = blockIdx.x;
   int kind = -1;
@@ -67,11 +69,11 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   const LayersDev &M = d.M;
   if (PH == PH_INIT) {
     if (kind == 0) {
-      if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_stiff_cell<LL>(M, d.h, d.theta, i));
+      if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_stiff_cell<LL>(M, d.h, d.theta, i));
       else ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
       if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, fp64::div_cell<LL>(M, d.u, i));
     } else if (kind == 1) {
-      if (!M.air) ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
+      if (!(AIR && M.air)) ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
     } else if (M.nu4 != 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::curl_vertex<LL>(M, d.u, i));
     }
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_A) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) {
-      if (M.air) {
+      if (AIR && M.air) {
         ISW_BATCH_L(d.L, LMAXK, fp64::air_bern_cell<LL>(M, a.hs, a.us, d.theta, i));
         ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_cell<LL>(M, a.h0, i));
       } else {
@@ -97,18 +99,18 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_E) {
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL, false>(M, a.hs, a.us, i));
-    if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_edge<LL>(M, a.u0, i));
+    if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_edge<LL>(M, a.u0, i));
   } else if (PH == PH_S) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i, M.air ? d.theta : nullptr));
+    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i, AIR && M.air ? d.theta : nullptr));
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) {
-      if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
+      if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
       else fp64::bt_eta_cell_y(M, d.tau[st], j, i);
     }
   } else if (PH == PH_U || PH == PH_UF) {
     if (!d.tiled && j < d.n[st]) {
-      if (M.air) {
+      if (AIR && M.air) {
         ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(M, d.tau[st], i));
       } else {
         fp64::bt_u_edge_y(M, d.tau[st], i);
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     }
   } else if (PH == PH_C || PH == PH_CS) {
     const StageArgs a = stage_args(d, st);
-    if (M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
+    if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
     else if (PH == PH_C) ISW_BATCH_L(d.L, LMAXK, (fp64::scale_cell<LL, false>(M, a, i)));
     else ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     if (kind == 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
       if (st == 2) check_finite_column(d.h, M.g.N, d.L, i, sc.status);
-    } else if (M.air) {
+    } else if (AIR && M.air) {
       ISW_BATCH_L(d.L, LMAXK, fp64::air_u_edge<LL>(M, a, i));
     } else {
       ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_VMIX) {
     if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
   } else if (PH == PH_VHEAT) {
-    if (M.air && d.theta && (M.vmix != 0 || M.vmix_cd != 0) && d.L > 1)
+    if (AIR && M.air && d.theta && (M.vmix != 0 || M.vmix_cd != 0) && d.L > 1)
       ISW_BATCH_L(d.L, LMAXK, fp64::vmix_heat_cell<LL>(M, d.h, d.theta, i));
   } else if (PH == PH_HF1) {
     ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
 // walk the edge chunks (the ubar pass; with flux != 0 a stack's last sub-step also forms its layer fluxes, as PH_UF
 // does) and meet again. The per-item arithmetic is PH_ETA's and PH_U's / PH_UF's, which otherwise take two launches
 // per sub-step; the barrier's acquire makes every block's writes of one pass visible to the next pass.
-template <int LMAXK>
+template <int LMAXK, bool AIR>
 __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restrict__ S, const Sched sc, int st, int nsub,
                                                         int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
   __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        if (d.M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(d.M, d.tau[st], i));
+        if (AIR && d.M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(d.M, d.tau[st], i));
         else fp64::bt_eta_cell_y(d.M, d.tau[st], j, i);
       }
     }
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        if (d.M.air) {
+        if (AIR && d.M.air) {
           ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(d.M, d.tau[st], i));
         } else {
           fp64::bt_u_edge_y(d.M, d.tau[st], i);
@@ -323,14 +325,17 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
   }
 }
 
-const void *fast_grid_kernel(int lmax) {
+template <bool AIR>
+const void *fast_grid_kernel_t(int lmax) {
   switch (lmax) {
-    case 2: return (const void *)k_fast_grid<2>;
-    case 3: return (const void *)k_fast_grid<3>;
-    case 5: return (const void *)k_fast_grid<5>;
-    default: return (const void *)k_fast_grid<8>;
+    case 2: return (const void *)k_fast_grid<2, AIR>;
+    case 3: return (const void *)k_fast_grid<3, AIR>;
+    case 5: return (const void *)k_fast_grid<5, AIR>;
+    default: return (const void *)k_fast_grid<8, AIR>;
   }
 }
+
+const void *fast_grid_kernel(int lmax, bool air) { return air ? fast_grid_kernel_t<true>(lmax) : fast_grid_kernel_t<false>(lmax); }
 
 }  // namespace
 }  // namespace isw
@@ -814,8 +819,10 @@ void rebuild(isw_batch *b) {
   b->s_smem[0] = s_smem[0];
   b->s_smem[1] = s_smem[1];
   if (s_smem[0] > 48 * 1024)
-    for (const void *fn : {(const void *)k_phase<PH_S, 2>, (const void *)k_phase<PH_S, 3>, (const void *)k_phase<PH_S, 5>,
-                           (const void *)k_phase<PH_S, 8>})
+    for (const void *fn : {(const void *)k_phase<PH_S, 2, false>, (const void *)k_phase<PH_S, 3, false>,
+                           (const void *)k_phase<PH_S, 5, false>, (const void *)k_phase<PH_S, 8, false>,
+                           (const void *)k_phase<PH_S, 2, true>, (const void *)k_phase<PH_S, 3, true>,
+                           (const void *)k_phase<PH_S, 5, true>, (const void *)k_phase<PH_S, 8, true>})
       ISW_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_smem[0]));
   if (s_smem[1] > 48 * 1024) slow_phase_smem_mixed(s_smem[1]);
   for (int f = 0; f < 2; f++) {
@@ -823,7 +830,7 @@ void rebuild(isw_batch *b) {
     b->grid_blocks[f] = 0;
     if (!untiled[f]) continue;
     int per = 0;
-    const void *fn = f == 0 ? fast_grid_kernel(b->lmax) : fast_grid_kernel_mixed();
+    const void *fn = f == 0 ? fast_grid_kernel(b->lmax, b->any_air) : fast_grid_kernel_mixed();
     ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, THREADS, 0));
     b->grid_blocks[f] = std::max(1, per) * b->sms;
   }
@@ -848,11 +855,20 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = tr
       continue;
     }
     const size_t smem = PH == PH_S ? b->s_smem[0] : 0;
-    switch (b->lmax) {
-      case 2: launch_phase_kernel(k_phase<PH, 2>, nb, st, p, smem, b->cur, sc, stage, j); break;
-      case 3: launch_phase_kernel(k_phase<PH, 3>, nb, st, p, smem, b->cur, sc, stage, j); break;
-      case 5: launch_phase_kernel(k_phase<PH, 5>, nb, st, p, smem, b->cur, sc, stage, j); break;
-      default: launch_phase_kernel(k_phase<PH, 8>, nb, st, p, smem, b->cur, sc, stage, j); break;
+    if (b->any_air) {
+      switch (b->lmax) {
+        case 2: launch_phase_kernel(k_phase<PH, 2, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        case 3: launch_phase_kernel(k_phase<PH, 3, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        case 5: launch_phase_kernel(k_phase<PH, 5, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        default: launch_phase_kernel(k_phase<PH, 8, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
+      }
+    } else {
+      switch (b->lmax) {
+        case 2: launch_phase_kernel(k_phase<PH, 2, false>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        case 3: launch_phase_kernel(k_phase<PH, 3, false>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        case 5: launch_phase_kernel(k_phase<PH, 5, false>, nb, st, p, smem, b->cur, sc, stage, j); break;
+        default: launch_phase_kernel(k_phase<PH, 8, false>, nb, st, p, smem, b->cur, sc, stage, j); break;
+      }
     }
   }
 }
@@ -904,12 +920,10 @@ void launch_fast_grid(isw_batch *b, cudaStream_t st, int stage, bool flux) {
     cfg.numAttrs = 1;
     if (f == 0) {
       const int fl = flux ? 1 : 0, ns = b->nsub[stage];
-      switch (b->lmax) {
-        case 2: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<2>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
-        case 3: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<3>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
-        case 5: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<5>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
-        default: ISW_CUDA(cudaLaunchKernelEx(&cfg, k_fast_grid<8>, b->cur, sc, stage, ns, fl, b->bar, b->status, DEFAULT_TIMEOUT_NS)); break;
-      }
+      long long to = DEFAULT_TIMEOUT_NS;
+      void *args[] = {(void *)&b->cur, (void *)&sc, (void *)&stage, (void *)&ns, (void *)&fl, (void *)&b->bar,
+                      (void *)&b->status, (void *)&to};
+      ISW_CUDA(cudaLaunchKernelExC(&cfg, fast_grid_kernel(b->lmax, b->any_air), args));
     } else
       launch_fast_grid_mixed(cfg, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status, DEFAULT_TIMEOUT_NS);
   }
