@@ -40,9 +40,10 @@ using namespace bt;
 namespace {
 
 
-// AIR: the kernel also carries the air branch (instantiated only for batches holding air stacks, so the Boussinesq
-// phases keep their register count).
-template <int PH, int LMAXK, bool AIR>
+// EXT: the kernel also carries the air branch and the option branches (walls, the shelf and its bed flags, per-cell
+// buoyancy, the tide, the bottom's drag), instantiated only for batches holding such stacks, so that the plain
+// Boussinesq phases keep their register count.
+template <int PH, int LMAXK, bool EXT>
 __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
   int b = blockIdx.x;
   int kind = -1;
@@ -62,18 +63,20 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::stage_pk<LL>(d.M, ch.begin / THREADS, stg));
     __syncthreads();
-    if (i < ch.end) ISW_BATCH_L(d.L, LMAXK, (fp64::slow_edge<LL, false, true>(d.M, a.us, a.cdt, i, nullptr, stg)));
+    if (i < ch.end) ISW_BATCH_L(d.L, LMAXK, (fp64::slow_edge<LL, EXT, true>(d.M, a.us, a.cdt, i, nullptr, stg)));
     return;
   }
   if (i >= ch.end) return;
   const LayersDev &M = d.M;
-  if (PH == PH_INIT) {
+  if (PH == PH_ONBED) {                      // the shelf's bed flags of every layer, before the step's first pass reads them
+    if (EXT && M.ob) ISW_BATCH_L(d.L, LMAXK, fp64::onbed_cell<LL>(M, d.h, i));
+  } else if (PH == PH_INIT) {
     if (kind == 0) {
-      if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_stiff_cell<LL>(M, d.h, d.theta, i));
+      if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_stiff_cell<LL>(M, d.h, d.theta, i));
       else ISW_BATCH_L(d.L, LMAXK, fp64::eta0_cell<LL>(M, d.h, i));
       if (M.nu4 != 0) ISW_BATCH_L(d.L, LMAXK, fp64::div_cell<LL>(M, d.u, i));
     } else if (kind == 1) {
-      if (!(AIR && M.air)) ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, false>(M, d.h, d.u, i));
+      if (!(EXT && M.air)) ISW_BATCH_L(d.L, LMAXK, fp64::ubar0_edge<LL, EXT>(M, d.h, d.u, i));
     } else if (M.nu4 != 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::curl_vertex<LL>(M, d.u, i));
     }
@@ -87,61 +90,61 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_A) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) {
-      if (AIR && M.air) {
+      if (EXT && M.air) {
         ISW_BATCH_L(d.L, LMAXK, fp64::air_bern_cell<LL>(M, a.hs, a.us, d.theta, i));
         ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_cell<LL>(M, a.h0, i));
       } else {
-        ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL, false>(M, a.hs, a.us, i));
+        ISW_BATCH_L(d.L, LMAXK, fp64::bern_cell<LL, EXT>(M, a.hs, a.us, i));
       }
     } else {
       ISW_BATCH_L(d.L, LMAXK, fp64::pv_vertex<LL>(M, a.hs, a.us, i));
     }
   } else if (PH == PH_E) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL, false>(M, a.hs, a.us, i));
-    if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_edge<LL>(M, a.u0, i));
+    ISW_BATCH_L(d.L, LMAXK, fp64::edge_hq<LL, EXT>(M, a.hs, a.us, i));
+    if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_fast_init_edge<LL>(M, a.u0, i));
   } else if (PH == PH_S) {
     const StageArgs a = stage_args(d, st);
-    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, false>(M, a.us, a.cdt, i, AIR && M.air ? d.theta : nullptr));
+    ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, EXT>(M, a.us, a.cdt, i, EXT && M.air ? d.theta : nullptr));
   } else if (PH == PH_ETA) {
     if (!d.tiled && j < d.n[st]) {
-      if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
+      if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
       else fp64::bt_eta_cell_y(M, d.tau[st], j, i);
     }
   } else if (PH == PH_U || PH == PH_UF) {
     if (!d.tiled && j < d.n[st]) {
-      if (AIR && M.air) {
+      if (EXT && M.air) {
         ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(M, d.tau[st], i));
       } else {
-        fp64::bt_u_edge_y(M, d.tau[st], i);
-        if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<false>(M, stage_args(d, st), M.acc[i], i);
+        fp64::bt_u_edge_y<EXT>(M, d.tau[st], i);
+        if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<EXT>(M, stage_args(d, st), M.acc[i], i);
       }
     }
   } else if (PH == PH_C || PH == PH_CS) {
     const StageArgs a = stage_args(d, st);
-    if (AIR && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
-    else if (PH == PH_C) ISW_BATCH_L(d.L, LMAXK, (fp64::scale_cell<LL, false>(M, a, i)));
+    if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
+    else if (PH == PH_C) ISW_BATCH_L(d.L, LMAXK, (fp64::scale_cell<LL, EXT>(M, a, i)));
     else ISW_BATCH_L(d.L, LMAXK, fp64::scale_sum_cell<LL>(M, a, i));
   } else if (PH == PH_D) {
     const StageArgs a = stage_args(d, st);
     if (kind == 0) {
       ISW_BATCH_L(d.L, LMAXK, fp64::h_cell<LL>(M, a, i));
       if (st == 2) check_finite_column(d.h, M.g.N, d.L, i, sc.status);
-    } else if (AIR && M.air) {
+    } else if (EXT && M.air) {
       ISW_BATCH_L(d.L, LMAXK, fp64::air_u_edge<LL>(M, a, i));
     } else {
-      ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, false>(M, a, i));
+      ISW_BATCH_L(d.L, LMAXK, fp64::u_edge<LL, EXT>(M, a, i));
     }
   } else if (PH == PH_VMIX) {
-    if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
+    if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, EXT>(M, d.h, d.u, d.dt, i));
   } else if (PH == PH_VHEAT) {
-    if (AIR && M.air && d.theta && (M.vmix != 0 || M.vmix_cd != 0) && d.L > 1)
+    if (EXT && M.air && d.theta && (M.vmix != 0 || M.vmix_cd != 0) && d.L > 1)
       ISW_BATCH_L(d.L, LMAXK, fp64::vmix_heat_cell<LL>(M, d.h, d.theta, i));
   } else if (PH == PH_HF1) {
     ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
   } else if (PH == PH_POST) {
     if (kind == 1) {
-      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, false>(M, d.h, d.u, d.dt, i));
+      if ((M.vmix != 0 || M.vmix_cd != 0) && d.L > 1) ISW_BATCH_L(d.L, LMAXK, fp64::vmix_edge<LL, EXT>(M, d.h, d.u, d.dt, i));
     } else {
       ISW_BATCH_L(d.L, LMAXK, fp64::tr_hf_edge<LL>(d.T, d.tr, 1, i / M.g.E, i % M.g.E));
     }
@@ -282,7 +285,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast(const StackDesc *__restrict__
 // walk the edge chunks (the ubar pass; with flux != 0 a stack's last sub-step also forms its layer fluxes, as PH_UF
 // does) and meet again. The per-item arithmetic is PH_ETA's and PH_U's / PH_UF's, which otherwise take two launches
 // per sub-step; the barrier's acquire makes every block's writes of one pass visible to the next pass.
-template <int LMAXK, bool AIR>
+template <int LMAXK, bool EXT>
 __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restrict__ S, const Sched sc, int st, int nsub,
                                                         int flux, GridBarrier *bar, BatchStatus *status, long long timeout_ns) {
   __shared__ __align__(16) unsigned char buf[sizeof(StackDesc)];
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        if (AIR && d.M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(d.M, d.tau[st], i));
+        if (EXT && d.M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(d.M, d.tau[st], i));
         else fp64::bt_eta_cell_y(d.M, d.tau[st], j, i);
       }
     }
@@ -313,11 +316,11 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        if (AIR && d.M.air) {
+        if (EXT && d.M.air) {
           ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(d.M, d.tau[st], i));
         } else {
-          fp64::bt_u_edge_y(d.M, d.tau[st], i);
-          if (flux && j == d.n[st] - 1) fp64::flux_edge<false>(d.M, stage_args(d, st), d.M.acc[i], i);
+          fp64::bt_u_edge_y<EXT>(d.M, d.tau[st], i);
+          if (flux && j == d.n[st] - 1) fp64::flux_edge<EXT>(d.M, stage_args(d, st), d.M.acc[i], i);
         }
       }
     }
@@ -325,17 +328,17 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid(const StackDesc *__restri
   }
 }
 
-template <bool AIR>
+template <bool EXT>
 const void *fast_grid_kernel_t(int lmax) {
   switch (lmax) {
-    case 2: return (const void *)k_fast_grid<2, AIR>;
-    case 3: return (const void *)k_fast_grid<3, AIR>;
-    case 5: return (const void *)k_fast_grid<5, AIR>;
-    default: return (const void *)k_fast_grid<8, AIR>;
+    case 2: return (const void *)k_fast_grid<2, EXT>;
+    case 3: return (const void *)k_fast_grid<3, EXT>;
+    case 5: return (const void *)k_fast_grid<5, EXT>;
+    default: return (const void *)k_fast_grid<8, EXT>;
   }
 }
 
-const void *fast_grid_kernel(int lmax, bool air) { return air ? fast_grid_kernel_t<true>(lmax) : fast_grid_kernel_t<false>(lmax); }
+const void *fast_grid_kernel(int lmax, bool ext) { return ext ? fast_grid_kernel_t<true>(lmax) : fast_grid_kernel_t<false>(lmax); }
 
 }  // namespace
 }  // namespace isw
@@ -348,6 +351,7 @@ struct BatchSlot {
   isw_transport *tr = nullptr;
   double *h = nullptr, *u = nullptr, *Fm = nullptr, *M = nullptr, *M1 = nullptr;
   double *theta = nullptr;                  // air layers: the layers' potential temperature (L x N), else null
+  int version = 0;                          // the layers' option version the descriptors were built from
   double *tracers[TRMAX] = {};
   int ntr = 0;
   double dt = 0;
@@ -377,6 +381,8 @@ struct isw_batch {
   int lmax = 1, nstacks = 0, ntiles = 0, nsub[3] = {0, 0, 0}, kused = 0;
   std::vector<FastGroup> groups;              // cooperative launches of the fast loop (tiles [begin, begin + count))
   int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, any_air = 0;
+  int any_ext = 0;                            // air or option stacks: the phase kernels with those branches
+  int any_ob = 0;                             // a stack with the shelf's bed flags: their pass opens the step
   size_t fast_smem = 0;
   int fast_bps = 2;                           // tile blocks per SM: 2 (512 threads each) or 1 (1024 threads)
   GridBarrier *bar = nullptr;
@@ -538,7 +544,14 @@ int form_of(const BatchSlot &sl) { return sl.layers->d.precision == ISW_MIXED ? 
 
 // A batch holding stacks of both forms tiles the fast loop of its mixed stacks only (one tile kernel per batch); its
 // FP64 stacks take the grid-wide sub-step kernels.
-bool tiles_form(const isw_batch *b, const BatchSlot &sl) { return sl.used && !sl.layers->d.air && form_of(sl) == b->mixed; }
+// Stacks with option branches: walls, the shelf (and its bed flags), per-cell buoyancy, the tide, the bottom's drag.
+bool has_options(const isw::LayersDev &d) {
+  return d.wall || d.ob || d.shelf > 0 || d.sig || d.tide || d.cbot || d.cd_bot > 0;
+}
+
+bool tiles_form(const isw_batch *b, const BatchSlot &sl) {
+  return sl.used && !sl.layers->d.air && !has_options(sl.layers->d) && form_of(sl) == b->mixed;
+}
 
 Tiling plan_shared(isw_batch *b, int bps) {
   Tiling t;
@@ -614,7 +627,7 @@ void rebuild(isw_batch *b) {
   b->mixed = 0;
   for (auto &sl : b->slots)
     if (sl.used && form_of(sl) == 1) b->mixed = 1;
-  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, any_air = 0, lmax = 1;
+  int any_nu4 = 0, any_vmix = 0, any_tr = 0, any_untiled = 0, any_air = 0, any_ext = 0, any_ob = 0, lmax = 1;
   int untiled[2] = {0, 0};
   size_t s_smem[2] = {0, 0};
   const double cs[3] = {1.0 / 3.0, 1.0 / 2.0, 1.0};
@@ -647,6 +660,8 @@ void rebuild(isw_batch *b) {
     d.h = sl.h; d.u = sl.u; d.Fm = sl.Fm; d.Mm = sl.M;
     d.theta = sl.theta;
     if (d.M.air) any_air = 1;
+    if (d.M.air || has_options(d.M)) any_ext = 1;
+    if (d.M.ob) any_ob = 1;
     d.dt = sl.dt;
     d.L = d.M.L;
     lmax = std::max(lmax, d.L);
@@ -815,6 +830,8 @@ void rebuild(isw_batch *b) {
   b->any_tr = any_tr;
   b->any_untiled = any_untiled;
   b->any_air = any_air;
+  b->any_ext = any_ext;
+  b->any_ob = any_ob;
   b->lmax = kernel_lmax(lmax);
   b->s_smem[0] = s_smem[0];
   b->s_smem[1] = s_smem[1];
@@ -830,7 +847,7 @@ void rebuild(isw_batch *b) {
     b->grid_blocks[f] = 0;
     if (!untiled[f]) continue;
     int per = 0;
-    const void *fn = f == 0 ? fast_grid_kernel(b->lmax, b->any_air) : fast_grid_kernel_mixed();
+    const void *fn = f == 0 ? fast_grid_kernel(b->lmax, b->any_ext) : fast_grid_kernel_mixed();
     ISW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, THREADS, 0));
     b->grid_blocks[f] = std::max(1, per) * b->sms;
   }
@@ -855,7 +872,7 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = tr
       continue;
     }
     const size_t smem = PH == PH_S ? b->s_smem[0] : 0;
-    if (b->any_air) {
+    if (b->any_ext) {
       switch (b->lmax) {
         case 2: launch_phase_kernel(k_phase<PH, 2, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
         case 3: launch_phase_kernel(k_phase<PH, 3, true>, nb, st, p, smem, b->cur, sc, stage, j); break;
@@ -923,7 +940,7 @@ void launch_fast_grid(isw_batch *b, cudaStream_t st, int stage, bool flux) {
       long long to = DEFAULT_TIMEOUT_NS;
       void *args[] = {(void *)&b->cur, (void *)&sc, (void *)&stage, (void *)&ns, (void *)&fl, (void *)&b->bar,
                       (void *)&b->status, (void *)&to};
-      ISW_CUDA(cudaLaunchKernelExC(&cfg, fast_grid_kernel(b->lmax, b->any_air), args));
+      ISW_CUDA(cudaLaunchKernelExC(&cfg, fast_grid_kernel(b->lmax, b->any_ext), args));
     } else
       launch_fast_grid_mixed(cfg, b->cur, sc, stage, b->nsub[stage], flux ? 1 : 0, b->bar, b->status, DEFAULT_TIMEOUT_NS);
   }
@@ -932,7 +949,8 @@ void launch_fast_grid(isw_batch *b, cudaStream_t st, int stage, bool flux) {
 // The dynamics of one step (through the last stage's D). The first kernel and the first after a tile launch (or a
 // memset) take plain stream order; the others are programmatic dependents of the kernel before them.
 void enqueue_dyn(isw_batch *b, cudaStream_t st) {
-  launch_phase<PH_INIT>(b, st, 0, 0, false);
+  if (b->any_ob) launch_phase<PH_ONBED>(b, st, 0, 0, false);
+  launch_phase<PH_INIT>(b, st, 0, 0, !b->any_ob ? false : true);
   if (b->any_nu4) {
     launch_phase<PH_LAPE1>(b, st, 0, 0);
     launch_phase<PH_LAPCV>(b, st, 0, 0);
@@ -1076,6 +1094,11 @@ void settle(isw_batch *b) {
 }
 
 void step(isw_batch *b, cudaStream_t st) {
+  for (auto &sl : b->slots)                  // an option set on a registered stack since: rebuild its descriptor
+    if (sl.used && sl.version != sl.layers->version) {
+      sl.version = sl.layers->version;
+      b->dirty = true;
+    }
   prepare(b);
   if (b->nstacks == 0) return;
   if (b->pipeline) {
@@ -1160,9 +1183,8 @@ int batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, do
     if (layers->grid->device != b->device) fail(ISW_EINVAL, "batch.add: the stack is on another device");
     if (layers->d.air && !theta) fail(ISW_EINVAL, "batch.add: air layers need their theta (isw_batch_add_air)");
     if (!layers->d.air && theta) fail(ISW_EINVAL, "batch.add: theta is for air layers");
-    if (layers->d.wall || layers->d.ob || layers->d.shelf > 0 || layers->d.sig || layers->d.tide || layers->d.cbot ||
-        layers->d.cd_bot > 0)
-      fail(ISW_EUNSUPPORTED, "batch.add: the option branches (walls, shelf, sig, tide, bottom drag) step call by call");
+    if (has_options(layers->d) && layers->d.precision != ISW_FP64)
+      fail(ISW_EUNSUPPORTED, "batch.add: the option branches step in the FP64 form");
     if (!(dt > 0) || !std::isfinite(dt) || nfast < 1) fail(ISW_EINVAL, "batch.add: dt must be positive and nfast >= 1");
     if (tr) {
       if (!M || !M1 || !tracers) fail(ISW_EINVAL, "batch.add: transport needs M, M1 and the tracers");
@@ -1178,6 +1200,7 @@ int batch_add(isw_batch *b, isw_layers *layers, isw_transport *tr, double *h, do
     sl.tr = tr;
     sl.h = h; sl.u = u; sl.Fm = Fm; sl.M = M; sl.M1 = M1;
     sl.theta = theta;
+    sl.version = layers->version;
     if (layers->d.air && layers->d.nu4 != 0) layers->nu4dt = layers->d.nu4 * dt;   // the step's nabla^4 loss (exchange heat)
     sl.ntr = tr ? ntr : 0;
     for (int j = 0; j < sl.ntr; j++) {

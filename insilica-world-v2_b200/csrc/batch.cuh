@@ -170,7 +170,7 @@ __device__ __forceinline__ const StackDesc &stage_desc(const StackDesc *S, int s
 // PH_UF / PH_CS: the grid-wide edge sub-step that also forms the layer fluxes on a stack's last sub-step, and phase C
 // summing them; used by batches with no tiled stack in place of PH_U / PH_C.
 enum Phase { PH_INIT, PH_LAPE1, PH_LAPCV, PH_LAPE2, PH_A, PH_E, PH_S, PH_ETA, PH_U, PH_C, PH_D, PH_POST, PH_P2, PH_P3, PH_P4,
-             PH_P1, PH_P2E, PH_P3E, PH_VMIX, PH_HF1, PH_UF, PH_CS, PH_VHEAT };
+             PH_P1, PH_P2E, PH_P3E, PH_VMIX, PH_HF1, PH_UF, PH_CS, PH_VHEAT, PH_ONBED };
 
 // Programmatic dependent launch between phase kernels: a phase kernel is launched while the previous one drains; it
 // stages only constant data (its stack descriptor) before waiting for the previous grid's completion and memory
@@ -197,7 +197,7 @@ void launch_phase_kernel(void (*kern)(KA...), int nb, cudaStream_t st, bool pdl,
 template <int PH>
 struct Dom {
   static constexpr bool cell = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A || PH == PH_ETA || PH == PH_C || PH == PH_D ||
-                               PH == PH_CS || PH == PH_VHEAT;
+                               PH == PH_CS || PH == PH_VHEAT || PH == PH_ONBED;
   static constexpr bool edge = PH == PH_INIT || PH == PH_LAPE1 || PH == PH_LAPE2 || PH == PH_E || PH == PH_S || PH == PH_U ||
                                PH == PH_D || PH == PH_POST || PH == PH_VMIX || PH == PH_UF;
   static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;

@@ -25,6 +25,7 @@ struct isw_layers {
   int colmax_blocks;
   int *nonfinite;
   double nu4dt = 0;                 // nu4 dt of the last step (the exchange books the step's nabla^4 loss as heat)
+  int version = 0;                  // bumped when an option is set: batches holding the stack rebuild its descriptor
   bool percall = false;             // FP64: step with the per-call kernels instead of the private batch
   // the mixed form steps call by call through a private one-stack batch (its step graph and tiles)
   isw_batch *solo = nullptr;

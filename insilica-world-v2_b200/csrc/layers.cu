@@ -679,6 +679,7 @@ int isw_layers_set_option(isw_layers *s, int option, const double *array, double
     }
     for (auto &e : s->graphs) cudaGraphExecDestroy(e.exec);   // the step graphs hold the old descriptor
     s->graphs.clear();
+    s->version++;
   });
 }
 

@@ -449,12 +449,17 @@ __device__ __forceinline__ void bt_eta_cell_y(const LayersDev &M, double tau, in
   M.eta_prev[i] = M.Gc[i] * (en + M.div_damp * (en - e0));
 }
 
+template <bool OPT = false>
 __device__ __forceinline__ void bt_u_edge_y(const LayersDev &M, double tau, int e) {
   const GridDev &g = M.g;
   const double v = M.ub[e];
   M.acc[e] += v;
   const double *Y = M.eta_prev;
   M.ub[e] = v + tau * ((-(Y[g.eJ[e]] - Y[g.eI[e]])) / g.de[e] + M.G[e]);
+  if (walled<OPT>(M, e)) {         // walls (reference layers.py:173-174), as bt_u_edge
+    M.ub[e] = 0.0;
+    M.acc[e] = 0.0;
+  }
 }
 
 // The layer fluxes of edge e once the stage's fast loop has finished (reference lay_flux, layers.cu:392-397), every

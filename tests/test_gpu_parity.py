@@ -441,21 +441,27 @@ def test_exchange_bit_exact(dev, isw, grid4):
 def test_option_branches_golden(dev, isw, grid4):
     """Every option branch of Boussinesq layers at once on the reference's outcrop case (walls, the shelf with its bed
     flags, per-cell buoyancy, a tide potential, the bottom's quadratic and internal-tide drag), set as the reference's
-    callers set them: h, u, Fm after 1 and 12 steps to 1e-12 of the reference's (its stress term calls exp), and the
-    step with walls refused by a batch."""
+    callers set them: h, u, Fm after 1 and 12 steps to 1e-12 of the reference's (its stress term calls exp), call by
+    call and through a batch (beside a plain stack, with two launches per sub-step and with the persistent loop), the
+    batched run equal to the call-by-call one bit for bit."""
     gpu, layers, _ = isw
+    from isw.batch import Batch
     z = golden('options_n4')
     dg = gpu.DeviceGrid(grid4)
-    core = layers.Layers(dg, 2, b=z['b'], gprime=[0.02], stress=[0.0, 2.5e-4], nu4=float(z['nu4']), floor=1.0,
-                         wall=z['wall'], shelf=50.0, shelf_bed=True)
     sig, tide, cbot = T(z['sig'], dev), T(z['tide'], dev), T(z['cbot'], dev)
-    core.sig, core.zm = sig, torch.zeros_like(sig)
-    core.tide = tide
-    core.cd_bot = 2.5e-3
-    core.cbot = cbot
+    dt, nfast = float(z['dt']), int(z['nfast'])
+
+    def options_core():
+        core = layers.Layers(dg, 2, b=z['b'], gprime=[0.02], stress=[0.0, 2.5e-4], nu4=float(z['nu4']), floor=1.0,
+                             wall=z['wall'], shelf=50.0, shelf_bed=True)
+        core.sig, core.zm = sig, torch.zeros_like(sig)
+        core.tide = tide
+        core.cd_bot = 2.5e-3
+        core.cbot = cbot
+        return core
+    core = options_core()
     h, u = T(z['h0'], dev), T(z['u0'], dev)
     Fm = torch.zeros_like(u)
-    dt, nfast = float(z['dt']), int(z['nfast'])
     assert core.substeps(h, dt) * 1.2 <= nfast
     for s in range(1, 13):
         core.step(h, u, dt, nfast, Fm)
@@ -465,6 +471,19 @@ def test_option_branches_golden(dev, isw, grid4):
             for name, x in (('h', h), ('u', u), ('Fm', Fm)):
                 e = rel(x.cpu().numpy(), z[name + sfx])
                 assert e <= REL, (s, name, e)
-    from isw.batch import Batch
-    with pytest.raises(NotImplementedError):
-        Batch(0).add(core, h, u, Fm, dt=dt, nfast=nfast)
+    w2 = golden('w2_n4')
+    for persistent in (False, True):
+        bcore = options_core()
+        hb, ub = T(z['h0'], dev), T(z['u0'], dev)
+        Fb = torch.zeros_like(ub)
+        plain = layers.Layers(dg, 1, b=w2['b'])
+        hp, up = T(w2['h0'], dev), T(w2['u0'], dev)
+        batch = Batch(0)
+        batch.config(persistent=persistent)
+        batch.add(bcore, hb, ub, Fb, dt=dt, nfast=nfast)
+        batch.add(plain, hp, up, torch.zeros_like(up), dt=float(w2['dt']), nfast=int(w2['nfast']))
+        for _ in range(12):
+            batch.step()
+        torch.cuda.synchronize()
+        assert batch.status() == 0
+        assert torch.equal(hb, h) and torch.equal(ub, u) and torch.equal(Fb, Fm), persistent
