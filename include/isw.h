@@ -166,6 +166,10 @@ int isw_layers_mask(isw_layers *s, double *a, int rows, void *stream);
 /* The status word of the one-stack batch that isw_layers_step uses (as isw_batch_status; ISW_OK when the handle steps
  * call by call). While it holds ISW_ETIMEOUT or ISW_ENOTFINITE, isw_layers_step refuses with that status. */
 int isw_layers_status(isw_layers *s, void *stream, int reset);
+/* Replace the bottom height b (N values, a DEVICE pointer, copied on `stream`) the layers rest on: the reference's
+ * Layers.b (layers.py:55), which it fixes at construction; here a served request's layers are reused for the next
+ * request of the same kind with that request's own terrain. */
+int isw_layers_set_bottom(isw_layers *s, const double *b, void *stream);
 
 int isw_transport_create(isw_grid *g, int L, double beta, int tracers, int precision, isw_transport **out);
 int isw_transport_destroy(isw_transport *t);

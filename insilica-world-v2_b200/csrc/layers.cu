@@ -726,6 +726,15 @@ int isw_layers_mask(isw_layers *s, double *a, int rows, void *stream) {
   });
 }
 
+int isw_layers_set_bottom(isw_layers *s, const double *b, void *stream) {
+  return guarded([&] {
+    if (!s || !b) fail(ISW_EINVAL, "layers.set_bottom: null handle or array");
+    ISW_CUDA(cudaSetDevice(s->grid->device));
+    ISW_CUDA(cudaMemcpyAsync(const_cast<double *>(s->d.b), b, sizeof(double) * (size_t)s->d.g.N, cudaMemcpyDeviceToDevice,
+                             (cudaStream_t)stream));
+  });
+}
+
 int isw_layers_status(isw_layers *s, void *stream, int reset) {
   if (!s) {
     set_last_error("layers.status: null handle");

@@ -59,6 +59,7 @@ isw_layers_lap = _sig('isw_layers_lap', I, [P, P, P, P])
 isw_layers_vmix_heat = _sig('isw_layers_vmix_heat', I, [P, P, P, P, D, D, D, D, P])
 isw_layers_mask = _sig('isw_layers_mask', I, [P, P, I, P])
 isw_layers_status = _sig('isw_layers_status', I, [P, P, I])
+isw_layers_set_bottom = _sig('isw_layers_set_bottom', I, [P, P, P])
 isw_transport_create = _sig('isw_transport_create', I, [P, I, D, I, I, ctypes.POINTER(P)])
 isw_transport_destroy = _sig('isw_transport_destroy', I, [P])
 isw_transport_mass_after = _sig('isw_transport_mass_after', I, [P, P, P, P, P])

@@ -149,6 +149,14 @@ class Layers:
         _lib.check(_lib.isw_layers_mask(self._h, device_ptr(a, name='a', device=dev, numel=int(rows) * self.dg.E), int(rows),
                                         stream_of(dev, stream)))
 
+    def set_bottom(self, b, stream=None):
+        """Replace the bottom height the layers rest on (N values): the core's copy and this object's `b`."""
+        bt = b if isinstance(b, torch.Tensor) else torch.as_tensor(np.asarray(b, dtype=np.float64))
+        bt = bt.to(device=self.b.device, dtype=torch.float64).contiguous()
+        _lib.check(_lib.isw_layers_set_bottom(self._h, device_ptr(bt, shape=(self.dg.N,), name='b', device=self.dg.device),
+                                              stream_of(self.dg.device, stream)))
+        self.b.copy_(bt)
+
     def status(self, reset=False, stream=None):
         """The status word of the one-stack batch this Layers steps through: 0, ISW_ETIMEOUT (5) after a fast-loop barrier
         timed out, or ISW_ENOTFINITE (6) after a step left a NaN or Inf thickness. While it is set, step() raises; reset

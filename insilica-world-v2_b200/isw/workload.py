@@ -68,6 +68,22 @@ class Stack:
         for name, t in [('h', self.h), ('u', self.u), ('M', self.M)] + [(f'tr{j}', x) for j, x in enumerate(self.tracers)]:
             t.copy_(torch.as_tensor(arrays[prefix + name], device=t.device))
 
+    def reset(self, state):
+        """Start this stack over from a new initial state of the same kind (a stack_state dict for the same grid, layer
+        count and tracers): h, u, the tracers and the bottom from the state, M = h x area, M1 and Fm cleared. The Layers
+        and Transport objects and every device array are kept."""
+        s = state
+        dev = self.h.device
+        self.h.copy_(torch.as_tensor(np.ascontiguousarray(s['h']), dtype=torch.float64, device=dev))
+        self.u.copy_(torch.as_tensor(np.ascontiguousarray(s['u']), dtype=torch.float64, device=dev))
+        A = torch.as_tensor(self.dg.host.areaCell, dtype=torch.float64, device=dev)
+        self.M.copy_(self.h * A[None])
+        self.M1.zero_()
+        self.Fm.zero_()
+        for t, x in zip(self.tracers, s['tracers']):
+            t.copy_(torch.as_tensor(np.ascontiguousarray(x), dtype=torch.float64, device=dev))
+        self.core.set_bottom(s['b'])
+
     def register(self, batch):
         """Add this stack to a Batch: the batch's step then does this stack's step(), with M <- M1 copied (not swapped)."""
         return batch.add(self.core, self.h, self.u, self.Fm, tr=self.tr if self.T else None, M=self.M, M1=self.M1,
@@ -131,6 +147,13 @@ class Member:
     def finite(self):
         """Whether every stack's thicknesses are finite (a device reduction; synchronises)."""
         return all(bool(torch.isfinite(s.h).all()) for s in self.stacks)
+
+    def reset(self, states, batch=None):
+        """Reuse this member for new initial states of the same kinds (Stack.reset), registered with `batch` if given."""
+        for st, s in zip(self.stacks, states):
+            st.reset(s)
+        if batch is not None:
+            self.batch, self.slots = batch, [st.register(batch) for st in self.stacks]
 
     def unregister(self):
         if self.batch is not None:

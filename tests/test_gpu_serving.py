@@ -126,3 +126,23 @@ def test_nonfinite_request_dropped_others_complete(dev, grids):
         assert not res['with_bad'][rid].error
         for x, y in zip(res['clean'][rid].state, res['with_bad'][rid].state):
             assert torch.equal(x, y)
+
+
+def test_reused_member_equals_fresh(dev, grids):
+    """A request admitted into the member a finished request of the same kind left behind (its state, terrain and
+    tracers loaded into it) ends bit for bit where it ends in a fresh server."""
+    from isw.serving import Request, Server
+
+    def run(reqs, budget):
+        srv = Server(0, budget_bytes=budget, precision='mixed', ntracers=2, grids=grids, keep_state=True)
+        res, _ = srv.run(reqs)
+        assert srv.batch.status() == 0
+        return {r.rid: r for r in res}, srv
+    first = Request(0, 0.0, 4, 0.2, 5, seed=91)
+    second = Request(1, 0.0, 4, 0.1, 5, seed=92)
+    both, srv = run([first, second], 1.0)                 # one resident at a time: the second reuses the first's member
+    assert sum(len(v) for v in srv._pool.values()) == 1 and both[1].admitted >= both[0].done - 1e-3
+    alone, _ = run([Request(1, 0.0, 4, 0.1, 5, seed=92)], 150e9)
+    assert both[1].steps == alone[1].steps
+    for x, y in zip(both[1].state, alone[1].state):
+        assert torch.equal(x, y)
