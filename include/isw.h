@@ -220,6 +220,12 @@ int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, in
  * instead of two kernel launches per sub-step (0, the default). Results are bit-identical either way. This core's own
  * layout choice: no counterpart in the reference (whose Layers.step launches two kernels per sub-step, layers.py:168-175). */
 int isw_batch_grid_loop(isw_batch *b, int persistent);
+/* The fast-loop layout of the stacks on grids of one level (an ensemble or a serving mix holds several): mode 0 follows
+ * the batch's configuration (the default), 1 keeps them untiled (grid-wide sub-steps), 2 tiles them in the packed layout
+ * with about tile_cells owned cells per tile (0: the batch's) and an exchange interval of at most tile_k (0: the
+ * batch's); the packed layout must be allowed by isw_batch_config (tiles on). Results are the same under every layout.
+ * This core's layout choice: no counterpart in the reference. */
+int isw_batch_level_layout(isw_batch *b, int level, int mode, int tile_cells, int tile_k);
 /* Pipelined steps (on != 0): each isw_batch_step queues a step's dynamics beside the previous step's transport (two
  * branches of one graph, the step's layer fluxes Fm double-buffered), so the registered masses M and tracers lag the
  * dynamics by one step until isw_batch_flush, which completes the last step's transport and puts its Fm in the

@@ -394,6 +394,12 @@ struct isw_batch {
   int tile_cells = 0;                         // packed layout's owned cells per tile (0: by blocks per SM)
   int force_bps = 0;                          // 0: choose; 1 or 2 tile blocks per SM
   int layout = 0;                             // 0: choose; 1 shared; 2 packed
+  // per grid level: 0 follows the batch (default); 1 untiled; 2 packed tiles of about `cells` owned cells (0: the
+  // batch's), exchange interval at most `k` (0: the batch's)
+  struct LevelLayout {
+    int mode = 0, cells = 0, k = 0;
+  };
+  std::map<int, LevelLayout> levels;
   bool pdl = true;                            // programmatic dependent launch between phase kernels
   bool fast_grid = false;                     // untiled stacks' sub-steps: one cooperative launch per stage (k_fast_grid)
   int untiled_form[2] = {0, 0};               // per form (FP64, mixed): any untiled stack
@@ -549,8 +555,14 @@ bool has_options(const isw::LayersDev &d) {
   return d.wall || d.ob || d.shelf > 0 || d.sig || d.tide || d.cbot || d.cd_bot > 0;
 }
 
+isw_batch::LevelLayout level_layout(const isw_batch *b, const BatchSlot &sl) {
+  const auto it = b->levels.find(sl.layers->grid->n);
+  return it == b->levels.end() ? isw_batch::LevelLayout{} : it->second;
+}
+
 bool tiles_form(const isw_batch *b, const BatchSlot &sl) {
-  return sl.used && !sl.layers->d.air && !has_options(sl.layers->d) && form_of(sl) == b->mixed;
+  return sl.used && !sl.layers->d.air && !has_options(sl.layers->d) && form_of(sl) == b->mixed &&
+         level_layout(b, sl).mode != 1;
 }
 
 Tiling plan_shared(isw_batch *b, int bps) {
@@ -591,16 +603,19 @@ Tiling plan_packed(isw_batch *b, int bps) {
   t.group.assign(b->slots.size(), 0);
   const size_t budget = bps == 2 ? SMEM_TWO : SMEM_ONE;
   const int cap = b->sms * bps;
-  const int cells = b->tile_cells > 0 ? b->tile_cells : (bps == 2 ? 384 : 768);
+  const int cells_b = b->tile_cells > 0 ? b->tile_cells : (bps == 2 ? 384 : 768);
   int kmin = b->tile_k;
   bool any = false;
   for (size_t q = 0; q < b->slots.size(); q++) {
     const BatchSlot &sl = b->slots[q];
     if (!tiles_form(b, sl)) continue;
+    const isw_batch::LevelLayout lv = level_layout(b, sl);       // the level's own tile size and interval, if set
+    const int cells = lv.mode == 2 && lv.cells > 0 ? lv.cells : cells_b;
+    const int kcap = lv.mode == 2 && lv.k > 0 ? std::min(lv.k, b->tile_k) : b->tile_k;
     const int N = sl.layers->grid->d.N;
     const int Pq = std::min(cap, std::max(1, (N + cells - 1) / cells));
     if (Pq * 16 > N) continue;
-    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1,
+    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, kcap))->host, budget, b->mixed == 1,
                              bps == 2 ? 512 : 1024);
     if (kf == 0) continue;
     t.P[q] = Pq;
@@ -1254,6 +1269,21 @@ int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, in
     b->layout = layout;
     b->tile_cells = tile_cells;
     b->force_bps = blocks_per_sm;
+    b->dirty = true;
+  });
+}
+
+int isw_batch_level_layout(isw_batch *b, int level, int mode, int tile_cells, int tile_k) {
+  return guarded([&] {
+    if (!b) fail(ISW_EINVAL, "batch.level_layout: null handle");
+    if (level < 0 || level > 12) fail(ISW_EINVAL, "batch.level_layout: level outside 0..12");
+    if (mode < 0 || mode > 2) fail(ISW_EINVAL, "batch.level_layout: mode must be 0 (the batch's), 1 (untiled) or 2 (packed)");
+    if (tile_cells != 0 && (tile_cells < 64 || tile_cells > 4096)) fail(ISW_EINVAL, "batch.level_layout: tile_cells outside 64..4096");
+    if (tile_k < 0 || tile_k > K_PROBE) fail(ISW_EINVAL, "batch.level_layout: tile_k outside 0..8");
+    ISW_CUDA(cudaSetDevice(b->device));
+    settle(b);
+    if (mode == 0) b->levels.erase(level);
+    else b->levels[level] = isw_batch::LevelLayout{mode, tile_cells, tile_k};
     b->dirty = true;
   });
 }

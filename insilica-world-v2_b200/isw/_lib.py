@@ -80,6 +80,7 @@ isw_batch_info = _sig('isw_batch_info', I, [P, ctypes.POINTER(I), ctypes.POINTER
                                              ctypes.POINTER(I), ctypes.POINTER(I)])
 isw_batch_pipeline = _sig('isw_batch_pipeline', I, [P, I])
 isw_batch_grid_loop = _sig('isw_batch_grid_loop', I, [P, I])
+isw_batch_level_layout = _sig('isw_batch_level_layout', I, [P, I, I, I, I])
 isw_batch_flush = _sig('isw_batch_flush', I, [P, P])
 isw_batch_status = _sig('isw_batch_status', I, [P, P, I])
 isw_batch_fault_test = _sig('isw_batch_fault_test', I, [P, LL, P])

@@ -53,17 +53,26 @@ class Batch:
 
     LAYOUTS = {'auto': 0, 'shared': 1, 'packed': 2}
 
-    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0, persistent=False):
+    LEVEL_MODES = {'batch': 0, 'untiled': 1, 'packed': 2}
+
+    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0, persistent=False, levels=None):
         """The fast loop in shared-memory tiles exchanging every k <= tile_k sub-steps (the largest that fits), or
         grid-wide passes; layout 'shared' (one cooperative launch, tiles in proportion to each stack's cells), 'packed'
         (tiles of about tile_cells owned cells, stacks packed into launches) or 'auto'; blocks_per_sm 1, 2 or 0 (auto).
         persistent: the grid-wide passes of untiled stacks as one cooperative launch per stage (co-resident blocks meeting
-        at a grid barrier after every pass) instead of two launches per sub-step."""
+        at a grid barrier after every pass) instead of two launches per sub-step. levels: {grid level: (mode, tile_cells,
+        tile_k)} with mode 'untiled' or 'packed' (its own tile size and interval; 0 = the batch's): a layout per level."""
         self._config = dict(tiles=tiles, tile_k=tile_k, layout=layout, tile_cells=tile_cells, blocks_per_sm=blocks_per_sm,
                             persistent=persistent)
+        if levels:
+            self._config['levels'] = {int(k): tuple(v) for k, v in levels.items()}
         _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k), self.LAYOUTS[layout], int(tile_cells),
                                          int(blocks_per_sm)))
         _lib.check(_lib.isw_batch_grid_loop(self._h, 1 if persistent else 0))
+        for lv in set(getattr(self, '_levels', {})) | set((levels or {}).keys()):
+            mode, cells, k = (levels or {}).get(lv, ('batch', 0, 0))
+            _lib.check(_lib.isw_batch_level_layout(self._h, int(lv), self.LEVEL_MODES[mode], int(cells), int(k)))
+        self._levels = dict(levels or {})
 
     @property
     def persistent(self):
@@ -77,11 +86,13 @@ class Batch:
         return dict(stacks=v[0].value, tiles=v[1].value, tile_k=v[2].value, smem=v[3].value, groups=v[4].value,
                     blocks_per_sm=v[5].value, persistent=self.persistent)
 
-    def autotune(self, steps=5, candidates=None, stream=None):
+    def autotune(self, steps=5, candidates=None, stream=None, per_level=True):
         """Choose the fast-loop layout by timing: each candidate configuration (layout, blocks per SM, exchange interval,
-        tile size; or no tiles) runs `steps` batched steps after one warm-up step, timed with CUDA events; the fastest
-        stays configured. Every registered array is restored afterwards, so the stacks' states are as before. Returns
-        (best configuration, {configuration: ms per step})."""
+        tile size; or no tiles; the grid-wide loop persistent or not) runs `steps` batched steps after one warm-up step,
+        timed with CUDA events; then, for a batch of several grid levels (per_level), each level in turn tries its own
+        layout (untiled, or packed with its own tile size and interval) from the best one. The fastest stays configured.
+        Every registered array is restored afterwards, so the stacks' states are as before. Returns (best configuration,
+        {configuration: ms per step})."""
         import torch
         arrays = []
         for keep in self._keep.values():
@@ -96,14 +107,9 @@ class Batch:
                     candidates.append(dict(tiles=True, layout=layout, blocks_per_sm=bps, tile_k=k, tile_cells=c))
         dev = torch.device(f'cuda:{self.device}')
         st = torch.cuda.current_stream(dev) if stream is None else stream
-        times, seen = {}, set()
-        for cand in candidates:
+
+        def timed(cand):
             self.config(**cand)
-            lay = self.info()
-            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'], lay['persistent'])
-            if key in seen:                       # the same layout as an earlier candidate
-                continue
-            seen.add(key)
             self.step(st)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -111,8 +117,41 @@ class Batch:
                 self.step(st)
             e1.record(st)
             torch.cuda.synchronize(dev)
-            times[tuple(sorted(cand.items()))] = e0.elapsed_time(e1) / steps
-        best = dict(min(times, key=times.get))
+            return e0.elapsed_time(e1) / steps
+
+        def key_of(cand):
+            return tuple(sorted((k, tuple(sorted(v.items())) if isinstance(v, dict) else v) for k, v in cand.items()))
+        times, seen, configs = {}, set(), {}
+        for cand in candidates:
+            self.config(**cand)
+            lay = self.info()
+            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'], lay['persistent'])
+            if key in seen:                       # the same layout as an earlier candidate
+                continue
+            seen.add(key)
+            times[key_of(cand)] = timed(cand)
+            configs[key_of(cand)] = cand
+        best = configs[min(times, key=times.get)]
+        levels = sorted({keep[0].dg.host.n for keep in self._keep.values()})
+        if per_level and len(levels) > 1 and (not best.get('tiles', True) or best.get('layout') == 'packed'):
+            # a layout per grid level: from the best batch-wide one, each level in turn tries untiled and packed tile
+            # sizes and intervals with the others held (one pass of coordinate descent), keeping what is faster
+            cur = dict(best, tiles=True, layout='packed')
+            start = 'untiled' if not best.get('tiles', True) else 'batch'
+            cur['levels'] = {lv: (start, 0, 0) for lv in levels}
+            t_cur = times[key_of(best)]
+            for lv in levels:
+                for opt in (('untiled', 0, 0), ('packed', 512, 3), ('packed', 1024, 3), ('packed', 1024, 4),
+                            ('packed', 2048, 4)):
+                    if cur['levels'][lv] == opt:
+                        continue
+                    cand = dict(cur, levels={**cur['levels'], lv: opt})
+                    t = timed(cand)
+                    times[key_of(cand)] = t
+                    if t < t_cur:
+                        cur, t_cur = cand, t
+            if t_cur < times[key_of(best)]:
+                best = cur
         self.config(**best)
         for a, b in zip(arrays, saved):
             a.copy_(b)

@@ -120,6 +120,41 @@ def test_batch_mixed_levels_equal_alone(dev, grid4):
             assert torch.equal(x, y)
 
 
+@pytest.mark.parametrize('levels', [{3: ('untiled', 0, 0), 4: ('packed', 256, 3)}, {3: ('packed', 128, 2), 4: ('untiled', 0, 0)}])
+def test_batch_layout_per_level_equals_alone(dev, grid4, levels):
+    """A layout per grid level in one batch (one level's stacks in packed tiles of their own size and interval, the
+    other's grid-wide): each member equals its own run alone, bit for bit, and still does under the configuration the
+    autotuner (with its per-level pass) leaves."""
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg4 = DeviceGrid(planet_grid(grid4))
+    dg3 = DeviceGrid(planet_grid(G.build(3, device='cpu')))
+    batch = Batch(0)
+    mixed = [Member(dg3, 5, nfast=20, batch=batch), Member(dg4, 6, nfast=20, batch=batch)]
+    alone = [Member(dg3, 5, nfast=20), Member(dg4, 6, nfast=20)]
+    batch.config(tiles=True, layout='packed', levels=levels)
+    info = batch.info()
+    assert info['tiles'] > 0 and info['groups'] >= 1
+    for _ in range(4):
+        batch.step()
+        for m in alone:
+            m.step()
+    torch.cuda.synchronize()
+    for mb, ma in zip(mixed, alone):
+        for x, y in zip(mb.state(), ma.state()):
+            assert torch.equal(x, y)
+    best, times = batch.autotune(steps=1)
+    batch.step()
+    for m in alone:
+        m.step()
+    torch.cuda.synchronize()
+    for mb, ma in zip(mixed, alone):
+        for x, y in zip(mb.state(), ma.state()):
+            assert torch.equal(x, y)
+
+
 def test_barrier_timeout_refuses_then_recovers(dev, grid4):
     """A block that never arrives at a grid barrier: the others' bounded waits run out and the host reads ISW_ETIMEOUT.
     While the status is set the batch refuses to step (ISW_ETIMEOUT, nothing launched), so a caller that never polls
