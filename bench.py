@@ -198,6 +198,13 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def member_status(m):
+    """The failure status of the batch a member steps through (0 when none, or when it steps call by call)."""
+    if m is None or getattr(m, 'batch', None) is None:
+        return 0
+    return m.batch.status()
+
+
 def max_over_ranks(x, dist, device):
     """The largest of every rank's x (a time: the job runs at its slowest rank's pace); x itself without a process
     group. Every rank takes this collective at the same point."""
@@ -297,7 +304,7 @@ def ensemble_result(steps, warmup, autotune_steps=3):
         e1.record(st)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    finite = all(bool(torch.isfinite(a).all()) for m in ens for a in m.state())
+    finite = all(bool(torch.isfinite(a).all()) for m in ens for a in m.state()) and ens.batch.status() == 0
     value = ens.member_days_per_step() / (ms / 1e3)
     launches = ens.members[0].launches() * steps
     footprint = ens.footprint()
@@ -532,10 +539,14 @@ def main():
             batched[form] = dict(value=world * ens.member_days_per_step() / (t_b / 1e3), unit='member-days/s',
                                  ms_per_step=t_b, layout=ens.batch.info(), autotuned=tuned,
                                  autotune_ms={str(dict(k)): round(v, 4) for k, v in sorted(tried.items(), key=lambda x: x[1])[:6]},
-                                 finite=all(bool(torch.isfinite(a).all()) for m_ in ens for a in m_.state()))
+                                 finite=all(bool(torch.isfinite(a).all()) for m_ in ens for a in m_.state()),
+                                 status=ens.batch.status())
             del ens
 
     finite = all(bool(torch.isfinite(a).all()) for a in member.state())
+    status = [st for st in (member_status(member), member_status(mixed)) if st]   # a failed step voids the line
+    if status:
+        raise RuntimeError(f'bench: a timed step reported failure status {status}')
     dt = member.dt
     value = job_value(world, dt, ms)
     if batched is not None:
