@@ -37,47 +37,50 @@ __device__ __forceinline__ void air_stiff_cell(const LayersDev &M, const double 
   }
 }
 
+// Stage A for air, cells: the layers' mass-mean Exner function pibar (from the pressures at each layer's top and
+// bottom), the Montgomery potential summed up from the ground with each interface's theta jump, the stiffness potential
+// summed down from the top with the mass above, and the kinetic energy of the cell's edges.
 template <int L>
 __device__ __forceinline__ void air_bern_cell(const LayersDev &M, const double *__restrict__ h, const double *__restrict__ u,
                                               const double *__restrict__ theta, int i) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
-  double xb[L];
-  double p = 0, xt = 0;
+  double exner_bot[L];                       // (p / p0)^kappa at each layer's bottom
+  double pbot = 0, exner_top = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
-    const double hk = h[(size_t)k * N + i];
-    const double pt = p;
-    p = p + M.grav * hk;
-    const double x = pow(p / M.p0, M.kap);
-    xb[k] = x;
-    M.pibar[(size_t)k * N + i] = M.cpa * (p * x - pt * xt) / ((M.kap + 1) * (p - pt));
-    xt = x;
+    const double mass = h[(size_t)k * N + i];
+    const double ptop = pbot;
+    pbot = pbot + M.grav * mass;
+    const double xk = pow(pbot / M.p0, M.kap);
+    exner_bot[k] = xk;
+    M.pibar[(size_t)k * N + i] = M.cpa * (pbot * xk - ptop * exner_top) / ((M.kap + 1) * (pbot - ptop));
+    exner_top = xk;
   }
-  double Mv = M.grav * M.b[i] + theta[(size_t)(L - 1) * N + i] * M.cpa * xb[L - 1];
-  double Mk[L];
-  Mk[L - 1] = Mv;
+  double mont = M.grav * M.b[i] + theta[(size_t)(L - 1) * N + i] * M.cpa * exner_bot[L - 1];
+  double mont_k[L];
+  mont_k[L - 1] = mont;
 #pragma unroll
   for (int k = L - 2; k >= 0; k--) {
-    Mv = Mv + (theta[(size_t)k * N + i] - theta[(size_t)(k + 1) * N + i]) * M.cpa * xb[k];
-    Mk[k] = Mv;
+    mont = mont + (theta[(size_t)k * N + i] - theta[(size_t)(k + 1) * N + i]) * M.cpa * exner_bot[k];
+    mont_k[k] = mont;
   }
-  double P[L], Phi[L];
-  double a = 0;
+  double load[L], stiff_pot[L];             // mass down to each layer's bottom; the stiffness potential below
+  double above = 0;
 #pragma unroll
-  for (int k = 0; k < L; k++) { a += h[(size_t)k * N + i]; P[k] = a; }
-  double ph = 0;
+  for (int k = 0; k < L; k++) { above += h[(size_t)k * N + i]; load[k] = above; }
+  double pot = 0;
 #pragma unroll
-  for (int k = L - 1; k >= 0; k--) { ph += M.S[(size_t)k * N + i] * P[k]; Phi[k] = ph; }
+  for (int k = L - 1; k >= 0; k--) { pot += M.S[(size_t)k * N + i] * load[k]; stiff_pot[k] = pot; }
   int es[6];
-  double c[6];
+  double kin[6];                             // l_e d_e / 4 of each slot
   slots6(g.cellEdge, i, es);
 #pragma unroll
   for (int t = 0; t < 6; t++) {
     const int e = es[t];
-    c[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
+    kin[t] = e >= 0 ? g.le[e] * g.de[e] * 0.25 : 0.0;
   }
-  const double A = g.areaCell[i];
+  const double area = g.areaCell[i];
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const double *ul = u + (size_t)k * E;
@@ -86,9 +89,9 @@ __device__ __forceinline__ void air_bern_cell(const LayersDev &M, const double *
     for (int t = 0; t < 6; t++)
       if (es[t] >= 0) {
         const double ue = ul[es[t]];
-        ke += c[t] * ue * ue;
+        ke += kin[t] * ue * ue;
       }
-    M.B[(size_t)k * N + i] = Mk[k] - Phi[k] + ke / A;
+    M.B[(size_t)k * N + i] = mont_k[k] - stiff_pot[k] + ke / area;
   }
 }
 
@@ -111,41 +114,43 @@ __device__ __forceinline__ void air_fast_init_edge(const LayersDev &M, const dou
   }
 }
 
+// A fast sub-step, cells: every layer's mass moved by its sub-step flux, then the forward-weighted fast potential
+// summed down from the top: the stiffness times the damped mass load above each layer's bottom.
 template <int L>
 __device__ __forceinline__ void af_muphi_cell(const LayersDev &M, double tau, int i) {
   const GridDev &g = M.g;
   const int N = g.N, E = g.E;
   int es[6];
-  double c[6];
+  double flux_coef[6];                       // sign l_e of each slot
   slots6(g.cellEdge, i, es);
   int sg[6];
   signs6(g.cellSign, i, sg);
 #pragma unroll
   for (int s = 0; s < 6; s++) {
     const int e = es[s];
-    c[s] = e >= 0 ? (double)sg[s] * g.le[e] : 0.0;
+    flux_coef[s] = e >= 0 ? (double)sg[s] * g.le[e] : 0.0;
   }
-  const double A = g.areaCell[i];
-  double P[L];
-  double a = 0;
+  const double area = g.areaCell[i];
+  double fast_load[L];
+  double above = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) {
     const double *hl = M.hedge + (size_t)k * E;
     const double *ul = M.uf + (size_t)k * E;
     const size_t o = (size_t)k * N + i;
-    const double m0 = M.muf[o];
+    const double mass_old = M.muf[o];
     double div = 0;
 #pragma unroll
     for (int s = 0; s < 6; s++)
-      if (es[s] >= 0) div += c[s] * hl[es[s]] * ul[es[s]];
-    const double m1 = m0 - (tau * div) / A;
-    M.muf[o] = m1;
-    a += m1 + M.div_damp * (m1 - m0);
-    P[k] = a;
+      if (es[s] >= 0) div += flux_coef[s] * hl[es[s]] * ul[es[s]];
+    const double mass_new = mass_old - (tau * div) / area;
+    M.muf[o] = mass_new;
+    above += mass_new + M.div_damp * (mass_new - mass_old);
+    fast_load[k] = above;
   }
-  double ph = 0;
+  double pot = 0;
 #pragma unroll
-  for (int k = L - 1; k >= 0; k--) { ph += M.S[(size_t)k * N + i] * P[k]; M.phi[(size_t)k * N + i] = ph; }
+  for (int k = L - 1; k >= 0; k--) { pot += M.S[(size_t)k * N + i] * fast_load[k]; M.phi[(size_t)k * N + i] = pot; }
 }
 
 template <int L>

@@ -6,7 +6,8 @@ current CUDA stream. Air layers (``air=dict(cp=, kappa=, rd=)``: h is mass per a
 the layers' potential temperature theta, updated in place by the interfacial stress's heating) run in the FP64 form.
 The option branches of Boussinesq layers are built in the FP64 form: thin walls (``wall``), the shelf and its bed flags
 (``shelf``, ``shelf_bed``), and the per-step fields the ocean and the tides set as attributes (``sig`` with ``zm``,
-``tide``, ``cd_bot``, ``cbot``). Air layers or options in the mixed form raise ``NotImplementedError``.
+``tide``, ``cd_bot``, ``cbot``). Air layers, walls and the shelf asked of the mixed form step in the FP64 form (the
+object's ``precision`` says which form it runs).
 """
 import ctypes
 import math
@@ -38,8 +39,10 @@ class Layers:
         if precision not in (None, 'double', 'mixed'):
             raise ValueError(f'Layers: precision {precision!r}, want double or mixed')
         mixed = dg.mixed if precision is None else precision == 'mixed'
-        if (wall is not None or shelf or shelf_bed) and mixed:
-            raise NotImplementedError('Layers: walls and the shelf run in the FP64 form only')
+        if mixed and (air or wall is not None or shelf or shelf_bed):
+            # air layers, walls and the shelf step in the FP64 form on a grid of either form (the reference's mixed
+            # build keeps its air kernels in FP64 too); this object reports precision ISW_FP64
+            mixed = False
         assert wall is None or not air, 'walls are for Boussinesq layers'
         assert 1 <= layers <= LMAX and len(gprime) == layers - 1
         if not isinstance(dg, DeviceGrid):
@@ -51,8 +54,6 @@ class Layers:
         self.air = air
         # the air's constants (reference layers.py:64-65: cp 1004.6, kappa, R 287.04 unless the air dict gives them)
         self.cpa, self.kap, self.rda = (air or {}).get('cp', CP_DRY), (air or {}).get('kappa', KAPPA), (air or {}).get('rd', R_DRY)
-        if air and mixed:
-            raise NotImplementedError('Layers: air layers run in the FP64 form only')
         self.shelf = float(shelf)
         self._wall = None if wall is None else np.ascontiguousarray(np.asarray(
             wall.detach().cpu().numpy() if isinstance(wall, torch.Tensor) else wall, dtype=np.float64).reshape(-1))

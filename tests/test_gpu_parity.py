@@ -224,17 +224,30 @@ def test_repeat_runs_identical(dev, isw, grid4):
         assert torch.equal(x, y)
 
 
-def test_unsupported_options_refused(dev, isw, grid4):
-    """The option branches and air layers run in the FP64 form; in the mixed form they are refused at construction."""
+def test_fp64_branches_on_a_mixed_grid(dev, isw, grid4):
+    """Walls, the shelf and air layers asked of the mixed form step in the FP64 form (as the reference's mixed build
+    keeps its air kernels in FP64): the object reports it, and its steps equal the FP64 grid's bit for bit."""
+    from isw._lib import ISW_FP64
     gpu, layers, _ = isw
     gpu.set_precision('mixed')
     try:
         dgm = gpu.DeviceGrid(grid4)
     finally:
         gpu.set_precision('double')
-    for kw in (dict(wall=np.ones(dgm.E)), dict(shelf=50.0), dict(air={'cp': 1004.6})):
-        with pytest.raises(NotImplementedError):
-            layers.Layers(dgm, 2, gprime=[0.0], **kw)
+    dgd = gpu.DeviceGrid(grid4)
+    z = golden('outcrop_n4')
+    for kw in (dict(wall=np.ones(dgm.E)), dict(shelf=50.0)):
+        cores = [layers.Layers(dg, 2, b=z['b'], gprime=[0.02], stress=[0.0, 2.5e-4], nu4=float(z['nu4']), floor=1.0, **kw)
+                 for dg in (dgm, dgd)]
+        assert cores[0].precision == ISW_FP64
+        states = [(T(z['h0'], dev), T(z['u0'], dev)) for _ in cores]
+        for core, (h, u) in zip(cores, states):
+            for _ in range(3):
+                core.step(h, u, float(z['dt']), int(z['nfast']))
+        torch.cuda.synchronize()
+        assert torch.equal(states[0][0], states[1][0]) and torch.equal(states[0][1], states[1][1])
+    air = layers.Layers(dgm, 2, gprime=[0.0], air={'cp': 1004.6})
+    assert air.precision == ISW_FP64
 
 
 def test_bad_arguments_rejected(dev, isw, grid4):
