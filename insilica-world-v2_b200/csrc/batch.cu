@@ -462,6 +462,19 @@ const std::vector<int32_t> &partition_for(isw_batch *b, const isw_grid *g, int P
   return b->parts[key] = partition_cells(g->d.N, g->h_nbr.data(), P);
 }
 
+TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k);
+int fitting_k(const TileSetHost &h, size_t budget, bool mixed, int threads);
+
+// The largest exchange interval a tiling of g into P tiles fits in the budget, or 0 when no tiling can be built (a
+// region too large or too scattered for the tiles' 16-bit local ids): the planners then leave the stack untiled.
+int fitting_k_or_none(isw_batch *b, const isw_grid *g, int P, int kcap, size_t budget, int threads) {
+  try {
+    return fitting_k(tiles_for(b, g, P, std::min(K_PROBE, kcap))->host, budget, b->mixed == 1, threads);
+  } catch (const Error &) {
+    return 0;
+  }
+}
+
 TileCache *tiles_for(isw_batch *b, const isw_grid *g, int P, int k) {
   auto key = std::make_tuple(g, P, k);
   auto it = b->tiles.find(key);
@@ -583,8 +596,7 @@ Tiling plan_shared(isw_batch *b, int bps) {
     const int N = sl.layers->grid->d.N;
     const int Pq = std::max(1, (int)((long long)slots * N / std::max(1LL, cells_total)));
     if (Pq * 16 > N) return Tiling{};          // tiles of at least 16 owned cells, for every stack
-    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, b->tile_k))->host, budget, b->mixed == 1,
-                             bps == 2 ? 512 : 1024);
+    const int kf = fitting_k_or_none(b, sl.layers->grid, Pq, b->tile_k, budget, bps == 2 ? 512 : 1024);
     if (kf == 0) return Tiling{};
     t.P[q] = Pq;
     kmin = std::min(kmin, kf);
@@ -615,8 +627,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
     const int N = sl.layers->grid->d.N;
     const int Pq = std::min(cap, std::max(1, (N + cells - 1) / cells));
     if (Pq * 16 > N) continue;
-    const int kf = fitting_k(tiles_for(b, sl.layers->grid, Pq, std::min(K_PROBE, kcap))->host, budget, b->mixed == 1,
-                             bps == 2 ? 512 : 1024);
+    const int kf = fitting_k_or_none(b, sl.layers->grid, Pq, kcap, budget, bps == 2 ? 512 : 1024);
     if (kf == 0) continue;
     t.P[q] = Pq;
     t.K[q] = kf;                               // each stack its own interval: a group's rounds follow its slowest
