@@ -440,3 +440,29 @@ def test_air_stack_in_batch_equals_per_call(dev, grid4, persistent):
         assert torch.equal(x, y)
     with pytest.raises(ValueError):
         batch.add(air['core'], air['h'], air['u'], air['Fm'], dt=dt, nfast=nfast)        # air layers need theta
+
+
+def test_autotune_two_level6_members(dev):
+    """The autotuner's candidates include tilings that cannot be built for two level-6 members (a region too large for
+    the tiles' 16-bit local ids); the planner leaves such stacks untiled instead of failing, and the tuned batch steps
+    the members to the same state as untuned ones."""
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    dg = DeviceGrid(planet_grid(G.build(6, device=0)))
+    batch = Batch(0)
+    tuned = [Member(dg, s, nfast=20, batch=batch) for s in (1, 2)]
+    plain = Batch(0)
+    plain.config(tiles=False)
+    ref = [Member(dg, s, nfast=20, batch=plain) for s in (1, 2)]
+    best, times = batch.autotune(steps=1)
+    assert len(times) > 2
+    for _ in range(2):
+        batch.step()
+        plain.step()
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    for a, b in zip(tuned, ref):
+        for x, y in zip(a.state(), b.state()):
+            assert torch.equal(x, y)
