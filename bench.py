@@ -400,8 +400,8 @@ def run_profile(args):
 
 def run_accuracy(args):
     """The mixed form against the plain FP64 form (error norms and mass drifts; no timing): the member over 10 model
-    days at levels 6 (config 2), 5 and 7 (the levels of the ensemble and serving configs), the level-7 Galewsky jet
-    over 6 model days (config 3) and Williamson 2 over 5 days at level 4 (config 1)."""
+    days at levels 6 (the benchmark member), 5 and 7 (the levels of the ensemble and serving workloads), the level-7
+    Galewsky jet over 6 model days and Williamson 2 over 5 days at level 4."""
     from isw import accuracy
     out = dict(metric='mixed-form accuracy against the FP64 form', impl='isw', data='synthetic',
                member=accuracy.member(6, args.days_member), galewsky=accuracy.galewsky(7, args.days_galewsky),

@@ -107,7 +107,7 @@ def main():
         return
     save('grid_n4.npz', {k: getattr(base, k) for k in GRID_KEYS})
 
-    # ---- config 1: Williamson 2, one layer ----
+    # ---- Williamson 2, one layer ----
     h0, b, u0 = rcases.initial_state(g, 'w2')
     core = Layers(dg, 1, b=b)
     h, u = cp.asarray(h0[None]), cp.asarray(u0[None])

@@ -88,7 +88,7 @@ def test_member_ten_days_at_ensemble_levels(dev, level):
 
 
 def test_level7_galewsky_six_days(dev):
-    """Config 3: the Galewsky jet at level 7 over the full 6 model days (9216 steps of 56.25 s), mixed form against the
+    """The Galewsky jet at level 7 over the full 6 model days (9216 steps of 56.25 s), mixed form against the
     FP64 form (reference tests/test_accuracy.py:51-55 vertex vorticity, :111-128 Galewsky): relative L2 and Linf of h
     <= 1e-5, of vertex vorticity <= 1e-3 (the jet's vorticity is small-scale where the instability rolls up), and mass
     drift <= 1e-13 in both forms. The norms are printed (pytest -s)."""

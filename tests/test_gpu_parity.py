@@ -39,7 +39,7 @@ def rel(a, b):
 
 
 def test_w2_bit_exact(dev, isw, grid4):
-    """Config 1 (Williamson 2, n = 4, dt 900 s, nfast from the reference's rule): 1, 96 and 480 steps bit for bit."""
+    """Williamson 2 (n = 4, dt 900 s, nfast from the reference's rule): 1, 96 and 480 steps bit for bit."""
     from isw import grid as G
     gpu, layers, _ = isw
     z = golden('w2_n4')
@@ -449,6 +449,33 @@ def test_exchange_bit_exact(dev, isw, grid4):
     for name, x, w in zip('h u M psi'.split(), got, want):
         assert np.array_equal(x.cpu().numpy(), w), ('air', name, rel(x.cpu().numpy(), w))
     assert rel(got[4].cpu().numpy(), want[4]) <= 1e-14
+
+
+def test_exchange_golden_after_batched_step(dev, isw, grid4):
+    """The exchange hook on layers that step in a batch (the ocean's between-step moves, ocean.py:159 and :245): after
+    one batched step, exchange equals the reference's golden vectors to 1e-12 (the step's stress calls exp)."""
+    from isw import grid as G
+    from isw.batch import Batch
+    gpu, layers, _ = isw
+    z = golden('exchange_n4')
+    dg = gpu.DeviceGrid(G.for_planet(grid4, 6.371e6, 7.292e-5, 9.80616))
+    A = T(dg.host.areaCell, dev)
+    core = layers.Layers(dg, 3, b=z['b_b'], gprime=list(z['b_gprime']), stress=list(z['b_stress']), nu4=float(z['b_nu4']),
+                         floor=float(z['b_floor']), vmix=float(z['b_vmix']))
+    h0, u0 = T(z['b_h0'], dev), T(z['b_u0'], dev)
+    batch = Batch(0)
+    batch.add(core, h0, u0, torch.zeros_like(u0), dt=float(z['b_dt']), nfast=20)
+    batch.step()
+    torch.cuda.synchronize()
+    for tag, seq in (('plain', False), ('seq', True)):
+        h, u = h0.clone(), u0.clone()
+        M = (h * A[None]).contiguous()
+        psi = T(z['b_psi0'], dev)
+        core.exchange(T(z['b_wx'], dev), h, u, M, psi, seq=seq)
+        torch.cuda.synchronize()
+        for name, x in (('h', h), ('u', u), ('M', M), ('psi', psi)):
+            e = rel(x.cpu().numpy(), z[f'b_{tag}_{name}'])
+            assert e <= REL, (tag, name, e)
 
 
 def test_option_branches_golden(dev, isw, grid4):

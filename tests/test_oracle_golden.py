@@ -21,7 +21,7 @@ def _grid(grid4, omega=None):
 
 @pytest.mark.parametrize('backend', BACKENDS)
 def test_w2_bit_exact(oracle_lib, grid4, backend):
-    """Config 1 (Williamson 2, n = 4, dt 900 s): 1, 96, 480 steps equal the reference's bit for bit; energy too."""
+    """Williamson 2 (n = 4, dt 900 s): 1, 96, 480 steps equal the reference's bit for bit; energy too."""
     M = oracle_lib
     z = golden('w2_n4')
     dg = M.OracleGrid(_grid(grid4, float(z['omega'])))
