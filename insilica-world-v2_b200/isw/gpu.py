@@ -6,6 +6,7 @@ shape, contiguity and device are read, and the C library works on the caller's m
 """
 import ctypes
 import os
+import weakref
 
 import numpy as np
 import torch
@@ -120,6 +121,31 @@ class DeviceGrid:
         if h is not None and h.value and destroy is not None:      # (module globals are gone at interpreter exit)
             destroy(h)
             self._h = None
+
+
+_FOREIGN = weakref.WeakKeyDictionary()
+
+
+def as_device_grid(dg):
+    """This core's DeviceGrid for `dg`: dg itself, or, for another device grid that carries the host Grid as `.host`
+    (the reference's own DeviceGrid, whose `kernel()` the rest of the model keeps using to build its other kernels),
+    an isw DeviceGrid built from that Grid once and cached with it, in the form its `mixed` attribute asks."""
+    if isinstance(dg, DeviceGrid):
+        return dg
+    host = getattr(dg, 'host', None)
+    if host is None:
+        raise TypeError('expected an isw DeviceGrid or a device grid carrying its host Grid as .host')
+    mine = _FOREIGN.get(dg)
+    if mine is None:
+        global PRECISION
+        prev = PRECISION
+        PRECISION = 'mixed' if getattr(dg, 'mixed', False) else 'double'
+        try:
+            mine = DeviceGrid(host)
+        finally:
+            PRECISION = prev
+        _FOREIGN[dg] = mine
+    return mine
 
 
 def dsum(x, y=None, stream=None):

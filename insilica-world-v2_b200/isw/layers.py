@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .gpu import DeviceGrid, device_ptr, dsum, stream_of
+from .gpu import as_device_grid, device_ptr, dsum, stream_of
 
 LMAX = 8
 FAST_COURANT = 0.5          # fast sub-step: tau sqrt(gH) / d_min <= this (reference layers.py:31)
@@ -38,6 +38,7 @@ class Layers:
         (the precision switch in force when the DeviceGrid was made)."""
         if precision not in (None, 'double', 'mixed'):
             raise ValueError(f'Layers: precision {precision!r}, want double or mixed')
+        dg = as_device_grid(dg)         # the reference's own DeviceGrid is accepted too (its host Grid is used)
         mixed = dg.mixed if precision is None else precision == 'mixed'
         if mixed and (air or wall is not None or shelf or shelf_bed):
             # air layers, walls and the shelf step in the FP64 form on a grid of either form (the reference's mixed
@@ -45,8 +46,6 @@ class Layers:
             mixed = False
         assert wall is None or not air, 'walls are for Boussinesq layers'
         assert 1 <= layers <= LMAX and len(gprime) == layers - 1
-        if not isinstance(dg, DeviceGrid):
-            raise TypeError('Layers: dg must be an isw DeviceGrid')
         self.dg, self.L = dg, layers
         self.grav, self.nu4, self.floor, self.div_damp, self.thin = grav, nu4, floor, div_damp, thin
         self.vmix, self.vmix_cd = vmix, vmix_cd

@@ -7,7 +7,7 @@ layered: psi, M0, M1 (L, N); Fm (L, E). Every tracer goes through the same launc
 import ctypes
 
 from . import _lib
-from .gpu import DeviceGrid, device_ptr, stream_of
+from .gpu import as_device_grid, device_ptr, stream_of
 
 BETA = 0.25         # upwind weight of the 3rd-order flux (reference transport.py:15)
 
@@ -16,10 +16,9 @@ class Transport:
     def __init__(self, dg, layers=1, beta=BETA, tracers=1, precision=None):
         """The reference's constructor (transport.py:19). precision (this core's): 'double' or 'mixed' for this object
         (the form of the batched FCT passes); None takes the grid's form."""
-        if not isinstance(dg, DeviceGrid):
-            raise TypeError('Transport: dg must be an isw DeviceGrid')
         if precision not in (None, 'double', 'mixed'):
             raise ValueError(f'Transport: precision {precision!r}, want double or mixed')
+        dg = as_device_grid(dg)         # the reference's own DeviceGrid is accepted too (its host Grid is used)
         self.dg, self.L, self.beta, self.K = dg, layers, beta, tracers
         h = ctypes.c_void_p()
         mixed = dg.mixed if precision is None else precision == 'mixed'

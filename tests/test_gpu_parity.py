@@ -146,6 +146,26 @@ def test_dsum_bit_exact(dev, isw):
         assert gpu.dsum(T(x, dev), T(y, dev)) == float(z[f'xy_{n}'])
 
 
+def test_reference_device_grid_accepted(dev, isw, grid4):
+    """Layers and Transport built on the reference's own DeviceGrid (an object carrying the host Grid as .host, its
+    precision as .mixed, and the kernel() the rest of the model compiles its other kernels with) use an isw grid made
+    from that Grid once, and step exactly as on an isw DeviceGrid."""
+    import types
+    from isw import grid as G
+    gpu, layers, transport = isw
+    z = golden('w2_n4')
+    g = G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616)
+    ref_dg = types.SimpleNamespace(host=g, mixed=False, kernel=lambda *a, **k: None)
+    a, b = layers.Layers(ref_dg, 1, b=z['b']), layers.Layers(gpu.DeviceGrid(g), 1, b=z['b'])
+    assert a.dg is gpu.as_device_grid(ref_dg) and transport.Transport(ref_dg).dg is a.dg
+    states = [(T(z['h0'], dev), T(z['u0'], dev)) for _ in range(2)]
+    for core, (h, u) in zip((a, b), states):
+        for _ in range(5):
+            core.step(h, u, float(z['dt']), int(z['nfast']))
+    torch.cuda.synchronize()
+    assert torch.equal(states[0][0], states[1][0]) and torch.equal(states[0][1], states[1][1])
+
+
 def test_graph_capture_equals_direct(dev, isw, grid4):
     """A step queued inside the caller's own CUDA-graph capture and replayed equals direct steps, bit for bit
     (reference REPRO: graph vs direct)."""
