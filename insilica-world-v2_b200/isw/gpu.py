@@ -135,7 +135,10 @@ def as_device_grid(dg):
     host = getattr(dg, 'host', None)
     if host is None:
         raise TypeError('expected an isw DeviceGrid or a device grid carrying its host Grid as .host')
-    mine = _FOREIGN.get(dg)
+    try:
+        mine = _FOREIGN.get(dg)
+    except TypeError:                         # an object without weak references: keep the grid on it
+        mine = getattr(dg, '_isw_device_grid', None)
     if mine is None:
         global PRECISION
         prev = PRECISION
@@ -144,7 +147,10 @@ def as_device_grid(dg):
             mine = DeviceGrid(host)
         finally:
             PRECISION = prev
-        _FOREIGN[dg] = mine
+        try:
+            _FOREIGN[dg] = mine
+        except TypeError:
+            setattr(dg, '_isw_device_grid', mine)
     return mine
 
 

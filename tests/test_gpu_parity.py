@@ -150,12 +150,18 @@ def test_reference_device_grid_accepted(dev, isw, grid4):
     """Layers and Transport built on the reference's own DeviceGrid (an object carrying the host Grid as .host, its
     precision as .mixed, and the kernel() the rest of the model compiles its other kernels with) use an isw grid made
     from that Grid once, and step exactly as on an isw DeviceGrid."""
-    import types
     from isw import grid as G
     gpu, layers, transport = isw
     z = golden('w2_n4')
     g = G.for_planet(grid4, 6.371e6, float(z['omega']), 9.80616)
-    ref_dg = types.SimpleNamespace(host=g, mixed=False, kernel=lambda *a, **k: None)
+
+    class ReferenceDeviceGrid:                # the attributes the reference's DeviceGrid carries that isw reads
+        def __init__(self, grid):
+            self.host, self.mixed = grid, False
+
+        def kernel(self, name, file, defs=()):
+            raise AssertionError('isw compiles nothing through the caller grid')
+    ref_dg = ReferenceDeviceGrid(g)
     a, b = layers.Layers(ref_dg, 1, b=z['b']), layers.Layers(gpu.DeviceGrid(g), 1, b=z['b'])
     assert a.dg is gpu.as_device_grid(ref_dg) and transport.Transport(ref_dg).dg is a.dg
     states = [(T(z['h0'], dev), T(z['u0'], dev)) for _ in range(2)]
