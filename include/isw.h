@@ -215,11 +215,13 @@ int isw_batch_step(isw_batch *b, void *stream);
  * 64..4096, 0 = by blocks per SM; stacks packed into cooperative launches of at most SMs x blocks-per-SM tiles).
  * blocks_per_sm: 0 choose, 1 (1024-thread tiles) or 2 (512-thread tiles). */
 int isw_batch_config(isw_batch *b, int tiles_enabled, int tile_k, int layout, int tile_cells, int blocks_per_sm);
-/* The grid-wide sub-steps of the untiled stacks (persistent != 0): one cooperative launch per stage and precision form
- * whose co-resident blocks run every sub-step, meeting at a bounded grid barrier after each cell pass and each edge pass,
- * instead of two kernel launches per sub-step (0, the default). Results are bit-identical either way. This core's own
- * layout choice: no counterpart in the reference (whose Layers.step launches two kernels per sub-step, layers.py:168-175). */
-int isw_batch_grid_loop(isw_batch *b, int persistent);
+/* How the untiled stacks run their grid-wide sub-steps. ISW_GRID_SPLIT (the default): two kernel launches per
+ * sub-step, a cell pass and an edge pass. ISW_GRID_PERSISTENT: one cooperative launch per stage and precision form whose
+ * co-resident blocks run every sub-step, meeting at a bounded grid barrier after each cell pass and each edge pass.
+ * Results are bit-identical either way. This core's own layout choice: no counterpart in the reference (whose
+ * Layers.step launches two kernels per sub-step, layers.py:168-175). */
+enum { ISW_GRID_SPLIT = 0, ISW_GRID_PERSISTENT = 1 };
+int isw_batch_grid_loop(isw_batch *b, int mode);
 /* The fast-loop layout of the stacks on grids of one level (an ensemble or a serving mix holds several): mode 0 follows
  * the batch's configuration (the default), 1 keeps them untiled (grid-wide sub-steps), 2 tiles them in the packed layout
  * with about tile_cells owned cells per tile (0: the batch's) and an exchange interval of at most tile_k (0: the

@@ -43,20 +43,46 @@ namespace {
 // EXT: the kernel also carries the air branch and the option branches (walls, the shelf and its bed flags, per-cell
 // buoyancy, the tide, the bottom's drag), instantiated only for batches holding such stacks, so that the plain
 // Boussinesq phases keep their register count.
+// The grid-wide sub-step passes over a wide chunk: PH_ETA's cells, PH_U's / PH_UF's edges (PH_UF also forming the
+// layer fluxes on the stack's last sub-step); air stacks and sub-step 0's cell pass (which also forms the slot
+// coefficients) item by item.
+template <int PH, int LMAXK, bool EXT>
+__device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j, const Chunk &ch) {
+  if (d.tiled || j >= d.n[st]) return;
+  const LayersDev &M = d.M;
+  const double tau = d.tau[st];
+  const int first = ch.begin + (int)threadIdx.x;
+  if (EXT && M.air) {
+    for (int i = first; i < ch.end; i += THREADS) {
+      if (PH == PH_ETA) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, tau, i));
+      else ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(M, tau, i));
+    }
+  } else if (PH == PH_ETA) {
+    if (j == 0)
+      for (int i = first; i < ch.end; i += THREADS) fp64::bt_eta_cell_y(M, tau, 0, i);
+    else
+      fp64::bt_eta_cells_y<SUB_WC_FP64>(M, tau, first, ch.end);
+  } else {
+    fp64::bt_u_edges_y<SUB_W_FP64, EXT>(M, tau, first, ch.end);
+    if (PH == PH_UF && j == d.n[st] - 1) {
+      const StageArgs a = stage_args(d, st);
+      for (int i = first; i < ch.end; i += THREADS) fp64::flux_edge<EXT>(M, a, M.acc[i], i);
+    }
+  }
+}
+
 template <int PH, int LMAXK, bool EXT>
 __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
-  int b = blockIdx.x;
-  int kind = -1;
   Chunk ch{0, 0, 0};
-  if (Dom<PH>::cell) { if (b < sc.ncell) { kind = 0; ch = sc.cell[b]; } else b -= sc.ncell; }
-  if (kind < 0 && Dom<PH>::edge) { if (b < sc.nedge) { kind = 1; ch = sc.edge[b]; } else b -= sc.nedge; }
-  if (kind < 0 && Dom<PH>::vert) { if (b < sc.nvert) { kind = 2; ch = sc.vert[b]; } else b -= sc.nvert; }
-  if (kind < 0 && Dom<PH>::rows) { if (b < sc.nrows) { kind = 3; ch = sc.rows[b]; } else b -= sc.nrows; }
-  if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
+  const int kind = phase_chunk<PH>(sc, blockIdx.x, ch);
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
   pdl_wait();
   pdl_trigger();
+  if (Dom<PH>::wide) {                       // the grid-wide sub-step passes: a wide chunk, SUB_W items a thread
+    substep_chunk<PH, LMAXK, EXT>(d, st, j, ch);
+    return;
+  }
   const int i = ch.begin + (int)threadIdx.x;
   if (PH == PH_S && d.s_stage) {             // the block stages its rows' distinct neighbour records, then computes
     extern __shared__ __align__(16) double stg[];
@@ -106,20 +132,6 @@ __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__
   } else if (PH == PH_S) {
     const StageArgs a = stage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, fp64::slow_edge<LL, EXT>(M, a.us, a.cdt, i, EXT && M.air ? d.theta : nullptr));
-  } else if (PH == PH_ETA) {
-    if (!d.tiled && j < d.n[st]) {
-      if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::af_muphi_cell<LL>(M, d.tau[st], i));
-      else fp64::bt_eta_cell_y(M, d.tau[st], j, i);
-    }
-  } else if (PH == PH_U || PH == PH_UF) {
-    if (!d.tiled && j < d.n[st]) {
-      if (EXT && M.air) {
-        ISW_BATCH_L(d.L, LMAXK, fp64::af_u_edge<LL>(M, d.tau[st], i));
-      } else {
-        fp64::bt_u_edge_y<EXT>(M, d.tau[st], i);
-        if (PH == PH_UF && j == d.n[st] - 1) fp64::flux_edge<EXT>(M, stage_args(d, st), M.acc[i], i);
-      }
-    }
   } else if (PH == PH_C || PH == PH_CS) {
     const StageArgs a = stage_args(d, st);
     if (EXT && M.air) ISW_BATCH_L(d.L, LMAXK, fp64::air_scale_cell<LL>(M, a, i));
@@ -649,6 +661,7 @@ Tiling plan_packed(isw_batch *b, int bps) {
 void rebuild(isw_batch *b) {
   std::vector<StackDesc> desc;
   std::vector<Chunk> cell[2], edge[2], vert[2], rows[2], erows[2];      // per form: [0] FP64 stacks, [1] mixed
+  std::vector<Chunk> wcell[2], wedge[2];                                // the sub-step passes' wide chunks
   int nsub[3] = {0, 0, 0};
   b->mixed = 0;
   for (auto &sl : b->slots)
@@ -729,14 +742,18 @@ void rebuild(isw_batch *b) {
       d.s_stage = form_of(sl) == 1 && need <= S_STAGE_MAX ? 1 : 0;
       if (d.s_stage) s_smem[form_of(sl)] = std::max(s_smem[form_of(sl)], need);
     }
-    auto chunks = [&](std::vector<Chunk> &v, int n) {
-      for (int i = 0; i < n; i += THREADS) v.push_back(Chunk{s, i, std::min(n, i + THREADS)});
+    auto chunks = [&](std::vector<Chunk> &v, int n, int w = THREADS) {
+      for (int i = 0; i < n; i += w) v.push_back(Chunk{s, i, std::min(n, i + w)});
     };
     const int f = form_of(sl);
     if (!d.tiled) untiled[f] = 1;
     chunks(cell[f], d.M.g.N);
     chunks(edge[f], d.M.g.E);
     chunks(vert[f], d.M.g.NV);
+    if (!d.tiled) {
+      chunks(wcell[f], d.M.g.N, (f == 0 ? SUB_WC_FP64 : SUB_W) * THREADS);
+      chunks(wedge[f], d.M.g.E, (f == 0 ? SUB_W_FP64 : SUB_W) * THREADS);
+    }
     if (d.has_tr) chunks(rows[f], sl.ntr * d.M.g.N);       // (tracer, cell) pairs
     if (d.has_tr) chunks(erows[f], sl.ntr * d.M.g.E);      // (tracer, edge) pairs
     desc.push_back(d);
@@ -776,6 +793,8 @@ void rebuild(isw_batch *b) {
     all.insert(all.end(), vert[f].begin(), vert[f].end());
     all.insert(all.end(), rows[f].begin(), rows[f].end());
     all.insert(all.end(), erows[f].begin(), erows[f].end());
+    all.insert(all.end(), wcell[f].begin(), wcell[f].end());
+    all.insert(all.end(), wedge[f].begin(), wedge[f].end());
   }
   ISW_CUDA(cudaMalloc(&b->d_desc, sizeof(StackDesc) * desc.size()));
   ISW_CUDA(cudaMalloc(&b->d_chunks, sizeof(Chunk) * all.size()));
@@ -843,7 +862,11 @@ void rebuild(isw_batch *b) {
     sc.nrows = (int)rows[f].size();
     sc.erows = sc.rows + sc.nrows;
     sc.nerows = (int)erows[f].size();
-    base = sc.erows + sc.nerows;
+    sc.wcell = sc.erows + sc.nerows;
+    sc.nwcell = (int)wcell[f].size();
+    sc.wedge = sc.wcell + sc.nwcell;
+    sc.nwedge = (int)wedge[f].size();
+    base = sc.wedge + sc.nwedge;
   }
   b->ntiles = (int)refs.size();
   size_t smax = 0;
@@ -887,8 +910,7 @@ void launch_phase(isw_batch *b, cudaStream_t st, int stage, int j, bool pdl = tr
   bool first = true;
   for (int f = 0; f < 2; f++) {
     const Sched &sc = b->scf[f];
-    const int nb = (Dom<PH>::cell ? sc.ncell : 0) + (Dom<PH>::edge ? sc.nedge : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
-                   (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
+    const int nb = phase_blocks<PH>(sc);
     if (nb == 0) continue;
     if (!b->cur) fail(ISW_EINVAL, "batch: no stack descriptors selected for the launch");
     const bool p = (first ? pdl : true) && b->pdl;
@@ -1299,12 +1321,13 @@ int isw_batch_level_layout(isw_batch *b, int level, int mode, int tile_cells, in
   });
 }
 
-int isw_batch_grid_loop(isw_batch *b, int persistent) {
+int isw_batch_grid_loop(isw_batch *b, int mode) {
   return guarded([&] {
     if (!b) fail(ISW_EINVAL, "batch.grid_loop: null handle");
     ISW_CUDA(cudaSetDevice(b->device));
     settle(b);
-    b->fast_grid = persistent != 0;
+    if (mode != ISW_GRID_SPLIT && mode != ISW_GRID_PERSISTENT) fail(ISW_EINVAL, "batch.grid_loop: mode must be 0 or 1");
+    b->fast_grid = mode == ISW_GRID_PERSISTENT;
     b->dirty = true;
   });
 }

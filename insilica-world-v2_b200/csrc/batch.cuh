@@ -64,6 +64,8 @@ __device__ __forceinline__ void raise_status(BatchStatus *s, int code) {
 struct Sched {
   const Chunk *cell, *edge, *vert, *rows, *erows;   // rows: (tracer, cell) pairs; erows: (tracer, edge) pairs
   int ncell, nedge, nvert, nrows, nerows;
+  const Chunk *wcell, *wedge;                       // the same in the sub-step passes' chunks (SUB_W... x THREADS)
+  int nwcell, nwedge;
   BatchStatus *status;
 };
 
@@ -203,7 +205,35 @@ struct Dom {
   static constexpr bool vert = PH == PH_INIT || PH == PH_LAPCV || PH == PH_A;
   static constexpr bool rows = PH == PH_P1 || PH == PH_P2 || PH == PH_P3 || PH == PH_P4;
   static constexpr bool erows = PH == PH_POST || PH == PH_P2E || PH == PH_P3E || PH == PH_HF1;
+  static constexpr bool wide = PH == PH_ETA || PH == PH_U || PH == PH_UF;   // cells / edges in the wide chunks
 };
+
+// Blocks of a phase over a schedule.
+template <int PH>
+inline int phase_blocks(const Sched &sc) {
+  return (Dom<PH>::cell ? (Dom<PH>::wide ? sc.nwcell : sc.ncell) : 0) +
+         (Dom<PH>::edge ? (Dom<PH>::wide ? sc.nwedge : sc.nedge) : 0) + (Dom<PH>::vert ? sc.nvert : 0) +
+         (Dom<PH>::rows ? sc.nrows : 0) + (Dom<PH>::erows ? sc.nerows : 0);
+}
+
+// The chunk of block b of a phase and its kind (0 cell, 1 edge, 2 vertex, 3 (tracer, cell), 4 (tracer, edge)), or -1.
+template <int PH>
+__device__ __forceinline__ int phase_chunk(const Sched &sc, int b, Chunk &ch) {
+  if (Dom<PH>::cell) {
+    const int n = Dom<PH>::wide ? sc.nwcell : sc.ncell;
+    if (b < n) { ch = (Dom<PH>::wide ? sc.wcell : sc.cell)[b]; return 0; }
+    b -= n;
+  }
+  if (Dom<PH>::edge) {
+    const int n = Dom<PH>::wide ? sc.nwedge : sc.nedge;
+    if (b < n) { ch = (Dom<PH>::wide ? sc.wedge : sc.edge)[b]; return 1; }
+    b -= n;
+  }
+  if (Dom<PH>::vert) { if (b < sc.nvert) { ch = sc.vert[b]; return 2; } b -= sc.nvert; }
+  if (Dom<PH>::rows) { if (b < sc.nrows) { ch = sc.rows[b]; return 3; } b -= sc.nrows; }
+  if (Dom<PH>::erows) { if (b < sc.nerows) { ch = sc.erows[b]; return 4; } }
+  return -1;
+}
 
 
 constexpr size_t S_STAGE_MAX = 64 * 1024;   // the slow tendency's staged neighbour records: at most this per block

@@ -9,6 +9,8 @@ namespace isw {
 namespace bt {
 namespace {
 
+constexpr int SUB_ETA_W = 2;        // cells a thread holds at once in the wide sub-step cell pass
+
 __device__ __forceinline__ mixed::MStageArgs mstage_args(const StackDesc &d, int st) {
   const LayersDev &M = d.M;
   mixed::MStageArgs a;
@@ -29,20 +31,40 @@ __device__ __forceinline__ mixed::MStageArgs mstage_args(const StackDesc &d, int
   return a;
 }
 
+// The grid-wide sub-step passes over a wide chunk: PH_ETA's cells (sub-step 0 item by item, as it also forms the slot
+// coefficients), PH_U's / PH_UF's edges (PH_UF also forming the layer fluxes on the stack's last sub-step).
+template <int PH>
+__device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j, const Chunk &ch) {
+  if (d.tiled || j >= d.n[st]) return;
+  const LayersDev &M = d.M;
+  const float tau = (float)d.tau[st];
+  const int first = ch.begin + (int)threadIdx.x;
+  if (PH == PH_ETA) {
+    if (j == 0)
+      for (int i = first; i < ch.end; i += THREADS) mixed::bt_eta_cell(M, tau, 0, i);
+    else
+      mixed::bt_eta_cells<SUB_ETA_W>(M, tau, first, ch.end);
+  } else {
+    mixed::bt_u_edges(M, tau, first, ch.end);
+    if (PH == PH_UF && j == d.n[st] - 1) {
+      const mixed::MStageArgs a = mstage_args(d, st);
+      for (int i = first; i < ch.end; i += THREADS) mixed::flux_edge(M, a, M.acc[i], i);
+    }
+  }
+}
+
 template <int PH, int LMAXK>
 __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
-  int b = blockIdx.x;
-  int kind = -1;
   Chunk ch{0, 0, 0};
-  if (Dom<PH>::cell) { if (b < sc.ncell) { kind = 0; ch = sc.cell[b]; } else b -= sc.ncell; }
-  if (kind < 0 && Dom<PH>::edge) { if (b < sc.nedge) { kind = 1; ch = sc.edge[b]; } else b -= sc.nedge; }
-  if (kind < 0 && Dom<PH>::vert) { if (b < sc.nvert) { kind = 2; ch = sc.vert[b]; } else b -= sc.nvert; }
-  if (kind < 0 && Dom<PH>::rows) { if (b < sc.nrows) { kind = 3; ch = sc.rows[b]; } else b -= sc.nrows; }
-  if (kind < 0 && Dom<PH>::erows) { if (b < sc.nerows) { kind = 4; ch = sc.erows[b]; } else b -= sc.nerows; }
+  const int kind = phase_chunk<PH>(sc, blockIdx.x, ch);
   if (kind < 0) return;
   const StackDesc &d = stage_desc(S, ch.s);
   pdl_wait();
   pdl_trigger();
+  if (Dom<PH>::wide) {                       // the grid-wide sub-step passes: a wide chunk, SUB_W items a thread
+    substep_chunk<PH>(d, st, j, ch);
+    return;
+  }
   const int i = ch.begin + (int)threadIdx.x;
   if (PH == PH_S && d.s_stage) {             // the block stages its rows' distinct neighbour records, then computes
     extern __shared__ __align__(16) float4 stg4[];
@@ -80,13 +102,6 @@ __global__ void __launch_bounds__(THREADS) k_phase_m(const StackDesc *__restrict
   } else if (PH == PH_S) {
     const mixed::MStageArgs a = mstage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, mixed::slow_edge<LL>(M, a.us, a.cdt, i));
-  } else if (PH == PH_ETA) {
-    if (!d.tiled && j < d.n[st]) mixed::bt_eta_cell(M, (float)d.tau[st], j, i);
-  } else if (PH == PH_U || PH == PH_UF) {
-    if (!d.tiled && j < d.n[st]) {
-      mixed::bt_u_edge(M, (float)d.tau[st], i);
-      if (PH == PH_UF && j == d.n[st] - 1) mixed::flux_edge(M, mstage_args(d, st), M.acc[i], i);
-    }
   } else if (PH == PH_C) {
     const mixed::MStageArgs a = mstage_args(d, st);
     ISW_BATCH_L(d.L, LMAXK, mixed::scale_cell<LL>(M, a, i));

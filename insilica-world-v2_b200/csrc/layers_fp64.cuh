@@ -462,6 +462,110 @@ __device__ __forceinline__ void bt_u_edge_y(const LayersDev &M, double tau, int 
   }
 }
 
+// ---- The split sub-step passes over a wide chunk (W items a thread, THREADS apart; mixed::bt_u_edges' scheme): the
+// plain loads of all the thread's items, then their gathers, then the arithmetic and stores of bt_u_edge_y /
+// bt_eta_cell_y (the latter for sub-steps j >= 1). ----
+template <int W, bool OPT>
+__device__ __forceinline__ void bt_u_edges_y(const LayersDev &M, double tau, int first, int end) {
+  const int *__restrict__ eI = M.g.eI;
+  const int *__restrict__ eJ = M.g.eJ;
+  const double *__restrict__ de = M.g.de;
+  const double *__restrict__ G = M.G;
+  const double *__restrict__ Y = M.eta_prev;
+  double *__restrict__ ub = M.ub;
+  double *__restrict__ acc = M.acc;
+  for (int base = first; base < end; base += W * THREADS) {
+    double v[W], aq[W], gq[W], dq[W], ya[W], yb[W];
+    int ia[W], ib[W];
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int e = base + q * THREADS;
+      v[q] = aq[q] = gq[q] = 0.0;
+      dq[q] = 1.0;
+      ia[q] = ib[q] = 0;
+      if (e < end) {
+        v[q] = ub[e];
+        aq[q] = acc[e];
+        gq[q] = G[e];
+        dq[q] = de[e];
+        ia[q] = eI[e];
+        ib[q] = eJ[e];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      ya[q] = yb[q] = 0.0;
+      if (base + q * THREADS < end) {
+        ya[q] = Y[ia[q]];
+        yb[q] = Y[ib[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int e = base + q * THREADS;
+      if (e < end) {
+        const bool w = walled<OPT>(M, e);
+        acc[e] = w ? 0.0 : aq[q] + v[q];
+        ub[e] = w ? 0.0 : v[q] + tau * ((-(yb[q] - ya[q])) / dq[q] + gq[q]);
+      }
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void bt_eta_cells_y(const LayersDev &M, double tau, int first, int end) {
+  const int *__restrict__ cellEdge = M.g.cellEdge;
+  const double *__restrict__ cwt = M.cw;
+  const double *__restrict__ area = M.g.areaCell;
+  const double *__restrict__ Gc = M.Gc;
+  const double *__restrict__ ub = M.ub;
+  double *__restrict__ eta = M.eta;
+  double *__restrict__ Y = M.eta_prev;
+  const double gam = M.div_damp;
+  for (int base = first; base < end; base += W * THREADS) {
+    int es[W][6];
+    double c[W][6], u[W][6], e0[W], ar[W], gc[W];
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int i = base + q * THREADS;
+      e0[q] = gc[q] = 0.0;
+      ar[q] = 1.0;
+#pragma unroll
+      for (int s = 0; s < 6; s++) { es[q][s] = -1; c[q][s] = 0.0; }
+      if (i < end) {
+        slots6(cellEdge, i, es[q]);
+        const double2 *cw = reinterpret_cast<const double2 *>(cwt + (size_t)i * 6);
+#pragma unroll
+        for (int h = 0; h < 3; h++) {
+          const double2 x = cw[h];
+          c[q][2 * h] = x.x;
+          c[q][2 * h + 1] = x.y;
+        }
+        e0[q] = eta[i];
+        ar[q] = area[i];
+        gc[q] = Gc[i];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < W; q++)
+#pragma unroll
+      for (int s = 0; s < 6; s++) u[q][s] = es[q][s] >= 0 ? ub[es[q][s]] : 0.0;
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int i = base + q * THREADS;
+      if (i < end) {
+        double div = 0;
+#pragma unroll
+        for (int s = 0; s < 6; s++)
+          if (es[q][s] >= 0) div += c[q][s] * u[q][s];
+        const double en = e0[q] - (tau * div) / ar[q];
+        eta[i] = en;
+        Y[i] = gc[q] * (en + gam * (en - e0[q]));
+      }
+    }
+  }
+}
+
 // The layer fluxes of edge e once the stage's fast loop has finished (reference lay_flux, layers.cu:392-397), every
 // layer: F = h_e (u - ubar_s) + h_e acc / n, acc the sub-steps' sum of ubar. A batch with no tiled stack forms them in
 // the last grid-wide sub-step's edge pass, once per edge, and its phase C only sums them (scale_sum_cell); batches

@@ -270,6 +270,19 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
   M.ubs32[e] = U / H;
 }
 
+// The grid-wide fast loop's per-item roundings, written out (explicit fused multiply-adds) so that every form of the
+// loop that uses them (item by item, over wide chunks, the persistent loop) gives the same bits: an edge's new dub, a
+// cell's new deta and its Y = Gc (deta + gamma (deta - deta_prev)).
+__device__ __forceinline__ float bt_u_new(float v, float tau, float G, float yi, float yj, float rde) {
+  return __fmaf_rn(tau, __fmaf_rn(-__fsub_rn(yj, yi), rde, G), v);
+}
+__device__ __forceinline__ float bt_eta_new(float d0, float tau, float div, float rA) {
+  return __fmaf_rn(-__fmul_rn(tau, div), rA, d0);
+}
+__device__ __forceinline__ float bt_y_new(float gc, float gam, float dn, float d0) {
+  return __fmul_rn(gc, __fmaf_rn(gam, __fsub_rn(dn, d0), dn));
+}
+
 // ---- fast loop, grid-wide form (stacks without tiles): deviation variables; the cell pass stores Y = Gc (deta +
 // gamma (deta - deta_prev)) in deprev for the edge pass ----
 __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int i) {
@@ -304,10 +317,10 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
   float div = c0;
 #pragma unroll
   for (int s = 0; s < 6; s++)
-    if (es[s] >= 0) div += c[s] * M.dub[es[s]];
-  const float dn = d0 - tau * div * g.rA32[i];
+    if (es[s] >= 0) div = __fmaf_rn(c[s], M.dub[es[s]], div);
+  const float dn = bt_eta_new(d0, tau, div, g.rA32[i]);
   M.deta[i] = dn;
-  M.deprev[i] = M.Gc32[i] * (dn + (float)M.div_damp * (dn - d0));   // Y, what the edge pass reads
+  M.deprev[i] = bt_y_new(M.Gc32[i], (float)M.div_damp, dn, d0);   // Y, what the edge pass reads
 }
 
 __device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) {
@@ -315,7 +328,110 @@ __device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) 
   const float v = M.dub[e];
   M.acc[e] += (double)v;
   const float *Y = M.deprev;
-  M.dub[e] = v + tau * (M.G32[e] - (Y[g.eJ[e]] - Y[g.eI[e]]) * g.rde32[e]);
+  M.dub[e] = bt_u_new(v, tau, M.G32[e], Y[g.eI[e]], Y[g.eJ[e]], g.rde32[e]);
+}
+
+// ---- The split sub-step passes over a wide chunk (up to SUB_W items a thread, THREADS apart): each thread issues the
+// plain loads of all its items, then their gathers, then computes and stores, so a thread keeps SUB_W items' loads in
+// flight and reads the stack's pointers once for all of them. Per item the arithmetic of bt_u_edge / bt_eta_cell. ----
+__device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int first, int end) {
+  const int *__restrict__ eI = M.g.eI;
+  const int *__restrict__ eJ = M.g.eJ;
+  const float *__restrict__ rde = M.g.rde32;
+  const float *__restrict__ G = M.G32;
+  const float *__restrict__ Y = M.deprev;
+  float *__restrict__ dub = M.dub;
+  double *__restrict__ acc = M.acc;
+  float v[SUB_W], gq[SUB_W], rq[SUB_W], ya[SUB_W], yb[SUB_W];
+  double aq[SUB_W];
+  int ia[SUB_W], ib[SUB_W];
+#pragma unroll
+  for (int q = 0; q < SUB_W; q++) {
+    const int e = first + q * THREADS;
+    v[q] = gq[q] = rq[q] = 0.f;
+    aq[q] = 0.0;
+    ia[q] = ib[q] = 0;
+    if (e < end) {
+      v[q] = dub[e];
+      aq[q] = acc[e];
+      gq[q] = G[e];
+      rq[q] = rde[e];
+      ia[q] = eI[e];
+      ib[q] = eJ[e];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SUB_W; q++) {
+    ya[q] = yb[q] = 0.f;
+    if (first + q * THREADS < end) {
+      ya[q] = Y[ia[q]];
+      yb[q] = Y[ib[q]];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SUB_W; q++) {
+    const int e = first + q * THREADS;
+    if (e < end) {
+      acc[e] = aq[q] + (double)v[q];
+      dub[e] = bt_u_new(v[q], tau, gq[q], ya[q], yb[q], rq[q]);
+    }
+  }
+}
+
+// sub-steps j >= 1 of the cell pass (the slot coefficients and c0 formed by sub-step 0)
+template <int W>
+__device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int first, int end) {
+  const int *__restrict__ cellEdge = M.g.cellEdge;
+  const float *__restrict__ cw32 = M.cw32;
+  const float *__restrict__ c0 = M.c0;
+  const float *__restrict__ rA = M.g.rA32;
+  const float *__restrict__ Gc = M.Gc32;
+  const float *__restrict__ dub = M.dub;
+  float *__restrict__ deta = M.deta;
+  float *__restrict__ Y = M.deprev;
+  const float gam = (float)M.div_damp;
+  for (int base = first; base < end; base += W * THREADS) {
+    int es[W][6];
+    float c[W][6], u[W][6], cz[W], d0[W], ra[W], gc[W];
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int i = base + q * THREADS;
+      cz[q] = d0[q] = ra[q] = gc[q] = 0.f;
+#pragma unroll
+      for (int s = 0; s < 6; s++) { es[q][s] = -1; c[q][s] = 0.f; }
+      if (i < end) {
+        slots6(cellEdge, i, es[q]);
+        const float2 *cw = reinterpret_cast<const float2 *>(cw32 + (size_t)i * 6);
+#pragma unroll
+        for (int h = 0; h < 3; h++) {
+          const float2 x = cw[h];
+          c[q][2 * h] = x.x;
+          c[q][2 * h + 1] = x.y;
+        }
+        cz[q] = c0[i];
+        d0[q] = deta[i];
+        ra[q] = rA[i];
+        gc[q] = Gc[i];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < W; q++)
+#pragma unroll
+      for (int s = 0; s < 6; s++) u[q][s] = es[q][s] >= 0 ? dub[es[q][s]] : 0.f;
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int i = base + q * THREADS;
+      if (i < end) {
+        float div = cz[q];
+#pragma unroll
+        for (int s = 0; s < 6; s++)
+          if (es[q][s] >= 0) div = __fmaf_rn(c[q][s], u[q][s], div);
+        const float dn = bt_eta_new(d0[q], tau, div, ra[q]);
+        deta[i] = dn;
+        Y[i] = bt_y_new(gc[q], gam, dn, d0[q]);
+      }
+    }
+  }
 }
 
 // The layer fluxes of edge e in the last grid-wide sub-step of a batch with no tiled stack, every layer: F (FP64,

@@ -55,41 +55,56 @@ class Batch:
 
     LEVEL_MODES = {'batch': 0, 'untiled': 1, 'packed': 2}
 
-    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0, persistent=False, levels=None):
+    GRID_MODES = {'split': 0, 'persistent': 1}
+
+    def config(self, tiles=True, tile_k=8, layout='auto', tile_cells=0, blocks_per_sm=0, persistent=False, levels=None,
+               grid=None):
         """The fast loop in shared-memory tiles exchanging every k <= tile_k sub-steps (the largest that fits), or
         grid-wide passes; layout 'shared' (one cooperative launch, tiles in proportion to each stack's cells), 'packed'
         (tiles of about tile_cells owned cells, stacks packed into launches) or 'auto'; blocks_per_sm 1, 2 or 0 (auto).
-        persistent: the grid-wide passes of untiled stacks as one cooperative launch per stage (co-resident blocks meeting
-        at a grid barrier after every pass) instead of two launches per sub-step. levels: {grid level: (mode, tile_cells,
-        tile_k)} with mode 'untiled' or 'packed' (its own tile size and interval; 0 = the batch's): a layout per level."""
+        grid: how untiled stacks run their grid-wide sub-steps: 'split' (a cell launch and an edge launch per sub-step)
+        or 'persistent' (one cooperative launch per stage, co-resident blocks meeting at a grid barrier after every pass);
+        persistent=True is grid='persistent'. Results are the same bits either way.
+        levels: {grid level: (mode, tile_cells, tile_k)} with mode 'untiled' or 'packed' (its own tile size and
+        interval; 0 = the batch's): a layout per level."""
+        if grid is None:
+            grid = 'persistent' if persistent else 'split'
+        if grid not in self.GRID_MODES:
+            raise ValueError(f'batch.config: grid must be one of {sorted(self.GRID_MODES)}')
         self._config = dict(tiles=tiles, tile_k=tile_k, layout=layout, tile_cells=tile_cells, blocks_per_sm=blocks_per_sm,
-                            persistent=persistent)
+                            grid=grid)
         if levels:
             self._config['levels'] = {int(k): tuple(v) for k, v in levels.items()}
         _lib.check(_lib.isw_batch_config(self._h, 1 if tiles else 0, int(tile_k), self.LAYOUTS[layout], int(tile_cells),
                                          int(blocks_per_sm)))
-        _lib.check(_lib.isw_batch_grid_loop(self._h, 1 if persistent else 0))
+        _lib.check(_lib.isw_batch_grid_loop(self._h, self.GRID_MODES[grid]))
         for lv in set(getattr(self, '_levels', {})) | set((levels or {}).keys()):
             mode, cells, k = (levels or {}).get(lv, ('batch', 0, 0))
             _lib.check(_lib.isw_batch_level_layout(self._h, int(lv), self.LEVEL_MODES[mode], int(cells), int(k)))
         self._levels = dict(levels or {})
 
     @property
+    def grid(self):
+        """How untiled stacks run their grid-wide sub-steps: 'split' or 'persistent'."""
+        return getattr(self, '_config', {}).get('grid', 'split')
+
+    @property
     def persistent(self):
-        return bool(getattr(self, '_config', {}).get('persistent', False))
+        return self.grid == 'persistent'
 
     def info(self):
         """The current layout: stacks, tiles, exchange interval k, the largest tile's shared memory (bytes), cooperative
-        launches per stage (groups), tile blocks per SM, and whether untiled stacks run the persistent grid-wide loop."""
+        launches per stage (groups), tile blocks per SM, and how untiled stacks run their grid-wide sub-steps (grid;
+        persistent: whether that is the persistent loop)."""
         v = [ctypes.c_int() for _ in range(3)] + [ctypes.c_longlong()] + [ctypes.c_int() for _ in range(2)]
         _lib.check(_lib.isw_batch_info(self._h, *[ctypes.byref(x) for x in v]))
         return dict(stacks=v[0].value, tiles=v[1].value, tile_k=v[2].value, smem=v[3].value, groups=v[4].value,
-                    blocks_per_sm=v[5].value, persistent=self.persistent)
+                    blocks_per_sm=v[5].value, grid=self.grid, persistent=self.persistent)
 
     def autotune(self, steps=5, candidates=None, stream=None, per_level=True):
         """Choose the fast-loop layout by timing: each candidate configuration (layout, blocks per SM, exchange interval,
-        tile size; or no tiles; the grid-wide loop persistent or not) runs `steps` batched steps after one warm-up step,
-        timed with CUDA events; then, for a batch of several grid levels (per_level), each level in turn tries its own
+        tile size; or no tiles, with the grid-wide sub-steps split or persistent) runs `steps` batched steps after
+        one warm-up step, timed with CUDA events; then, for a batch of several grid levels (per_level), each level in turn tries its own
         layout (untiled, or packed with its own tile size and interval) from the best one. The fastest stays configured.
         Every registered array is restored afterwards, so the stacks' states are as before. Returns (best configuration,
         {configuration: ms per step})."""
@@ -100,7 +115,7 @@ class Batch:
             arrays += [a for a in (h, u, Fm, M, M1) + tuple(tracers) if a is not None]
         saved = [a.clone() for a in arrays]
         if candidates is None:
-            candidates = [dict(tiles=False), dict(tiles=False, persistent=True)]
+            candidates = [dict(tiles=False, grid=g) for g in ('split', 'persistent')]
             for layout, bps, k in itertools.product(('shared', 'packed'), (1, 2), (2, 3, 4, 6, 8)):
                 cells = (0,) if layout == 'shared' else ((256, 512) if bps == 2 else (512, 1024))
                 for c in cells:
@@ -125,7 +140,7 @@ class Batch:
         for cand in candidates:
             self.config(**cand)
             lay = self.info()
-            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'], lay['persistent'])
+            key = (lay['tiles'], lay['tile_k'], lay['groups'], lay['blocks_per_sm'], lay['smem'], lay['grid'])
             if key in seen:                       # the same layout as an earlier candidate
                 continue
             seen.add(key)

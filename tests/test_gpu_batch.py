@@ -257,6 +257,46 @@ def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
         assert torch.equal(x, y) and torch.equal(x, z)
 
 
+@pytest.mark.parametrize('precision', ['double', 'mixed'])
+def test_grid_wide_forms_equal(dev, grid4, precision):
+    """The grid-wide sub-steps as two launches each (over wide chunks, several items a thread) give the persistent
+    loop's result (item by item) bit for bit: members of different sub-step counts in one batch (nfast 20 and 7), and a
+    grid-wide level beside a tiled one (the layer fluxes then formed in phase C)."""
+    from isw import gpu
+    from isw import grid as G
+    from isw.batch import Batch
+    from isw.gpu import DeviceGrid
+    from isw.workload import Member, planet_grid
+    gpu.set_precision(precision)
+    try:
+        dg4 = DeviceGrid(planet_grid(grid4))
+        dg3 = DeviceGrid(planet_grid(G.build(3, device='cpu')))
+        uneven, beside = {}, {}
+        for grid in ('split', 'persistent'):
+            bt = Batch(0)
+            bt.config(tiles=False, grid=grid)
+            uneven[grid] = (bt, [Member(dg4, 30, nfast=20, ntracers=2, batch=bt, fp64_kinds=()),
+                                 Member(dg4, 31, nfast=7, ntracers=2, batch=bt, fp64_kinds=())])
+            bt = Batch(0)
+            bt.config(tiles=True, layout='packed', grid=grid, levels={3: ('packed', 128, 2), 4: ('untiled', 0, 0)})
+            beside[grid] = (bt, [Member(dg3, 5, nfast=20, ntracers=2, batch=bt, fp64_kinds=()),
+                                 Member(dg4, 6, nfast=20, ntracers=2, batch=bt, fp64_kinds=())])
+    finally:
+        gpu.set_precision('double')
+    assert uneven['persistent'][0].info()['grid'] == 'persistent' and beside['split'][0].info()['tiles'] > 0
+    for _ in range(3):
+        for bt, _m in list(uneven.values()) + list(beside.values()):
+            bt.step()
+    torch.cuda.synchronize()
+    for group in (uneven, beside):
+        ref = group['split'][1]
+        for grid, (bt, ms) in group.items():
+            assert bt.status() == 0, grid
+            for a, b in zip(ms, ref):
+                for x, y in zip(a.state(), b.state()):
+                    assert torch.equal(x, y), grid
+
+
 def test_batch_of_both_forms(dev, grid4):
     """One batch holding FP64 and mixed stacks (each phase one kernel per form, the mixed stacks' fast loop in tiles, the
     FP64 stacks' as grid-wide sub-steps): every FP64 stack equals the same stack in an FP64-only batch bit for bit, and
@@ -402,8 +442,8 @@ def _air_world(dg, z, dev, batched_core=True):
     return st
 
 
-@pytest.mark.parametrize('persistent', [False, True])
-def test_air_stack_in_batch_equals_per_call(dev, grid4, persistent):
+@pytest.mark.parametrize('grid', ['split', 'persistent'])
+def test_air_stack_in_batch_equals_per_call(dev, grid4, grid):
     """Air layers registered in a batch (isw_batch_add_air) beside a Boussinesq stack: 12 batched steps equal 12 ticks
     of Layers.step(theta=) + mass_after + step_many([psi, theta]) + M <- M1 call by call, bit for bit (h, u, M, Fm,
     the tracer and theta), with the grid-wide sub-steps as two launches each or as one persistent launch per stage;
@@ -425,7 +465,7 @@ def test_air_stack_in_batch_equals_per_call(dev, grid4, persistent):
     air = _air_world(dg, za, dev)
     bous = make_stack(dg, zb, dev)
     batch = Batch(0)
-    batch.config(tiles=False, persistent=persistent)
+    batch.config(tiles=False, grid=grid)
     batch.add(air['core'], air['h'], air['u'], air['Fm'], tr=air['tr'], M=air['M'], M1=air['M1'], tracers=air['trc'],
               dt=dt, nfast=nfast, theta=air['theta'])
     batch.add(bous['core'], bous['h'], bous['u'], bous['Fm'], tr=bous['tr'], M=bous['M'], M1=bous['M1'],

@@ -508,7 +508,7 @@ def test_option_branches_golden(dev, isw, grid4):
     """Every option branch of Boussinesq layers at once on the reference's outcrop case (walls, the shelf with its bed
     flags, per-cell buoyancy, a tide potential, the bottom's quadratic and internal-tide drag), set as the reference's
     callers set them: h, u, Fm after 1 and 12 steps to 1e-12 of the reference's (its stress term calls exp), call by
-    call and through a batch (beside a plain stack, with two launches per sub-step and with the persistent loop), the
+    call and through a batch (beside a plain stack, with the grid-wide sub-steps split and persistent), the
     batched run equal to the call-by-call one bit for bit."""
     gpu, layers, _ = isw
     from isw.batch import Batch
@@ -538,18 +538,18 @@ def test_option_branches_golden(dev, isw, grid4):
                 e = rel(x.cpu().numpy(), z[name + sfx])
                 assert e <= REL, (s, name, e)
     w2 = golden('w2_n4')
-    for persistent in (False, True):
+    for grid in ('split', 'persistent'):
         bcore = options_core()
         hb, ub = T(z['h0'], dev), T(z['u0'], dev)
         Fb = torch.zeros_like(ub)
         plain = layers.Layers(dg, 1, b=w2['b'])
         hp, up = T(w2['h0'], dev), T(w2['u0'], dev)
         batch = Batch(0)
-        batch.config(persistent=persistent)
+        batch.config(grid=grid)
         batch.add(bcore, hb, ub, Fb, dt=dt, nfast=nfast)
         batch.add(plain, hp, up, torch.zeros_like(up), dt=float(w2['dt']), nfast=int(w2['nfast']))
         for _ in range(12):
             batch.step()
         torch.cuda.synchronize()
         assert batch.status() == 0
-        assert torch.equal(hb, h) and torch.equal(ub, u) and torch.equal(Fb, Fm), persistent
+        assert torch.equal(hb, h) and torch.equal(ub, u) and torch.equal(Fb, Fm), grid
