@@ -41,11 +41,11 @@ __device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j,
   const int first = ch.begin + (int)threadIdx.x;
   if (PH == PH_ETA) {
     if (j == 0)
-      for (int i = first; i < ch.end; i += THREADS) mixed::bt_eta_cell(M, tau, 0, i);
+      for (int i = first; i < ch.end; i += THREADS) mixed::bt_eta_cell(M, tau, 0, d.n[st], i);
     else
-      mixed::bt_eta_cells<SUB_ETA_W>(M, tau, first, ch.end);
+      mixed::bt_eta_cells<SUB_ETA_W>(M, tau, j, d.n[st], first, ch.end);
   } else {
-    mixed::bt_u_edges(M, tau, first, ch.end);
+    mixed::bt_u_edges(M, tau, j, d.n[st], first, ch.end);
     if (PH == PH_UF && j == d.n[st] - 1) {
       const mixed::MStageArgs a = mstage_args(d, st);
       for (int i = first; i < ch.end; i += THREADS) mixed::flux_edge(M, a, M.acc[i], i);
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid_m(const StackDesc *__rest
       const Chunk ch = sc.cell[c];
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
-      if (i < ch.end && !d.tiled && j < d.n[st]) mixed::bt_eta_cell(d.M, (float)d.tau[st], j, i);
+      if (i < ch.end && !d.tiled && j < d.n[st]) mixed::bt_eta_cell(d.M, (float)d.tau[st], j, d.n[st], i);
     }
     if (!grid_sync(bar, status, timeout_ns, 0)) return;
     for (int c = blockIdx.x; c < sc.nedge; c += gridDim.x) {
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(THREADS) k_fast_grid_m(const StackDesc *__rest
       select(ch.s);
       const int i = ch.begin + (int)threadIdx.x;
       if (i < ch.end && !d.tiled && j < d.n[st]) {
-        mixed::bt_u_edge(d.M, (float)d.tau[st], i);
+        mixed::bt_u_edge(d.M, (float)d.tau[st], j, d.n[st], i);
         if (flux && j == d.n[st] - 1) mixed::flux_edge(d.M, mstage_args(d, st), d.M.acc[i], i);
       }
     }

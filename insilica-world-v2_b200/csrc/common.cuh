@@ -160,6 +160,7 @@ struct LayersDev {
   float *u32, *u1f, *u2f, *D1f, *Z1f, *L1f, *L2f, *q32, *Tp32, *G32, *He32, *ubs32, *Gc32;
   float *c0, *dub, *deta, *deprev, *xeta[2], *xdub[2], *cw32;
   float *F32, *scale32;                      // mixed form: stored layer fluxes (L x E) and limiter factors (L x N)
+  double *wsum;                              // mixed form, grid-wide fast loop: W, the weighted sum of Y (N)
   float4 *pk4;
 };
 

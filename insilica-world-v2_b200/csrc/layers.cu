@@ -435,6 +435,7 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
       d.q32 = f((size_t)L * NV); d.Tp32 = f((size_t)L * E); d.G32 = f(E); d.He32 = f(E); d.ubs32 = f(E);
       d.c0 = f(N); d.dub = f(E); d.deta = f(N); d.deprev = f(N); d.cw32 = f((size_t)N * 6);
       d.F32 = f((size_t)L * E); d.scale32 = f((size_t)L * N);
+      d.wsum = dalloc(s, N);
       d.xeta[0] = f(N); d.xeta[1] = f(N); d.xdub[0] = f(E); d.xdub[1] = f(E);
       d.pk4 = talloc_t<float4>(s, (size_t)L * E);
       std::vector<float> gc32(N, (float)p->grav);

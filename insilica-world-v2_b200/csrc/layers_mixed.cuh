@@ -283,9 +283,24 @@ __device__ __forceinline__ float bt_y_new(float gc, float gam, float dn, float d
   return __fmul_rn(gc, __fmaf_rn(gam, __fsub_rn(dn, d0), dn));
 }
 
+// The sub-steps' sum of dub at an edge without a per-edge running sum. With dub_0 = 0 and dub_{j+1} = dub_j +
+// tau (G - (Y_j[J] - Y_j[I]) / d_e), the sum over j < n of dub_j is
+//     tau (G n (n - 1) / 2 - (W[J] - W[I]) / d_e),   W = sum over j <= n - 2 of (n - 1 - j) Y_j,
+// so the cell pass keeps W per cell in FP64 (bt_w_next: set at sub-step 0, added to through sub-step n - 2) and the
+// last sub-step's edge pass forms the sum from W (bt_acc_of). This replaces a FP64 read and write per edge and sub-step
+// by one per cell and sub-step; each edge's sum still comes from one expression, so both of its cells see the same flux.
+__device__ __forceinline__ void bt_w_next(double *__restrict__ W, int i, float y, int j, int n) {
+  if (j == 0) W[i] = __dmul_rn((double)(n - 1), (double)y);
+  else if (j <= n - 2) W[i] = __fma_rn((double)(n - 1 - j), (double)y, W[i]);
+}
+__device__ __forceinline__ double bt_acc_of(float tau, float G, double wi, double wj, float rde, int n) {
+  const double half = 0.5 * (double)n * (double)(n - 1);
+  return (double)tau * __fma_rn(-__dsub_rn(wj, wi), (double)rde, __dmul_rn((double)G, half));
+}
+
 // ---- fast loop, grid-wide form (stacks without tiles): deviation variables; the cell pass stores Y = Gc (deta +
-// gamma (deta - deta_prev)) in deprev for the edge pass ----
-__device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int i) {
+// gamma (deta - deta_prev)) in deprev for the edge pass, and adds its share to W ----
+__device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int n, int i) {
   const GridDev &g = M.g;
   int es[6];
   float c[6];
@@ -320,40 +335,40 @@ __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j
     if (es[s] >= 0) div = __fmaf_rn(c[s], M.dub[es[s]], div);
   const float dn = bt_eta_new(d0, tau, div, g.rA32[i]);
   M.deta[i] = dn;
-  M.deprev[i] = bt_y_new(M.Gc32[i], (float)M.div_damp, dn, d0);   // Y, what the edge pass reads
+  const float y = bt_y_new(M.Gc32[i], (float)M.div_damp, dn, d0);
+  M.deprev[i] = y;                           // Y, what the edge pass reads
+  bt_w_next(M.wsum, i, y, j, n);
 }
 
-__device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int e) {
+// sub-step j of edge e; on the last one (j = n - 1) also its sum acc, from W
+__device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int j, int n, int e) {
   const GridDev &g = M.g;
   const float v = M.dub[e];
-  M.acc[e] += (double)v;
   const float *Y = M.deprev;
-  M.dub[e] = bt_u_new(v, tau, M.G32[e], Y[g.eI[e]], Y[g.eJ[e]], g.rde32[e]);
+  const int a = g.eI[e], b = g.eJ[e];
+  M.dub[e] = bt_u_new(v, tau, M.G32[e], Y[a], Y[b], g.rde32[e]);
+  if (j == n - 1) M.acc[e] = bt_acc_of(tau, M.G32[e], M.wsum[a], M.wsum[b], g.rde32[e], n);
 }
 
 // ---- The split sub-step passes over a wide chunk (up to SUB_W items a thread, THREADS apart): each thread issues the
 // plain loads of all its items, then their gathers, then computes and stores, so a thread keeps SUB_W items' loads in
 // flight and reads the stack's pointers once for all of them. Per item the arithmetic of bt_u_edge / bt_eta_cell. ----
-__device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int first, int end) {
+__device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int j, int n, int first, int end) {
   const int *__restrict__ eI = M.g.eI;
   const int *__restrict__ eJ = M.g.eJ;
   const float *__restrict__ rde = M.g.rde32;
   const float *__restrict__ G = M.G32;
   const float *__restrict__ Y = M.deprev;
   float *__restrict__ dub = M.dub;
-  double *__restrict__ acc = M.acc;
   float v[SUB_W], gq[SUB_W], rq[SUB_W], ya[SUB_W], yb[SUB_W];
-  double aq[SUB_W];
   int ia[SUB_W], ib[SUB_W];
 #pragma unroll
   for (int q = 0; q < SUB_W; q++) {
     const int e = first + q * THREADS;
     v[q] = gq[q] = rq[q] = 0.f;
-    aq[q] = 0.0;
     ia[q] = ib[q] = 0;
     if (e < end) {
       v[q] = dub[e];
-      aq[q] = acc[e];
       gq[q] = G[e];
       rq[q] = rde[e];
       ia[q] = eI[e];
@@ -371,16 +386,31 @@ __device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int fi
 #pragma unroll
   for (int q = 0; q < SUB_W; q++) {
     const int e = first + q * THREADS;
-    if (e < end) {
-      acc[e] = aq[q] + (double)v[q];
-      dub[e] = bt_u_new(v[q], tau, gq[q], ya[q], yb[q], rq[q]);
+    if (e < end) dub[e] = bt_u_new(v[q], tau, gq[q], ya[q], yb[q], rq[q]);
+  }
+  if (j == n - 1) {
+    const double *__restrict__ W = M.wsum;
+    double *__restrict__ acc = M.acc;
+    double wa[SUB_W], wb[SUB_W];
+#pragma unroll
+    for (int q = 0; q < SUB_W; q++) {
+      wa[q] = wb[q] = 0.0;
+      if (first + q * THREADS < end) {
+        wa[q] = W[ia[q]];
+        wb[q] = W[ib[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < SUB_W; q++) {
+      const int e = first + q * THREADS;
+      if (e < end) acc[e] = bt_acc_of(tau, gq[q], wa[q], wb[q], rq[q], n);
     }
   }
 }
 
 // sub-steps j >= 1 of the cell pass (the slot coefficients and c0 formed by sub-step 0)
 template <int W>
-__device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int first, int end) {
+__device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int j, int n, int first, int end) {
   const int *__restrict__ cellEdge = M.g.cellEdge;
   const float *__restrict__ cw32 = M.cw32;
   const float *__restrict__ c0 = M.c0;
@@ -389,6 +419,7 @@ __device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int 
   const float *__restrict__ dub = M.dub;
   float *__restrict__ deta = M.deta;
   float *__restrict__ Y = M.deprev;
+  double *__restrict__ wsum = M.wsum;
   const float gam = (float)M.div_damp;
   for (int base = first; base < end; base += W * THREADS) {
     int es[W][6];
@@ -428,7 +459,9 @@ __device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int 
           if (es[q][s] >= 0) div = __fmaf_rn(c[q][s], u[q][s], div);
         const float dn = bt_eta_new(d0[q], tau, div, ra[q]);
         deta[i] = dn;
-        Y[i] = bt_y_new(gc[q], gam, dn, d0[q]);
+        const float y = bt_y_new(gc[q], gam, dn, d0[q]);
+        Y[i] = y;
+        bt_w_next(wsum, i, y, j, n);
       }
     }
   }
