@@ -61,7 +61,7 @@ __device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j,
     if (j == 0)
       for (int i = first; i < ch.end; i += THREADS) fp64::bt_eta_cell_y(M, tau, 0, i);
     else
-      fp64::bt_eta_cells_y<SUB_WC_FP64>(M, tau, first, ch.end);
+      fp64::bt_eta_cells_y<SUB_WC>(M, tau, first, ch.end);
   } else {
     fp64::bt_u_edges_y<SUB_W_FP64, EXT>(M, tau, first, ch.end);
     if (PH == PH_UF && j == d.n[st] - 1) {
@@ -751,7 +751,7 @@ void rebuild(isw_batch *b) {
     chunks(edge[f], d.M.g.E);
     chunks(vert[f], d.M.g.NV);
     if (!d.tiled) {
-      chunks(wcell[f], d.M.g.N, (f == 0 ? SUB_WC_FP64 : SUB_W) * THREADS);
+      chunks(wcell[f], d.M.g.N, SUB_WC * THREADS);
       chunks(wedge[f], d.M.g.E, (f == 0 ? SUB_W_FP64 : SUB_W) * THREADS);
     }
     if (d.has_tr) chunks(rows[f], sl.ntr * d.M.g.N);       // (tracer, cell) pairs

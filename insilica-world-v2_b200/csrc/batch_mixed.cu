@@ -9,8 +9,6 @@ namespace isw {
 namespace bt {
 namespace {
 
-constexpr int SUB_ETA_W = 2;        // cells a thread holds at once in the wide sub-step cell pass
-
 __device__ __forceinline__ mixed::MStageArgs mstage_args(const StackDesc &d, int st) {
   const LayersDev &M = d.M;
   mixed::MStageArgs a;
@@ -43,7 +41,7 @@ __device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j,
     if (j == 0)
       for (int i = first; i < ch.end; i += THREADS) mixed::bt_eta_cell(M, tau, 0, d.n[st], i);
     else
-      mixed::bt_eta_cells<SUB_ETA_W>(M, tau, j, d.n[st], first, ch.end);
+      mixed::bt_eta_cells<SUB_WC>(M, tau, j, d.n[st], first, ch.end);
   } else {
     mixed::bt_u_edges(M, tau, j, d.n[st], first, ch.end);
     if (PH == PH_UF && j == d.n[st] - 1) {

@@ -13,11 +13,13 @@ namespace isw {
 constexpr int LMAX = 8;          // layers per column (reference layers.py:30)
 constexpr int TRMAX = 16;        // tracers moved in one transport call
 constexpr int THREADS = 256;     // threads per block of the phase kernels
-// Items per thread of the grid-wide sub-step passes (their chunks hold that many x THREADS): the mixed form's cells and
-// edges, the FP64 form's edges and cells (its cell pass keeps one: two raise it past 100 registers).
+// Items per thread of the grid-wide sub-step passes (their chunks hold that many x THREADS): the mixed form's edges,
+// the FP64 form's edges, and the cells of both (two a thread raised the cell pass to 75 (mixed) and 100 (FP64)
+// registers, and it ran slower at the lower occupancy; FP64 edges ran fastest at two: 8 level-6 members 3.84 ms a
+// step against 4.24 at one).
 constexpr int SUB_W = 4;
 constexpr int SUB_W_FP64 = 2;
-constexpr int SUB_WC_FP64 = 1;
+constexpr int SUB_WC = 1;
 constexpr int EOE_MAX = 10;      // TRiSK row length: the other edges of an edge's two cells (5 + 5 on hexagons)
 // The FP64 packed edge record: per edge, (h_e, u, q_e) of each layer, the edge's row padded to an even count of
 // doubles so that every row starts on a 16-byte boundary and is read as 16-byte pairs.
