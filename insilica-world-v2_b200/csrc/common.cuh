@@ -41,6 +41,7 @@ void check_cuda(cudaError_t e, const char *what);
 struct GridDev {
   int N, E, NV, nE2;              // nE2 = eoeStart[E], the length of the TRiSK CSR
   const int *eI, *eJ, *nbr, *cellEdge, *cellEdgeAsc, *ev1, *ev2, *vEdge, *vCell, *eoeStart, *eoe, *d2idx;
+  const int2 *eIJ;                // (eI, eJ) per edge, one 8-byte load
   const int8_t *cellSign, *vEdgeSign, *vSlot;
   const double *le, *de, *areaCell, *areaV, *fV, *kite, *w, *d2wt;
   const float *w32, *d2wt32, *le32, *de32, *rde32, *rle32, *rA32, *rAV32, *kite32;
@@ -160,7 +161,9 @@ struct LayersDev {
   // mixed-form scratch (allocated for ISW_MIXED only): FP32 stage winds and operators; the fast loop in deviation form
   // (deta = eta - eta0, dub = ubar - ubar0) with its exchange buffers; pk4 = per edge and layer (h_e, u, q_e, 0)
   float *u32, *u1f, *u2f, *D1f, *Z1f, *L1f, *L2f, *q32, *Tp32, *G32, *He32, *ubs32, *Gc32;
-  float *c0, *dub, *deta, *deprev, *xeta[2], *xdub[2], *cw32;
+  float *dub, *deta, *deprev, *xeta[2], *xdub[2];
+  float *cw32;                               // grid-wide fast loop, per cell (N x 8): sign l_e H_e / A per slot, c0 / A, Gc
+  float2 *Gr32;                              // per edge (G, 1/d_e): the grid-wide edge sub-step's two operands in one load
   float *F32, *scale32;                      // mixed form: stored layer fluxes (L x E) and limiter factors (L x N)
   double *wsum;                              // mixed form, grid-wide fast loop: W, the weighted sum of Y (N)
   float4 *pk4;

@@ -167,6 +167,11 @@ static isw_grid *grid_create(const isw_grid_host *h, int device) {
     GridDev &d = g->d;
     d.N = N; d.E = E; d.NV = NV; d.nE2 = nE2;
     d.eI = upload(g, h->eI, E); d.eJ = upload(g, h->eJ, E);
+    {
+      std::vector<int32_t> eij((size_t)E * 2);
+      for (int e = 0; e < E; e++) { eij[2 * (size_t)e] = h->eI[e]; eij[2 * (size_t)e + 1] = h->eJ[e]; }
+      d.eIJ = reinterpret_cast<const int2 *>(upload(g, eij.data(), eij.size()));
+    }
     d.nbr = upload(g, h->nbr, (size_t)N * 6);
     d.cellEdge = upload(g, h->cellEdge, (size_t)N * 6);
     d.cellEdgeAsc = upload(g, h->cellEdgeAsc, (size_t)N * 6);

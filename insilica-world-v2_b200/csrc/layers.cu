@@ -433,7 +433,8 @@ isw_layers *layers_create(isw_grid *g, const isw_layers_params *p) {
       d.u32 = f((size_t)L * E); d.u1f = f((size_t)L * E); d.u2f = f((size_t)L * E);
       d.D1f = f((size_t)L * N); d.Z1f = f((size_t)L * NV); d.L1f = f((size_t)L * E); d.L2f = f((size_t)L * E);
       d.q32 = f((size_t)L * NV); d.Tp32 = f((size_t)L * E); d.G32 = f(E); d.He32 = f(E); d.ubs32 = f(E);
-      d.c0 = f(N); d.dub = f(E); d.deta = f(N); d.deprev = f(N); d.cw32 = f((size_t)N * 6);
+      d.dub = f(E); d.deta = f(N); d.deprev = f(N); d.cw32 = f((size_t)N * 8);
+      d.Gr32 = talloc_t<float2>(s, E);
       d.F32 = f((size_t)L * E); d.scale32 = f((size_t)L * N);
       d.wsum = dalloc(s, N);
       d.xeta[0] = f(N); d.xeta[1] = f(N); d.xdub[0] = f(E); d.xdub[1] = f(E);

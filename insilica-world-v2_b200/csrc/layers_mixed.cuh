@@ -265,7 +265,9 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
 #pragma unroll
   for (int k = 0; k < L; k++) M.Tp32[(size_t)k * E + e] = T[k] - gm;
   const double gb = (M.Gc[b] * M.eta0[b] - M.Gc[a] * M.eta0[a]) * rde;   // eta0's gradient, FP64
-  M.G32[e] = (float)((double)gm - gb);
+  const float G = (float)((double)gm - gb);
+  M.G32[e] = G;
+  M.Gr32[e] = make_float2(G, (float)rde);
   M.He32[e] = H;
   M.ubs32[e] = U / H;
 }
@@ -276,8 +278,8 @@ __device__ __forceinline__ void slow_edge(const LayersDev &M, const float *__res
 __device__ __forceinline__ float bt_u_new(float v, float tau, float G, float yi, float yj, float rde) {
   return __fmaf_rn(tau, __fmaf_rn(-__fsub_rn(yj, yi), rde, G), v);
 }
-__device__ __forceinline__ float bt_eta_new(float d0, float tau, float div, float rA) {
-  return __fmaf_rn(-__fmul_rn(tau, div), rA, d0);
+__device__ __forceinline__ float bt_eta_new(float d0, float tau, float div) {   // div already over the cell's area
+  return __fmaf_rn(-tau, div, d0);
 }
 __device__ __forceinline__ float bt_y_new(float gc, float gam, float dn, float d0) {
   return __fmul_rn(gc, __fmaf_rn(gam, __fsub_rn(dn, d0), dn));
@@ -299,65 +301,66 @@ __device__ __forceinline__ double bt_acc_of(float tau, float G, double wi, doubl
 }
 
 // ---- fast loop, grid-wide form (stacks without tiles): deviation variables; the cell pass stores Y = Gc (deta +
-// gamma (deta - deta_prev)) in deprev for the edge pass, and adds its share to W ----
+// gamma (deta - deta_prev)) in deprev for the edge pass, and adds its share to W. Sub-step 0 forms each cell's row of
+// constants for the stage (cw32, 32 bytes: the six slot coefficients sign l_e H_e and c0 = their sum against ubar0,
+// all over the cell's area, then Gc), which later sub-steps read as two 16-byte loads. ----
 __device__ __forceinline__ void bt_eta_cell(const LayersDev &M, float tau, int j, int n, int i) {
   const GridDev &g = M.g;
   int es[6];
   float c[6];
   slots6(g.cellEdge, i, es);
-  float c0;
-  if (j == 0) {                              // slot coefficients sign l_e H_e and c0, constant over the stage
+  float c0, gc;
+  float4 *row = reinterpret_cast<float4 *>(M.cw32 + (size_t)i * 8);
+  if (j == 0) {
     int sg[6];
     signs6(g.cellSign, i, sg);
+    const float rA = g.rA32[i];
     c0 = 0.f;
 #pragma unroll
     for (int s = 0; s < 6; s++) {
       const int e = es[s];
-      c[s] = e >= 0 ? (float)sg[s] * g.le32[e] * M.He32[e] : 0.f;
-      M.cw32[(size_t)i * 6 + s] = c[s];
-      if (e >= 0) c0 += c[s] * (float)M.ub0[e];
+      const float cs = e >= 0 ? (float)sg[s] * g.le32[e] * M.He32[e] : 0.f;
+      if (e >= 0) c0 += cs * (float)M.ub0[e];
+      c[s] = __fmul_rn(cs, rA);
     }
-    M.c0[i] = c0;
+    c0 = __fmul_rn(c0, rA);
+    gc = M.Gc32[i];
+    row[0] = make_float4(c[0], c[1], c[2], c[3]);
+    row[1] = make_float4(c[4], c[5], c0, gc);
   } else {
-    const float2 *cw = reinterpret_cast<const float2 *>(M.cw32 + (size_t)i * 6);   // 24-byte rows: three 8-byte loads
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const float2 v = cw[q];
-      c[2 * q] = v.x;
-      c[2 * q + 1] = v.y;
-    }
-    c0 = M.c0[i];
+    const float4 r0 = row[0], r1 = row[1];
+    c[0] = r0.x; c[1] = r0.y; c[2] = r0.z; c[3] = r0.w; c[4] = r1.x; c[5] = r1.y;
+    c0 = r1.z;
+    gc = r1.w;
   }
   const float d0 = M.deta[i];
   float div = c0;
 #pragma unroll
   for (int s = 0; s < 6; s++)
     if (es[s] >= 0) div = __fmaf_rn(c[s], M.dub[es[s]], div);
-  const float dn = bt_eta_new(d0, tau, div, g.rA32[i]);
+  const float dn = bt_eta_new(d0, tau, div);
   M.deta[i] = dn;
-  const float y = bt_y_new(M.Gc32[i], (float)M.div_damp, dn, d0);
+  const float y = bt_y_new(gc, (float)M.div_damp, dn, d0);
   M.deprev[i] = y;                           // Y, what the edge pass reads
   bt_w_next(M.wsum, i, y, j, n);
 }
 
 // sub-step j of edge e; on the last one (j = n - 1) also its sum acc, from W
 __device__ __forceinline__ void bt_u_edge(const LayersDev &M, float tau, int j, int n, int e) {
-  const GridDev &g = M.g;
   const float v = M.dub[e];
   const float *Y = M.deprev;
-  const int a = g.eI[e], b = g.eJ[e];
-  M.dub[e] = bt_u_new(v, tau, M.G32[e], Y[a], Y[b], g.rde32[e]);
-  if (j == n - 1) M.acc[e] = bt_acc_of(tau, M.G32[e], M.wsum[a], M.wsum[b], g.rde32[e], n);
+  const int2 ij = M.g.eIJ[e];
+  const float2 gr = M.Gr32[e];
+  M.dub[e] = bt_u_new(v, tau, gr.x, Y[ij.x], Y[ij.y], gr.y);
+  if (j == n - 1) M.acc[e] = bt_acc_of(tau, gr.x, M.wsum[ij.x], M.wsum[ij.y], gr.y, n);
 }
 
 // ---- The split sub-step passes over a wide chunk (up to SUB_W items a thread, THREADS apart): each thread issues the
 // plain loads of all its items, then their gathers, then computes and stores, so a thread keeps SUB_W items' loads in
 // flight and reads the stack's pointers once for all of them. Per item the arithmetic of bt_u_edge / bt_eta_cell. ----
 __device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int j, int n, int first, int end) {
-  const int *__restrict__ eI = M.g.eI;
-  const int *__restrict__ eJ = M.g.eJ;
-  const float *__restrict__ rde = M.g.rde32;
-  const float *__restrict__ G = M.G32;
+  const int2 *__restrict__ eIJ = M.g.eIJ;
+  const float2 *__restrict__ Gr = M.Gr32;
   const float *__restrict__ Y = M.deprev;
   float *__restrict__ dub = M.dub;
   float v[SUB_W], gq[SUB_W], rq[SUB_W], ya[SUB_W], yb[SUB_W];
@@ -369,10 +372,12 @@ __device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int j,
     ia[q] = ib[q] = 0;
     if (e < end) {
       v[q] = dub[e];
-      gq[q] = G[e];
-      rq[q] = rde[e];
-      ia[q] = eI[e];
-      ib[q] = eJ[e];
+      const float2 gr = Gr[e];
+      gq[q] = gr.x;
+      rq[q] = gr.y;
+      const int2 ij = eIJ[e];
+      ia[q] = ij.x;
+      ib[q] = ij.y;
     }
   }
 #pragma unroll
@@ -412,10 +417,7 @@ __device__ __forceinline__ void bt_u_edges(const LayersDev &M, float tau, int j,
 template <int W>
 __device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int j, int n, int first, int end) {
   const int *__restrict__ cellEdge = M.g.cellEdge;
-  const float *__restrict__ cw32 = M.cw32;
-  const float *__restrict__ c0 = M.c0;
-  const float *__restrict__ rA = M.g.rA32;
-  const float *__restrict__ Gc = M.Gc32;
+  const float4 *__restrict__ rows = reinterpret_cast<const float4 *>(M.cw32);
   const float *__restrict__ dub = M.dub;
   float *__restrict__ deta = M.deta;
   float *__restrict__ Y = M.deprev;
@@ -423,26 +425,20 @@ __device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int 
   const float gam = (float)M.div_damp;
   for (int base = first; base < end; base += W * THREADS) {
     int es[W][6];
-    float c[W][6], u[W][6], cz[W], d0[W], ra[W], gc[W];
+    float c[W][6], u[W][6], cz[W], d0[W], gc[W];
 #pragma unroll
     for (int q = 0; q < W; q++) {
       const int i = base + q * THREADS;
-      cz[q] = d0[q] = ra[q] = gc[q] = 0.f;
+      cz[q] = d0[q] = gc[q] = 0.f;
 #pragma unroll
       for (int s = 0; s < 6; s++) { es[q][s] = -1; c[q][s] = 0.f; }
       if (i < end) {
         slots6(cellEdge, i, es[q]);
-        const float2 *cw = reinterpret_cast<const float2 *>(cw32 + (size_t)i * 6);
-#pragma unroll
-        for (int h = 0; h < 3; h++) {
-          const float2 x = cw[h];
-          c[q][2 * h] = x.x;
-          c[q][2 * h + 1] = x.y;
-        }
-        cz[q] = c0[i];
+        const float4 r0 = rows[2 * (size_t)i], r1 = rows[2 * (size_t)i + 1];
+        c[q][0] = r0.x; c[q][1] = r0.y; c[q][2] = r0.z; c[q][3] = r0.w; c[q][4] = r1.x; c[q][5] = r1.y;
+        cz[q] = r1.z;
+        gc[q] = r1.w;
         d0[q] = deta[i];
-        ra[q] = rA[i];
-        gc[q] = Gc[i];
       }
     }
 #pragma unroll
@@ -457,7 +453,7 @@ __device__ __forceinline__ void bt_eta_cells(const LayersDev &M, float tau, int 
 #pragma unroll
         for (int s = 0; s < 6; s++)
           if (es[q][s] >= 0) div = __fmaf_rn(c[q][s], u[q][s], div);
-        const float dn = bt_eta_new(d0[q], tau, div, ra[q]);
+        const float dn = bt_eta_new(d0[q], tau, div);
         deta[i] = dn;
         const float y = bt_y_new(gc[q], gam, dn, d0[q]);
         Y[i] = y;
