@@ -39,10 +39,6 @@ namespace isw {
 using namespace bt;
 namespace {
 
-
-// EXT: the kernel also carries the air branch and the option branches (walls, the shelf and its bed flags, per-cell
-// buoyancy, the tide, the bottom's drag), instantiated only for batches holding such stacks, so that the plain
-// Boussinesq phases keep their register count.
 // The grid-wide sub-step passes over a wide chunk: PH_ETA's cells, PH_U's / PH_UF's edges (PH_UF also forming the
 // layer fluxes on the stack's last sub-step); air stacks and sub-step 0's cell pass (which also forms the slot
 // coefficients) item by item.
@@ -71,6 +67,9 @@ __device__ __forceinline__ void substep_chunk(const StackDesc &d, int st, int j,
   }
 }
 
+// EXT: the kernel also carries the air branch and the option branches (walls, the shelf and its bed flags, per-cell
+// buoyancy, the tide, the bottom's drag), instantiated only for batches holding such stacks, so that the plain
+// Boussinesq phases keep their register count.
 template <int PH, int LMAXK, bool EXT>
 __global__ void __launch_bounds__(THREADS) k_phase(const StackDesc *__restrict__ S, const Sched sc, int st, int j) {
   Chunk ch{0, 0, 0};
