@@ -45,7 +45,7 @@ def _masses(stack):
     return np.array(vol), np.array(trm)
 
 
-def member(level=6, days=10.0, seed=0, device=0, fp64_kinds=None):
+def member(level=6, days=10.0, seed=0, device=0, fp64_kinds=None, tiles=None):
     g = planet_grid(G.build(level, device=device))
     forms = {}
     for prec in ('double', 'mixed'):
@@ -55,6 +55,8 @@ def member(level=6, days=10.0, seed=0, device=0, fp64_kinds=None):
         finally:
             gpu.set_precision('double')
         b = Batch(device)
+        if tiles is not None:                  # the fast loop in tiles or in grid-wide passes (None: the default)
+            b.config(tiles=tiles)
         m = Member(dg, seed, batch=b, fp64_kinds=fp64_kinds)
         forms[prec] = (m, b, [_masses(s) for s in m.stacks])
     steps = int(round(days * SECONDS_PER_DAY / forms['double'][0].dt))

@@ -87,6 +87,19 @@ def test_member_ten_days_at_ensemble_levels(dev, level):
             assert row['form'] == 'mixed', row
 
 
+@pytest.mark.parametrize('level', [5, 6])
+def test_member_ten_days_grid_wide(dev, level):
+    """The member over 10 model days with the fast loop in grid-wide passes (the layout batches of several members
+    run; in the mixed form its sub-step sum comes from the per-cell weighted sum of Y): the same bounds against the FP64
+    form as in tiles, relative L2 of h and u <= 1e-5 and layer-volume and tracer-mass drift <= 1e-13."""
+    from isw import accuracy
+    r = accuracy.member(level, 10.0, tiles=False)
+    assert r['status'] == [0, 0]
+    for row in r['stacks']:
+        assert row['h_l2'] <= 1e-5 and row['u_l2'] <= 1e-5, row
+        assert row['volume_drift_mixed'] <= 1e-13 and row['tracer_mass_drift_mixed'] <= 1e-13, row
+
+
 def test_level7_galewsky_six_days(dev):
     """The Galewsky jet at level 7 over the full 6 model days (9216 steps of 56.25 s), mixed form against the
     FP64 form (reference tests/test_accuracy.py:51-55 vertex vorticity, :111-128 Galewsky): relative L2 and Linf of h
