@@ -260,8 +260,9 @@ def test_tiled_fast_loop_equals_grid_wide(dev, grid4, k):
 @pytest.mark.parametrize('precision', ['double', 'mixed'])
 def test_grid_wide_forms_equal(dev, grid4, precision):
     """The grid-wide sub-steps as two launches each (over wide chunks, several items a thread) give the persistent
-    loop's result (item by item) bit for bit: members of different sub-step counts in one batch (nfast 20 and 7), and a
-    grid-wide level beside a tiled one (the layer fluxes then formed in phase C)."""
+    loop's result (item by item) bit for bit: members of different sub-step counts in one batch (nfast 20, 7 and 2, the
+    last with stages of one sub-step), and a grid-wide level beside a tiled one (the layer fluxes then formed in phase
+    C)."""
     from isw import gpu
     from isw import grid as G
     from isw.batch import Batch
@@ -276,7 +277,8 @@ def test_grid_wide_forms_equal(dev, grid4, precision):
             bt = Batch(0)
             bt.config(tiles=False, grid=grid)
             uneven[grid] = (bt, [Member(dg4, 30, nfast=20, ntracers=2, batch=bt, fp64_kinds=()),
-                                 Member(dg4, 31, nfast=7, ntracers=2, batch=bt, fp64_kinds=())])
+                                 Member(dg4, 31, nfast=7, ntracers=2, batch=bt, fp64_kinds=()),
+                                 Member(dg4, 32, nfast=2, dt=60.0, ntracers=2, batch=bt, fp64_kinds=())])
             bt = Batch(0)
             bt.config(tiles=True, layout='packed', grid=grid, levels={3: ('packed', 128, 2), 4: ('untiled', 0, 0)})
             beside[grid] = (bt, [Member(dg3, 5, nfast=20, ntracers=2, batch=bt, fp64_kinds=()),
